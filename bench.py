@@ -1,0 +1,394 @@
+"""Benchmark: radial integrals/s of the DWBA radial matrix-element hot path on B200.
+
+Workload (synthetic kernel batch): exponential grid N = 15000 on r in [1e-5, 400] a0;
+4 seeded bound products u_i u_f with u = r^a e^{-br} P2(r), a in {1,2}, b in U[0.5,2];
+2048 seeded continuum pairs (chi_i, chi_f), chi_l = sin(kr - l pi/2 + d)(1 - e^{-(r/r0)^{l+1}}),
+k in U[0.5, 8], d in U[0, pi], l in 0..63, r0 = (l+1)/k; multipoles L = 0..8; direct and
+exchange for every (continuum pair, bound pair): 147,456 integrals per step, each with the
+reference's phase-split Clenshaw-Curtis quadrature (idx_match = -1, so n1 = N).
+
+A step evaluates all of them. ``value`` times the device work (node-set operators, operand
+folds, bilinear forms) with every input resident in HBM; ``e2e`` times the public batched API
+(``radial_ME_all_L_batch``) from host NumPy arrays: planning, host->device copies, kernels and
+the device->host read of the results. Inputs (~1 GB of operands per step) exceed the 126 MB L2.
+
+--impl reference times the oracle port (a NumPy restatement of the reference's CPU algorithm:
+dense N x N multipole matrices, Filon direct and the CC exchange gather) on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "radial integrals/s (split-BF16 vs FP64, 1 B200) at <=1e-6 rel TCS error; ms per energy"
+N_GRID, R_MAX, N_CONT, N_BOUND, L_MAX = 15000, 400.0, 2048, 4, 8
+
+
+# ----------------------------------------------------------------------------- workload
+class _Grid:
+    def __init__(self, r, dr, w_trapz, w_simpson):
+        self.r, self.dr, self.w_trapz, self.w_simpson = r, dr, w_trapz, w_simpson
+
+
+class _Bound:
+    def __init__(self, l, u):
+        self.l, self.energy_au, self.u_of_r, self.n_index = l, -0.5, u, 1
+
+
+class _Wave:
+    def __init__(self, l, k, d, chi):
+        self.l, self.k_au, self.phase_shift, self.chi_of_r = l, k, d, chi
+        self.idx_match, self.eta, self.sigma_l = -1, 0.0, 0.0
+
+
+def make_grid(N=N_GRID, r_min=1e-5, r_max=R_MAX):
+    """Exponential grid with trapezoid and non-uniform Simpson weights (grid.py:419-611 formulas)."""
+    idx = np.linspace(0.0, 1.0, N)
+    r = r_min * ((r_max / r_min) ** idx)
+    dr = np.diff(r)
+    wt = np.zeros(N)
+    wt[0], wt[-1] = 0.5 * dr[0], 0.5 * dr[-1]
+    wt[1:-1] = 0.5 * (r[2:] - r[:-2])
+    ws = np.zeros(N)
+    h1, h2 = dr[0:N - 2:2], dr[1:N - 1:2]
+    c = (h1 + h2) / 6.0
+    ws[0:N - 2:2] += c * (2.0 - h2 / h1)
+    ws[1:N - 1:2] += c * ((h1 + h2) ** 2 / (h1 * h2))
+    ws[2:N:2] += c * (2.0 - h1 / h2)
+    if N % 2 == 0:
+        ws[-2] += 0.5 * dr[-1]
+        ws[-1] += 0.5 * dr[-1]
+    return _Grid(r, np.append(dr, dr[-1]), wt, ws)
+
+
+def make_workload(N=N_GRID, n_cont=N_CONT, n_bound=N_BOUND, seed_shift=0):
+    g = make_grid(N)
+    r = g.r
+    rng0 = np.random.default_rng(0 + seed_shift)
+    bounds = []
+    for _ in range(n_bound):
+        us = []
+        for _ in range(2):
+            a = int(rng0.integers(1, 3))
+            b = float(rng0.uniform(0.5, 2.0))
+            c = rng0.uniform(-1, 1, size=3)
+            u = r ** a * np.exp(-b * r) * (c[0] + c[1] * r + c[2] * r * r)
+            us.append(u / np.sqrt(np.sum(g.w_trapz * u * u)))
+        bounds.append((_Bound(0, us[0]), _Bound(1, us[1])))
+    rng1 = np.random.default_rng(1 + seed_shift)
+    pairs = []
+    for _ in range(n_cont):
+        w = []
+        for _ in range(2):
+            k = float(rng1.uniform(0.5, 8.0))
+            d = float(rng1.uniform(0.0, np.pi))
+            l = int(rng1.integers(0, 64))
+            r0 = (l + 1) / k
+            w.append(_Wave(l, k, d, np.sin(k * r - 0.5 * l * np.pi + d) * (1.0 - np.exp(-(r / r0) ** (l + 1)))))
+        pairs.append((w[0], w[1]))
+    zeros = np.zeros(N)
+    return g, zeros, bounds, pairs
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.rows, self.proc, self.gpu = [], None, gpu_index
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) > 8:
+                for n, v in zip(names, r[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------------------------- reference / CPU baseline
+def cpu_sample(seconds_hint=20.0, N=N_GRID):
+    """Bounded sample of the reference algorithm (oracle port) on this workload.
+
+    The reference's CPU path (dwba_matrix_elements.py:1057-1116 with oscillatory_integrals.py:2555-2777)
+    spends its time in per-row work: build K_L rows (1/r_> exp(L log ratio)), contract them with
+    rho2 w over N columns (direct) and gather/interpolate them at the N_cc CC nodes (exchange).
+    The sample runs exactly that work, the reference's way, for a block of rows of one
+    continuum/bound pair at L = 0..8, and scales by the fraction of rows: integrals/s =
+    18 * (rows done / n1) / seconds."""
+    import oracle  # noqa: F401  (the oracle is the checker and the CPU baseline, never the product)
+    from oracle.quadrature import adaptive_phase_increment, cc_nodes_on_breakpoints, generate_phase_nodes, \
+        interp_on_radial_grid
+    g, zeros, bounds, pairs = make_workload(N, n_cont=1, n_bound=1)
+    (bi, bf), (ci, cf) = bounds[0], pairs[0]
+    r, w = g.r, g.w_simpson
+    n1 = N
+    k_total = ci.k_au + cf.k_au
+    d = adaptive_phase_increment(r[:n1], k_total, 1.5708)
+    X, W, _ = cc_nodes_on_breakpoints(generate_phase_nodes(r[0], r[n1 - 1], k_total, d), 5)
+    rho2_dir = bf.u_of_r * bi.u_of_r * w
+    rho2_cc = interp_on_radial_grid(X, r, cf.chi_of_r * bi.u_of_r) * W
+    iR = np.clip(np.searchsorted(r, X), 1, N - 1)
+    iL = iR - 1
+    wR = (X - r[iL]) / (r[iR] - r[iL] + 1e-30)
+    wL = 1.0 - wR
+    block = 64
+    rows = 0
+    t0 = time.perf_counter()
+    i0 = 0
+    while time.perf_counter() - t0 < seconds_hint and i0 < n1:
+        ri = r[i0:i0 + block, None]
+        rl = np.minimum(ri, r[None, :])
+        rg = np.maximum(ri, r[None, :])
+        ratio = rl / rg
+        inv = 1.0 / rg
+        lr = np.log(np.minimum(ratio, 1.0 - 1e-12) + 1e-300)
+        for L in range(L_MAX + 1):
+            K = inv if L == 0 else inv * np.exp(L * lr)
+            _ = K @ rho2_dir
+            Kcc = K[:, iL] * wL + K[:, iR] * wR
+            _ = Kcc @ rho2_cc
+        rows += ri.shape[0]
+        i0 += block
+    dt = time.perf_counter() - t0
+    ips = 2 * (L_MAX + 1) * (rows / n1) / dt
+    return ips, dt, rows
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = os.cpu_count()
+    vals = []
+    for _ in range(args.warmup):
+        cpu_sample(seconds_hint=2.0)
+    for _ in range(args.steps):
+        ips, dt, rows = cpu_sample(seconds_hint=max(2.0, min(20.0, 120.0 / max(1, args.steps))))
+        vals.append(ips)
+    v = float(np.median(vals))
+    line = {"metric": METRIC, "value": v, "unit": "integrals/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * 147456 / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "synthetic kernel batch N=15000 r<=400, 2048 continuum x 4 bound pairs, L<=8",
+                       "integrals_per_step": 147456},
+            "cpu_baseline": {"value": v, "unit": "integrals/s", "cores": cores, "kind": "port",
+                             "sample": "oracle port of the reference CPU algorithm: row blocks of one pair at "
+                                       "N=15000, L=0..8, direct+exchange, scaled by rows/n1"},
+            "e2e": {"value": v, "unit": "integrals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ----------------------------------------------------------------------------- our arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--engine", default=os.environ.get("DWBA_BENCH_ENGINE", "semisep"),
+                    choices=["dense", "semisep"])
+    ap.add_argument("--n-cont", type=int, default=N_CONT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    from dwba_b200.dwba_matrix_elements import GPUCache, _make_job, radial_ME_all_L_batch
+    from dwba_b200.engine import PreparedJob
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    # each rank owns its shard of independent continuum pairs (weak scaling: fixed work per GPU)
+    g, zeros, bounds, pairs = make_workload(n_cont=args.n_cont, seed_shift=1000 * rank)
+    n_int = len(pairs) * len(bounds) * (L_MAX + 1) * 2
+    cache = GPUCache.from_grid(g)
+    kw = dict(use_oscillatory_quadrature=True, oscillatory_method="advanced", CC_nodes=5, phase_increment=1.5708,
+              min_grid_fraction=0.10, k_threshold=0.5)
+    preps = []
+    for bi, bf in bounds:
+        job = _make_job(g, zeros, zeros, bi, bf, pairs, L_MAX, zeros, kw, cache)
+        preps.append(PreparedJob(job, cache.dg, args.engine, rebuild_nodesets=True))
+    st = torch.cuda.current_stream()
+
+    def step():
+        for p in preps:
+            p.launch()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    # kernel-level split of one step (events on the launching stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record(st)
+    for p in preps:
+        p.nodesets.launch()
+    ev[1].record(st)
+    for p in preps:
+        p.launch_folds()
+    ev[2].record(st)
+    for p in preps:
+        p.launch_forms()
+    ev[3].record(st)
+    barrier()
+    split = {"nodesets_ms": ev[0].elapsed_time(ev[1]), "folds_ms": ev[1].elapsed_time(ev[2]),
+             "forms_ms": ev[2].elapsed_time(ev[3])}
+    # timed region
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        t_start.record(st)
+        for _ in range(args.steps):
+            step()
+        t_end.record(st)
+        barrier()
+    ms = t_start.elapsed_time(t_end) / args.steps
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * n_int / (ms * 1e-3)
+    # results of the last step, checked for finiteness
+    outs = [p.collect() for p in preps]
+    finite = all(np.isfinite(d).all() and np.isfinite(e).all() for d, e in outs)
+
+    # dominant kernel roofline
+    forms_ms = split["forms_ms"]
+    flops = sum(p.algorithmic_flops() for p in preps)
+    fb = sum(float(np.sum(8.0 * (p.forms_host["n_rows"].astype(np.float64) + p.forms_host["n_cols"] +
+                                 np.maximum(p.forms_host["n_rows"], p.forms_host["n_cols"])))) for p in preps)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    if args.engine == "semisep":
+        ach = fb / (forms_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
+                "traffic": None, "kernel": "semisep_kernel",
+                "note": "algorithmic bytes = 8*(n_rows + n_cols + n_grid) per form (a, b, r read once)"}
+    else:
+        ach = flops / (forms_ms * 1e-3) / 1e12
+        roof = {"bound": "fp64", "achieved": ach, "peak": None, "unit": "TFLOP/s (dense-equivalent 2 n1 n2 per L)",
+                "frac": None, "traffic": None, "kernel": "dense_tri_kernel"}
+
+    # end to end through the public API from host arrays
+    e2e = None
+    if not args.no_e2e:
+        def e2e_step():
+            h2d = 0
+            for bi, bf in bounds:
+                res = radial_ME_all_L_batch(g, zeros, zeros, bi, bf, pairs, L_MAX, U_f_array=zeros,
+                                            gpu_cache=cache, engine=args.engine)
+            return res
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        e_steps = max(1, min(args.steps, 3))
+        for _ in range(e_steps):
+            e2e_step()
+        barrier()
+        e_ms = (time.perf_counter() - t0) * 1e3 / e_steps
+        if world > 1:
+            tt = torch.tensor([e_ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e_ms = float(tt.item())
+        uniq_waves = len({id(w) for pr in pairs for w in pr})
+        h2d = len(bounds) * (uniq_waves + 2) * N_GRID * 8
+        d2h = len(bounds) * len(pairs) * 2 * (L_MAX + 1) * 8
+        e2e = {"value": world * n_int / (e_ms * 1e-3), "unit": "integrals/s", "ms_per_step": e_ms,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "path": "radial_ME_all_L_batch per bound pair from host NumPy inputs"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ips, dt, rows = cpu_sample(seconds_hint=15.0)
+        cpu = {"value": ips, "unit": "integrals/s", "cores": 1, "kind": "port",
+               "sample": f"oracle port of the reference CPU algorithm, {rows} of {N_GRID} rows of one pair, "
+                         f"L=0..8 direct+exchange, {dt:.1f} s, scaled by rows/n1"}
+        try:
+            import threadpoolctl
+            cpu["cores"] = max(i.get("num_threads", 1) for i in threadpoolctl.threadpool_info()) or 1
+        except Exception:
+            pass
+    if rank == 0:
+        n_launch = sum((1 if p.nodesets.n else 0) * 2 + (p.n_folds + 65534) // 65535 +
+                       (2 if args.engine == "dense" else (L_MAX + 16) // 16) for p in preps)
+        line = {"metric": METRIC, "value": value, "unit": "integrals/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "synthetic kernel batch: N=15000 exp grid r in [1e-5,400], "
+                                       "2048 continuum pairs x 4 bound pairs per GPU, L=0..8, direct+exchange",
+                           "engine": args.engine, "integrals_per_step_per_gpu": n_int,
+                           "l2": "inputs larger than L2 (operands ~1 GB/step)", "parallelism": f"dp{world}"},
+                "split_ms": split, "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
+                "gpu_launches": n_launch * args.steps, "results_finite": bool(finite), "clocks": clk.summary()}
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

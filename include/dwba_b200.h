@@ -1,0 +1,169 @@
+/*
+ * dwba_b200.h -- C ABI of the B200 engine for the DWBA radial matrix elements
+ *
+ *     I_L = sum_{i<n_rows} sum_{j<n_cols} a_i K_L(r_i, r_j) b_j ,
+ *     K_L(r, r') = (1/r_>) (r_</r_>)^L      (diagonal: (1/r) (1-1e-12)^L)
+ *
+ * The reference (StaryPasterz/DWBA) is pure Python; its hot path is
+ * dwba_matrix_elements.py:radial_ME_all_L (CPU, :780-1300) and
+ * radial_ME_all_L_gpu (CuPy, :1563-2549), whose 2-D quadrature lives in
+ * oscillatory_integrals.py:oscillatory_kernel_integral_2d (:2385-2777).
+ * Each entry point below replaces one stage of that path; the host binding
+ * (dwba_b200/dwba_matrix_elements.py) keeps the reference call signatures.
+ *
+ * Conventions: every pointer named *_dev is device memory; descriptor arrays
+ * are device arrays of the structs below. All entry points are asynchronous
+ * on the given stream, return a dwba_status code, throw nothing, and never
+ * allocate device memory (scratch buffers are passed in by the caller).
+ */
+#ifndef DWBA_B200_H
+#define DWBA_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* dwba_stream_t; /* == cudaStream_t */
+
+enum dwba_status {
+  DWBA_OK = 0,
+  DWBA_ERR_INVALID_ARG = 1, /* null pointer, bad size, L_max out of range (reference: ValueError) */
+  DWBA_ERR_CUDA = 2,        /* CUDA launch or runtime failure */
+  DWBA_ERR_NO_DEVICE = 3,   /* no usable sm_100 device (reference: RuntimeError without a GPU runtime) */
+  DWBA_ERR_WORKSPACE = 4,   /* caller-provided scratch too small */
+  DWBA_ERR_UNSUPPORTED = 5, /* request outside the kernel's numeric range (e.g. r^-(L+1) overflow) */
+  DWBA_ERR_RANGE = 6        /* a device-side consistency check failed (status word set by a kernel) */
+};
+
+#define DWBA_ABI_VERSION 1
+#define DWBA_MAX_L 63
+
+/* ---------------------------------------------------------------------------
+ * Node set: the phase-split Clenshaw-Curtis quadrature of one (k_total, n1,
+ * eta, phase step) combination, folded into banded operators on the grid.
+ *
+ * Replaces the CC node / interpolation construction of
+ *   oscillatory_integrals.py:2578-2601 (filon) and :2681-2742 (filon_exchange),
+ *   oscillatory_integrals.py:279-302 (_interp_on_radial_grid).
+ * Outputs:
+ *   ta[3*i + d+1], i < n1, d in {-1,0,1}:  T = P1^T diag(W) P1   (outer fold, both terms)
+ *   bx[5*k + d+2], k < n_grid, d in -2..2:  B = Q^T diag(W) P2   (exchange inner fold)
+ * where P1/P2 interpolate (log-r on log grids) onto r[:n1] / r[:n_grid] and Q
+ * interpolates kernel columns linearly in r.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  const double* r_dev;      /* grid radii (n_grid), strictly increasing, > 0 */
+  const double* logr_dev;   /* log(r) (n_grid) */
+  const double* breaks_dev; /* phase breakpoints (n_breaks); NULL => linspace(r[0], r[n1-1], n_breaks) */
+  double* node_w_dev;       /* scratch, >= n_nodes doubles: W of each CC node, ascending order */
+  double* node_t1_dev;      /* scratch, >= n_nodes doubles */
+  double* node_t2_dev;      /* scratch, >= n_nodes doubles */
+  double* node_wr_dev;      /* scratch, >= n_nodes doubles */
+  int32_t* node_j1_dev;     /* scratch, >= n_nodes ints */
+  int32_t* node_j2_dev;     /* scratch, >= n_nodes ints */
+  int32_t* node_il_dev;     /* scratch, >= n_nodes ints */
+  double* ta_dev;           /* out: 3*n1 doubles */
+  double* bx_dev;           /* out: 5*n_grid doubles */
+  int32_t n_grid;
+  int32_t n1;               /* idx_limit */
+  int32_t n_breaks;         /* >= 2; n_nodes = (n_breaks-1) * n_cc */
+  int32_t log1;             /* 1: r[:n1] passes the log-spacing test (interpolate in log r) */
+  int32_t log2;             /* 1: r[:n_grid] passes the log-spacing test */
+  int32_t pad;
+} dwba_nodeset_t;
+
+/* Builds the banded quadrature operators of n_sets node sets.
+ * cc_x_dev/cc_w_dev: Clenshaw-Curtis reference nodes/weights on [-1, 1]
+ * (descending nodes, as oscillatory_integrals.py:120-171 builds them), n_cc <= 15.
+ * status_dev: one int, set non-zero if a band offset falls outside the stored band. */
+int dwba_build_nodesets(const dwba_nodeset_t* sets_dev, int n_sets, int max_nodes, int max_grid,
+                        const double* cc_x_dev, const double* cc_w_dev, int n_cc, int* status_dev,
+                        dwba_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Fold: out[i] = sum_{d=-h..h} op[(2h+1)*i + d+h] * f[i+d] * g[i+d],  i < n_out
+ * (h = 0: op is a weight vector, e.g. Simpson weights; h = 1: ta; h = 2: bx),
+ * and zero for n_out <= i < n_clear.
+ * Replaces the density products and weights of dwba_matrix_elements.py:1028-1046
+ * together with the interpolation/CC-weight folds of the node set.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  const double* op_dev;
+  const double* f_dev;
+  const double* g_dev;
+  double* out_dev;
+  int32_t half_band;   /* 0, 1 or 2 */
+  int32_t n_out;       /* rows written with the stencil */
+  int32_t n_src;       /* valid length of f, g (stencil taps outside [0, n_src) are skipped) */
+  int32_t n_clear;     /* rows [n_out, n_clear) are zeroed */
+} dwba_fold_t;
+
+int dwba_fold(const dwba_fold_t* folds_dev, int n_folds, int max_rows, dwba_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Bilinear forms in FP64: for each form f and L = 0..L_max,
+ *   out[f*(L_max+1) + L] = sum_{i<n_rows} sum_{j<n_cols} a_i K_L(r_i, r_j) b_j.
+ * Replaces the inner/outer contractions of dwba_matrix_elements.py:1113-1116 with
+ * oscillatory_integrals.py:2571/2644 (filon), :2745-2770 (filon_exchange),
+ * :2479-2490 (standard) and the CuPy gemv/dot path of :2324-2513.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  const double* r_dev;  /* grid radii */
+  const double* a_dev;  /* row operand (>= n_rows) */
+  const double* b_dev;  /* column operand (>= n_cols) */
+  int32_t n_rows;
+  int32_t n_cols;
+} dwba_form_t;
+
+/* Dense plain form: every K_L element is generated in registers (never stored),
+ * operands are staged in shared memory, partial sums are reduced with warp
+ * shuffles. Work is split into chunks (CTAs); dwba_dense_chunk_prefix fills
+ * prefix_host[0..n_forms] from m_host[f] = max(n_rows, n_cols) and returns the
+ * chunk total n_cta; the caller copies the prefix to chunk_prefix_dev. partial_dev
+ * needs n_cta*(L_max+1) doubles. diag_scale_host[L] = (1-1e-12)^L, the factor the
+ * reference's ratio clamp (dwba_matrix_elements.py:1079) puts on the diagonal. */
+int64_t dwba_dense_chunk_prefix(const int32_t* m_host, int n_forms, int64_t* prefix_host);
+int dwba_bilinear_dense_fp64(const dwba_form_t* forms_dev, int n_forms, int L_max, const double* diag_scale_host,
+                             const int64_t* chunk_prefix_dev, int64_t n_cta, double* partial_dev,
+                             int64_t partial_cap, double* out_dev, dwba_stream_t stream);
+
+/* Semiseparable form (exact in FP64, O(n L) per form): uses
+ * K_L(r_i, r_j) = r_j^L / r_i^(L+1) for j < i. Returns DWBA_ERR_UNSUPPORTED if
+ * r^-(L_max+1) or r^L could leave the normal FP64 range on [r_min_all, r_max_all]. */
+int dwba_bilinear_semisep_fp64(const dwba_form_t* forms_dev, int n_forms, int L_max,
+                               const double* diag_scale_host, double r_min_all, double r_max_all,
+                               double* out_dev, dwba_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Host helpers (no GPU work)
+ * ------------------------------------------------------------------------- */
+/* Coulomb-phase breakpoints r_{j+1} = r_j + dphi/|k + eta/r_j| (bounded steps),
+ * exactly as oscillatory_integrals.py:1677-1710 (generate_phase_nodes, eta != 0).
+ * Writes at most cap values; *n_out = count (<= 10002). */
+int dwba_phase_breaks_coulomb(double r_start, double r_end, double k_total, double dphi, double eta_total,
+                              double* out_host, int cap, int* n_out);
+
+/* Outer tail of the direct integral for L = 1..L_max of one pair (0 for L = 0):
+ * tail[L] = dwba_outer_integral_1d(M_L / r^(L+1), r_m .. r_max) + analytical r_max->inf tail
+ * (oscillatory_integrals.py:459-535, :1361-1451, :2064-2184; call site
+ * dwba_matrix_elements.py:1213-1241). moments_host[L] = sum w r^L u_f u_i;
+ * an entry with |M_L| <= 1e-12 gives 0. mode: 0 = advanced/full_split, 1 = legacy
+ * (analytical tail from r_m only). wave_host = {k_i, l_i, delta_i, eta_i, sigma_i,
+ * k_f, l_f, delta_f, eta_f, sigma_f}. */
+int dwba_outer_tails(const double* wave_host, double r_m, double r_max, int L_max, const double* moments_host,
+                     int mode, int max_filon_segments, double max_effective_dphi, double* tail_host);
+
+/* Library identity and device probe (the check_cupy_runtime analogue, dwba_matrix_elements.py:178-193). */
+int dwba_abi_version(void);
+const char* dwba_status_string(int status);
+int dwba_device_probe(int* n_devices, int* cc_major, int* cc_minor);
+/* sizeof(dwba_nodeset_t), sizeof(dwba_fold_t), sizeof(dwba_form_t) into sizes[0..2]. */
+int dwba_struct_sizes(int64_t* sizes, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DWBA_B200_H */

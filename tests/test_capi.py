@@ -1,0 +1,52 @@
+"""The C-ABI library loads and exports every entry point declared in include/dwba_b200.h."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+from dwba_b200 import _lib
+
+HDR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "dwba_b200.h")
+
+
+def declared_symbols():
+    text = open(HDR).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dwba_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    syms = declared_symbols()
+    assert len(syms) >= 10
+    for s in syms:
+        assert hasattr(lib, s), s
+
+
+def test_abi_version_and_struct_layout():
+    lib = _lib.load()
+    assert lib.dwba_abi_version() == 1
+    sizes = (ctypes.c_int64 * 3)()
+    assert lib.dwba_struct_sizes(sizes, 3) == 0
+    assert tuple(sizes) == (_lib.NODESET_DTYPE.itemsize, _lib.FOLD_DTYPE.itemsize, _lib.FORM_DTYPE.itemsize)
+
+
+def test_status_strings():
+    for s in range(7):
+        assert _lib.status_string(s)
+
+
+def test_invalid_args_rejected_without_gpu_work():
+    lib = _lib.load()
+    # null descriptors / bad sizes are rejected before any launch
+    assert lib.dwba_build_nodesets(None, 1, 10, 10, None, None, 5, None, None) == _lib.DWBA_ERR_INVALID_ARG
+    assert lib.dwba_fold(None, 1, 10, None) == _lib.DWBA_ERR_INVALID_ARG
+    assert lib.dwba_bilinear_semisep_fp64(None, 1, 4, None, 1e-5, 200.0, None, None) == _lib.DWBA_ERR_INVALID_ARG
+    ds = np.ones(70)
+    assert lib.dwba_bilinear_dense_fp64(None, 1, 99, ds.ctypes.data, None, 1, None, 0, None, None) \
+        == _lib.DWBA_ERR_INVALID_ARG
+    m = np.array([1000, 300], dtype=np.int32)
+    pre = np.zeros(3, dtype=np.int64)
+    assert lib.dwba_dense_chunk_prefix(m.ctypes.data, 2, pre.ctypes.data) == 4 + 2
+    assert list(pre) == [0, 4, 6]

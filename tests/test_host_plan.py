@@ -1,0 +1,101 @@
+"""Host planning (product code) plus a NumPy model of the kernels' index arithmetic, against the goldens.
+
+Runs without a GPU: it checks the integration limit, branch and node-set choice, the
+C++ outer tails and L=0 corrections, and the banded fold design of nodes.cu/fold.cu.
+"""
+import numpy as np
+import pytest
+
+import golden_cases as gc
+import kernel_model as km
+from oracle.folded import folded_eval
+from dwba_b200 import _lib
+from dwba_b200 import dwba_matrix_elements as dme
+from dwba_b200.engine import plan_job
+from dwba_b200.plan import GridInfo, cc_reference
+
+UNIT = np.load(gc.GOLDEN_DIR + "/unit_quadrature.npz")
+
+
+class _Cache:
+    def __init__(self, grid):
+        self.info = GridInfo(grid.r, grid.w_simpson, grid.w_trapz)
+
+
+def _model_eval(call):
+    grid, V, Ui, bi, bf, ci, cf, L_max = call["args"]
+    kw = dict(call["kwargs"])
+    Uf = kw.pop("U_f_array")
+    job = dme._make_job(grid, V, Ui, bi, bf, [(ci, cf)], L_max, Uf, kw, _Cache(grid))
+    pp = plan_job(job)[0]
+    g, N, r = job.grid, job.grid.N, job.grid.r
+    (wi, wf), = job.pairs
+    n1 = pp.n1
+    if pp.osc and pp.nodeset is not None:
+        ns = pp.nodeset
+        ta, bx = km.bands(r, n1, ns.n_breaks, ns.breaks, job.CC_nodes, ns.log1, ns.log2)
+        a_dir = km.fold(ta, 1, wf.chi_of_r, wi.chi_of_r, n1, n1, N)
+        a_ex = km.fold(ta, 1, job.u_f, wi.chi_of_r, n1, n1, N)
+        b_ex = km.fold(bx, 2, wf.chi_of_r, job.u_i, min(N, n1 + 2), N, N)
+        b_dir = g.w * job.u_f * job.u_i
+    else:
+        wl = g.w.copy()
+        wl[n1:] = 0
+        a_dir, a_ex = wl * wf.chi_of_r * wi.chi_of_r, wl * job.u_f * wi.chi_of_r
+        b_ex, b_dir = wl * wf.chi_of_r * job.u_i, wl * job.u_f * job.u_i
+    Id, Ie = folded_eval(r, a_dir, b_dir, L_max), folded_eval(r, a_ex, b_ex, L_max)
+    Sd = folded_eval(r, np.abs(a_dir), np.abs(b_dir), L_max)
+    Se = folded_eval(r, np.abs(a_ex), np.abs(b_ex), L_max)
+    if pp.tail is not None:
+        Id += pp.tail
+        Sd += np.abs(pp.tail)
+    Id[0] += pp.corr_dir
+    Ie[0] += pp.corr_ex
+    Sd[0] += abs(pp.corr_dir)
+    Se[0] += abs(pp.corr_ex)
+    return Id, Ie, Sd, Se, pp
+
+
+@pytest.mark.parametrize("call", gc.all_calls(), ids=[c["label"] for c in gc.all_calls()])
+def test_plan_and_kernel_model(call):
+    Id, Ie, Sd, Se, _ = _model_eval(call)
+    assert np.all(np.abs(Id - call["ref_dir"]) <= 1e-12 * np.abs(call["ref_dir"]) + 1e-14 * Sd)
+    assert np.all(np.abs(Ie - call["ref_exc"]) <= 1e-12 * np.abs(call["ref_exc"]) + 1e-14 * Se)
+
+
+def test_coulomb_breaks_bit_exact():
+    r = np.load(gc.GOLDEN_DIR + "/case_h_1s2p_50eV.npz")["r"]
+    for i in range(5):
+        n, k, dphi, eta, d = UNIT[f"phase_params_{i}"]
+        if abs(eta) < 1e-10:
+            continue
+        rr = r[: int(n)]
+        br = _lib.phase_breaks_coulomb(rr[0], rr[-1], k, d, eta)
+        np.testing.assert_array_equal(br, UNIT[f"phase_nodes_{i}"])
+
+
+def test_outer_tails_native():
+    for row in UNIT["tails"]:
+        rm, rmax, ki, kf, li, lf, di, df, ei, ef, si, sf, L, mom, t_out, t_inf, t_rm, _ = row
+        L = int(L)
+        moments = np.zeros(L + 1)
+        moments[L] = mom
+        wave = [ki, li, di, ei, si, kf, lf, df, ef, sf]
+        adv = _lib.outer_tails(wave, rm, rmax, L, moments, 0, 4096, np.pi / 2)[L]
+        leg = _lib.outer_tails(wave, rm, rmax, L, moments, 1, 4096, np.pi / 2)[L]
+        assert abs(adv - (t_out + t_inf)) <= 1e-12 * abs(t_out + t_inf) + 1e-16
+        assert abs(leg - t_rm) <= 1e-14 * abs(t_rm) + 1e-18
+
+
+def test_cc_tables_match_reference():
+    for n in (2, 3, 5, 7, 9):
+        x, w = cc_reference(n)
+        np.testing.assert_array_equal(x, UNIT[f"cc_x_{n}"])
+        np.testing.assert_array_equal(w, UNIT[f"cc_w_{n}"])
+
+
+def test_invalid_arguments_raise_value_error():
+    with pytest.raises(ValueError):
+        _lib.check(_lib.DWBA_ERR_INVALID_ARG, "x")
+    with pytest.raises(_lib.DWBAError):
+        _lib.check(_lib.DWBA_ERR_CUDA, "x")

@@ -23,8 +23,7 @@ DWBA_ERR_RANGE = 6
 DWBA_MAX_L = 63
 
 # Struct layouts (must match include/dwba_b200.h; checked against the library at load).
-NODESET_DTYPE = np.dtype([(n, "<u8") for n in ("r", "logr", "breaks", "node_w", "node_t1", "node_t2", "node_wr",
-                                              "node_j1", "node_j2", "node_il", "ta", "bx")]
+NODESET_DTYPE = np.dtype([(n, "<u8") for n in ("r", "logr", "breaks", "ta", "bx")]
                          + [(n, "<i4") for n in ("n_grid", "n1", "n_breaks", "log1", "log2", "pad")])
 FOLD_DTYPE = np.dtype([(n, "<u8") for n in ("op", "f", "g", "out")]
                       + [(n, "<i4") for n in ("half_band", "n_out", "n_src", "n_clear")])
@@ -49,7 +48,7 @@ def _declare(lib):
         "dwba_status_string": (ctypes.c_char_p, [c_int]),
         "dwba_device_probe": (c_int, [ctypes.POINTER(c_int)] * 3),
         "dwba_struct_sizes": (c_int, [ctypes.POINTER(c_i64), c_int]),
-        "dwba_build_nodesets": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_int, c_vp, c_vp]),
+        "dwba_build_nodesets": (c_int, [c_vp, c_int, c_int, c_vp, c_vp, c_int, c_vp, c_vp]),
         "dwba_fold": (c_int, [c_vp, c_int, c_int, c_vp]),
         "dwba_dense_chunk_prefix": (c_i64, [c_vp, c_int, c_vp]),
         "dwba_bilinear_dense_fp64": (c_int, [c_vp, c_int, c_int, c_vp, c_vp, c_i64, c_vp, c_i64, c_vp, c_vp]),

@@ -8,155 +8,183 @@
 //     intervals with b - a <= 1e-12 skipped (:2578-2601, :2701-2712);
 //   * outer interpolation P1: _interp_on_radial_grid on r[:n1] (:279-302);
 //   * exchange: rho2 interpolated by P2 on the full grid, kernel columns by
-//     linear-in-r weights Q (:2714-2742).
+//     linear-in-r weights Q with idx_right = clip(searchsorted(r, x), 1, N-1) (:2714-2742).
 // With these, the reference's outer sum sum_c W_c (P1 rho1)_c (P1 v)_c equals
 // rho1^T T v, T = P1^T diag(W) P1 (tridiagonal), and the exchange inner sum
 // sum_c K(r_i, x_c) W_c (P2 rho2)_c equals sum_k K_ik (B rho2)_k with
 // B = Q^T diag(W) P2 (band of half-width 2).
+//
+// One thread per grid row k gathers the nodes that touch row k: a node with
+// interpolation interval j feeds rows j and j+1, so row k needs exactly the
+// nodes in [r_{k-1}, r_{k+1}]. The thread enumerates the phase intervals that
+// overlap that window, recomputes their nodes with the reference's arithmetic,
+// and sums the contributions in ascending node order (deterministic, no scratch
+// memory, no atomics).
 #include "common.cuh"
 
 namespace {
 
-struct NodeGeom {
-  double x, w;
+constexpr int MAX_CC = 15;
+
+struct SetView {
+  const double* r;
+  const double* lr;
+  const double* br;  // breakpoints or nullptr (linspace)
+  int n_grid, n1, n_int, log1, log2;
+  double start, stop, step;
 };
 
-// Position and weight of node c (ascending order) of one node set.
-__device__ __forceinline__ NodeGeom node_geom(const dwba_nodeset_t& s, const double* __restrict__ ccx,
-                                              const double* __restrict__ ccw, int n_cc, int c) {
-  const int m = c / n_cc;
-  const int slot = n_cc - 1 - (c - m * n_cc);  // reference order runs x_ref from +1 down to -1
-  double a, b;
-  if (s.breaks_dev != nullptr) {
-    a = s.breaks_dev[m];
-    b = s.breaks_dev[m + 1];
-  } else {
-    // numpy.linspace(start, stop, num): y[i] = i*step + start, y[num-1] = stop
-    const double start = s.r_dev[0];
-    const double stop = s.r_dev[s.n1 - 1];
-    const int div = s.n_breaks - 1;
-    const double step = rn_sub(stop, start) / (double)div;
-    a = rn_add(rn_mul((double)m, step), start);
-    b = (m + 1 == div) ? stop : rn_add(rn_mul((double)(m + 1), step), start);
-  }
-  NodeGeom g;
-  const double hw = rn_mul(0.5, rn_sub(b, a));
-  g.x = rn_add(rn_mul(hw, rn_add(ccx[slot], 1.0)), a);
-  // Keep the node inside [a, b]: the top node hw*2 + a can round one ulp past b,
-  // and a sorted node list is what the row gathers below rely on.
-  g.x = fmin(fmax(g.x, a), b);
-  g.w = rn_sub(b, a) > 1e-12 ? rn_mul(ccw[slot], hw) : 0.0;
-  return g;
-}
-
-// Interpolation interval and weight on r[:n] for np.interp semantics after
-// clipping into [r0, r[n-1]] (log-r when log_grid): value = (1-t) y[j] + t y[j+1].
-__device__ __forceinline__ void interp_op(const double* __restrict__ r, const double* __restrict__ lr, int n,
-                                          int log_grid, double x, int& j, double& t) {
-  if (x <= r[0]) { j = 0; t = 0.0; return; }
-  if (x >= r[n - 1]) { j = n - 2; t = 1.0; return; }
-  j = dwba_floor_index(r, n, x);
-  if (j > n - 2) j = n - 2;
-  if (log_grid) {
-    t = (log(x) - lr[j]) / (lr[j + 1] - lr[j]);
-  } else {
-    t = (x - r[j]) / (r[j + 1] - r[j]);
+__device__ __forceinline__ void interval(const SetView& s, int m, double& a, double& b) {
+  if (s.br != nullptr) {
+    a = s.br[m];
+    b = s.br[m + 1];
+  } else {  // numpy.linspace: y[i] = i*step + start, y[num-1] = stop
+    a = rn_add(rn_mul((double)m, s.step), s.start);
+    b = (m + 1 == s.n_int) ? s.stop : rn_add(rn_mul((double)(m + 1), s.step), s.start);
   }
 }
 
-__global__ void nodes_kernel(const dwba_nodeset_t* __restrict__ sets, const double* __restrict__ ccx,
-                             const double* __restrict__ ccw, int n_cc) {
-  const dwba_nodeset_t s = sets[blockIdx.y];
-  const int n_nodes = (s.n_breaks - 1) * n_cc;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_nodes; c += gridDim.x * blockDim.x) {
-    const NodeGeom g = node_geom(s, ccx, ccw, n_cc, c);
-    int j1, j2;
-    double t1, t2;
-    interp_op(s.r_dev, s.logr_dev, s.n1, s.log1, g.x, j1, t1);
-    interp_op(s.r_dev, s.logr_dev, s.n_grid, s.log2, g.x, j2, t2);
-    // kernel-column weights: idx_right = clip(searchsorted(r, x), 1, N-1)
-    int ir = dwba_lower_bound(s.r_dev, s.n_grid, g.x);
-    ir = ir < 1 ? 1 : (ir > s.n_grid - 1 ? s.n_grid - 1 : ir);
-    const int il = ir - 1;
-    const double wr = (g.x - s.r_dev[il]) / (s.r_dev[ir] - s.r_dev[il] + 1e-30);
-    s.node_w_dev[c] = g.w;
-    s.node_t1_dev[c] = t1;
-    s.node_t2_dev[c] = t2;
-    s.node_wr_dev[c] = wr;
-    s.node_j1_dev[c] = j1;
-    s.node_j2_dev[c] = j2;
-    s.node_il_dev[c] = il;
-  }
-}
-
-// Row gathers (deterministic: each output row sums its nodes in ascending order).
-__global__ void bands_kernel(const dwba_nodeset_t* __restrict__ sets, int n_cc, int* status) {
-  const dwba_nodeset_t s = sets[blockIdx.y];
-  const int n_nodes = (s.n_breaks - 1) * n_cc;
-  const int n_rows = s.n_grid;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_rows; k += gridDim.x * blockDim.x) {
-    // --- T = P1^T diag(W) P1, rows k < n1 -------------------------------------------
-    if (k < s.n1) {
-      double lo = 0.0, di = 0.0, up = 0.0;
-      // nodes with j1 == k-1 contribute through their right tap (weight t)
-      if (k >= 1) {
-        int c0 = dwba_lower_bound_i(s.node_j1_dev, n_nodes, k - 1);
-        for (int c = c0; c < n_nodes && s.node_j1_dev[c] == k - 1; ++c) {
-          const double w = s.node_w_dev[c], t = s.node_t1_dev[c];
-          di += w * t * t;
-          lo += w * t * (1.0 - t);
-        }
-      }
-      int c0 = dwba_lower_bound_i(s.node_j1_dev, n_nodes, k);
-      for (int c = c0; c < n_nodes && s.node_j1_dev[c] == k; ++c) {
-        const double w = s.node_w_dev[c], t = s.node_t1_dev[c];
-        di += w * (1.0 - t) * (1.0 - t);
-        up += w * (1.0 - t) * t;
-      }
-      s.ta_dev[3 * k + 0] = lo;
-      s.ta_dev[3 * k + 1] = di;
-      s.ta_dev[3 * k + 2] = up;
+// last interval m whose left end a_m <= x (0 if none)
+__device__ __forceinline__ int interval_floor(const SetView& s, double x) {
+  if (s.br != nullptr) {
+    int lo = 0, hi = s.n_int;  // a_lo <= x < a_hi
+    if (!(s.br[0] <= x)) return 0;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (s.br[mid] <= x) lo = mid; else hi = mid;
     }
-    // --- B = Q^T diag(W) P2, all rows ----------------------------------------------
+    return lo;
+  }
+  double q = floor((x - s.start) / s.step);
+  int m = q < 0.0 ? 0 : (q > (double)(s.n_int - 1) ? s.n_int - 1 : (int)q);
+  // the closed form can be one off after rounding: correct against the exact interval ends
+  double a, b;
+  interval(s, m, a, b);
+  while (m > 0 && a > x) { --m; interval(s, m, a, b); }
+  while (m + 1 < s.n_int) {
+    double a2, b2;
+    interval(s, m + 1, a2, b2);
+    if (a2 <= x) { ++m; } else break;
+  }
+  return m;
+}
+
+__global__ void nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets, const double* __restrict__ ccx_g,
+                                    const double* __restrict__ ccw_g, int n_cc, int* status) {
+  __shared__ double ccx[MAX_CC], ccw[MAX_CC];
+  if (threadIdx.x < n_cc) {
+    ccx[threadIdx.x] = ccx_g[threadIdx.x];
+    ccw[threadIdx.x] = ccw_g[threadIdx.x];
+  }
+  __syncthreads();
+  const dwba_nodeset_t d = sets[blockIdx.y];
+  SetView s;
+  s.r = d.r_dev;
+  s.lr = d.logr_dev;
+  s.br = d.breaks_dev;
+  s.n_grid = d.n_grid;
+  s.n1 = d.n1;
+  s.n_int = d.n_breaks - 1;
+  s.log1 = d.log1;
+  s.log2 = d.log2;
+  s.start = s.r[0];
+  s.stop = s.r[s.n1 - 1];
+  s.step = rn_sub(s.stop, s.start) / (double)s.n_int;
+  const int N = s.n_grid, n1 = s.n1;
+  const double* __restrict__ r = s.r;
+
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const double wlo = k >= 1 ? r[k - 1] : -1.0e308;
+    const double whi = k + 1 <= N - 1 ? r[k + 1] : 1.0e308;
+    double t_lo = 0.0, t_di = 0.0, t_up = 0.0;
     double band[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     bool bad = false;
-    for (int side = 0; side < 2; ++side) {
-      // side 0: nodes with il == k (left column, weight 1-wr); side 1: il == k-1 (right column, wr)
-      const int key = k - side;
-      if (key < 0) continue;
-      int c0 = dwba_lower_bound_i(s.node_il_dev, n_nodes, key);
-      for (int c = c0; c < n_nodes && s.node_il_dev[c] == key; ++c) {
-        const double wr = s.node_wr_dev[c];
-        const double q = side == 0 ? 1.0 - wr : wr;
-        const double w = s.node_w_dev[c], t = s.node_t2_dev[c];
-        const int j = s.node_j2_dev[c];
-        const int d0 = j - k, d1 = j + 1 - k;
-        if (d0 < -2 || d1 > 2) { bad = true; continue; }
-        band[d0 + 2] += q * w * (1.0 - t);
-        band[d1 + 2] += q * w * t;
+    // nodes never leave [r0, r[n1-1]]; rows past n1+1 have none
+    if (k <= n1 + 1) {
+      // one interval earlier too: its top node can coincide with the window's lower end
+      const int m0 = max(0, interval_floor(s, wlo) - 1);
+      for (int m = m0; m < s.n_int; ++m) {
+        double a, b;
+        interval(s, m, a, b);
+        if (a > whi) break;
+        const double width = rn_sub(b, a);
+        if (!(width > 1e-12)) continue;
+        const double hw = rn_mul(0.5, width);
+        for (int sl = n_cc - 1; sl >= 0; --sl) {  // ascending positions within the interval
+          double x = rn_add(rn_mul(hw, rn_add(ccx[sl], 1.0)), a);
+          x = fmin(fmax(x, a), b);  // the top node can round one ulp past b
+          if (x < wlo || x > whi) continue;
+          const double w = rn_mul(ccw[sl], hw);
+          // interpolation interval on r[:n] (np.interp after clipping; x is inside [r_{k-1}, r_{k+1}])
+          const double lx = (s.log1 || s.log2) ? log(x) : 0.0;
+          int jf;  // floor index in the full grid
+          if (k + 1 <= N - 1 && x >= r[k + 1]) jf = k + 1;
+          else if (x >= r[k]) jf = k;
+          else jf = k - 1;
+          // --- T rows: nodes with j1 in {k-1, k}
+          if (k < n1) {
+            int j1;
+            double t1;
+            if (x <= r[0]) { j1 = 0; t1 = 0.0; }
+            else if (x >= r[n1 - 1]) { j1 = n1 - 2; t1 = 1.0; }
+            else {
+              j1 = jf > n1 - 2 ? n1 - 2 : jf;
+              t1 = s.log1 ? (lx - s.lr[j1]) / (s.lr[j1 + 1] - s.lr[j1]) : (x - r[j1]) / (r[j1 + 1] - r[j1]);
+            }
+            if (j1 == k) {
+              t_di += w * (1.0 - t1) * (1.0 - t1);
+              t_up += w * (1.0 - t1) * t1;
+            } else if (j1 == k - 1) {
+              t_di += w * t1 * t1;
+              t_lo += w * t1 * (1.0 - t1);
+            }
+          }
+          // --- B rows: nodes with il in {k-1, k}
+          int ir;  // searchsorted(r, x, 'left') within the window, then clipped to [1, N-1]
+          if (k >= 1 && x <= r[k - 1]) ir = k - 1;
+          else if (x <= r[k]) ir = k;
+          else ir = k + 1;
+          ir = ir < 1 ? 1 : (ir > N - 1 ? N - 1 : ir);
+          const int il = ir - 1;
+          if (il != k && il != k - 1) continue;
+          int j2;
+          double t2;
+          if (x <= r[0]) { j2 = 0; t2 = 0.0; }
+          else if (x >= r[N - 1]) { j2 = N - 2; t2 = 1.0; }
+          else {
+            j2 = jf > N - 2 ? N - 2 : jf;
+            t2 = s.log2 ? (lx - s.lr[j2]) / (s.lr[j2 + 1] - s.lr[j2]) : (x - r[j2]) / (r[j2 + 1] - r[j2]);
+          }
+          const double wr = (x - r[il]) / (r[ir] - r[il] + 1e-30);
+          const double q = il == k ? 1.0 - wr : wr;
+          const int d0 = j2 - k;
+          if (d0 < -2 || d0 + 1 > 2) { bad = true; continue; }
+          band[d0 + 2] += q * w * (1.0 - t2);
+          band[d0 + 3] += q * w * t2;
+        }
       }
     }
-    if (bad) atomicExch(status, 1);
+    if (k < n1) {
+      d.ta_dev[3 * k + 0] = t_lo;
+      d.ta_dev[3 * k + 1] = t_di;
+      d.ta_dev[3 * k + 2] = t_up;
+    }
 #pragma unroll
-    for (int d = 0; d < 5; ++d) s.bx_dev[5 * k + d] = band[d];
+    for (int q = 0; q < 5; ++q) d.bx_dev[5 * k + q] = band[q];
+    if (bad) atomicExch(status, 1);
   }
 }
 
 }  // namespace
 
-extern "C" int dwba_build_nodesets(const dwba_nodeset_t* sets_dev, int n_sets, int max_nodes, int max_grid,
-                                   const double* cc_x_dev, const double* cc_w_dev, int n_cc, int* status_dev,
-                                   dwba_stream_t stream) {
+extern "C" int dwba_build_nodesets(const dwba_nodeset_t* sets_dev, int n_sets, int max_grid, const double* cc_x_dev,
+                                   const double* cc_w_dev, int n_cc, int* status_dev, dwba_stream_t stream) {
   if (n_sets <= 0) return DWBA_OK;
-  if (!sets_dev || !cc_x_dev || !cc_w_dev || !status_dev || n_cc < 2 || n_cc > 15 || max_nodes < 0 ||
-      max_grid < 2 || n_sets > 65535)
+  if (!sets_dev || !cc_x_dev || !cc_w_dev || !status_dev || n_cc < 2 || n_cc > MAX_CC || max_grid < 2 ||
+      n_sets > 65535)
     return DWBA_ERR_INVALID_ARG;
-  cudaStream_t st = (cudaStream_t)stream;
-  dim3 g1(dwba_grid_1d(max_nodes, 256, 4096), n_sets);
-  nodes_kernel<<<g1, 256, 0, st>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc);
-  DWBA_CHECK_LAUNCH();
-  dim3 g2(dwba_grid_1d(max_grid, 256, 4096), n_sets);
-  bands_kernel<<<g2, 256, 0, st>>>(sets_dev, n_cc, status_dev);
+  dim3 grid(dwba_grid_1d(max_grid, 128, 4096), n_sets);
+  nodeset_rows_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc, status_dev);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;
 }

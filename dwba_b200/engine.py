@@ -80,7 +80,7 @@ class CCTables:
 
 
 class NodeSetBatch:
-    """Descriptors and scratch of the node sets a job uses; ``launch()`` (re)builds their operators."""
+    """Descriptors of the node sets a job uses; ``launch()`` (re)builds their banded operators."""
 
     def __init__(self, dg: DeviceGrid, plans: Sequence[NodeSetPlan], n_cc: int, rebuild: bool = False):
         self.dg, self.n_cc = dg, n_cc
@@ -93,24 +93,17 @@ class NodeSetBatch:
         self.ccx, self.ccw = CCTables.get(n_cc, dev)
         recs = np.zeros(len(todo), dtype=_lib.NODESET_DTYPE)
         self.keep = []
-        self.max_nodes = 0
         for i, p in enumerate(todo):
-            n_nodes = (p.n_breaks - 1) * n_cc
-            self.max_nodes = max(self.max_nodes, n_nodes)
-            scratch_d = torch.empty((4, n_nodes), dtype=torch.float64, device=dev)
-            scratch_i = torch.empty((3, n_nodes), dtype=torch.int32, device=dev)
             old = dg.nodesets.get(p.key)
             ta = old.ta if old is not None else torch.empty(3 * p.key.n1, dtype=torch.float64, device=dev)
             bx = old.bx if old is not None else torch.empty(5 * N, dtype=torch.float64, device=dev)
             br = _dev(p.breaks, dev) if p.breaks is not None else None
-            self.keep += [scratch_d, scratch_i, br]
-            recs[i] = (_ptr(dg.r), _ptr(dg.logr), _ptr(br), _ptr(scratch_d[0]), _ptr(scratch_d[1]),
-                       _ptr(scratch_d[2]), _ptr(scratch_d[3]), _ptr(scratch_i[0]), _ptr(scratch_i[1]),
-                       _ptr(scratch_i[2]), _ptr(ta), _ptr(bx), N, p.key.n1, p.n_breaks, int(p.log1), int(p.log2), 0)
+            self.keep.append(br)
+            recs[i] = (_ptr(dg.r), _ptr(dg.logr), _ptr(br), _ptr(ta), _ptr(bx), N, p.key.n1, p.n_breaks,
+                       int(p.log1), int(p.log2), 0)
             dg.nodesets[p.key] = DeviceNodeSet(p, ta, bx, 8 * (3 * p.key.n1 + 5 * N))
         self.recs_d = _dev(recs.view(np.uint8), dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
-        self.scratch_bytes = sum(int(t.numel()) * t.element_size() for t in self.keep if t is not None)
 
     def launch(self) -> None:
         if self.n == 0:
@@ -119,9 +112,9 @@ class NodeSetBatch:
         N = self.dg.info.N
         for s0 in range(0, self.n, 65535):
             n = min(65535, self.n - s0)
-            _lib.check(lib.dwba_build_nodesets(_ptr(self.recs_d) + s0 * _lib.NODESET_DTYPE.itemsize, n,
-                                               self.max_nodes, N, _ptr(self.ccx), _ptr(self.ccw), self.n_cc,
-                                               _ptr(self.status), _stream()), "dwba_build_nodesets")
+            _lib.check(lib.dwba_build_nodesets(_ptr(self.recs_d) + s0 * _lib.NODESET_DTYPE.itemsize, n, N,
+                                               _ptr(self.ccx), _ptr(self.ccw), self.n_cc, _ptr(self.status),
+                                               _stream()), "dwba_build_nodesets")
 
     def check(self) -> None:
         if self.n and int(self.status.item()) != 0:
@@ -177,7 +170,7 @@ def plan_job(job: Job) -> List[PairPlan]:
         ns = None
         if osc and n1 >= 2:
             d = adaptive_dphi(g, n1, k_total, job.phase_increment, eta_total)
-            ns = plan_nodeset(g, NodeSetKey(id(g), n1, k_total, d, eta_total))
+            ns = plan_nodeset(g, NodeSetKey(id(g), n1, k_total, d, eta_total, int(job.CC_nodes)))
         pp = PairPlan(n1=n1, osc=osc, nodeset=ns)
         # L=0 corrections with the limited Simpson weights (dwba_matrix_elements.py:1028-1046, :1249-1296)
         wl = w.copy()

@@ -163,6 +163,7 @@ class NodeSetKey:
     k_total: float
     dphi: float
     eta_total: float
+    n_cc: int
 
 
 @dataclass

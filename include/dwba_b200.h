@@ -58,30 +58,24 @@ typedef struct {
   const double* r_dev;      /* grid radii (n_grid), strictly increasing, > 0 */
   const double* logr_dev;   /* log(r) (n_grid) */
   const double* breaks_dev; /* phase breakpoints (n_breaks); NULL => linspace(r[0], r[n1-1], n_breaks) */
-  double* node_w_dev;       /* scratch, >= n_nodes doubles: W of each CC node, ascending order */
-  double* node_t1_dev;      /* scratch, >= n_nodes doubles */
-  double* node_t2_dev;      /* scratch, >= n_nodes doubles */
-  double* node_wr_dev;      /* scratch, >= n_nodes doubles */
-  int32_t* node_j1_dev;     /* scratch, >= n_nodes ints */
-  int32_t* node_j2_dev;     /* scratch, >= n_nodes ints */
-  int32_t* node_il_dev;     /* scratch, >= n_nodes ints */
   double* ta_dev;           /* out: 3*n1 doubles */
   double* bx_dev;           /* out: 5*n_grid doubles */
   int32_t n_grid;
   int32_t n1;               /* idx_limit */
-  int32_t n_breaks;         /* >= 2; n_nodes = (n_breaks-1) * n_cc */
+  int32_t n_breaks;         /* >= 2 */
   int32_t log1;             /* 1: r[:n1] passes the log-spacing test (interpolate in log r) */
   int32_t log2;             /* 1: r[:n_grid] passes the log-spacing test */
   int32_t pad;
 } dwba_nodeset_t;
 
-/* Builds the banded quadrature operators of n_sets node sets.
+/* Builds the banded quadrature operators of n_sets node sets (one thread per grid
+ * row gathers the CC nodes in [r_{k-1}, r_{k+1}]; no scratch memory).
  * cc_x_dev/cc_w_dev: Clenshaw-Curtis reference nodes/weights on [-1, 1]
  * (descending nodes, as oscillatory_integrals.py:120-171 builds them), n_cc <= 15.
- * status_dev: one int, set non-zero if a band offset falls outside the stored band. */
-int dwba_build_nodesets(const dwba_nodeset_t* sets_dev, int n_sets, int max_nodes, int max_grid,
-                        const double* cc_x_dev, const double* cc_w_dev, int n_cc, int* status_dev,
-                        dwba_stream_t stream);
+ * max_grid >= every set's n_grid. status_dev: one int, set non-zero if a band
+ * offset falls outside the stored band. */
+int dwba_build_nodesets(const dwba_nodeset_t* sets_dev, int n_sets, int max_grid, const double* cc_x_dev,
+                        const double* cc_w_dev, int n_cc, int* status_dev, dwba_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Fold: out[i] = sum_{d=-h..h} op[(2h+1)*i + d+h] * f[i+d] * g[i+d],  i < n_out

@@ -40,7 +40,7 @@ def test_status_strings():
 def test_invalid_args_rejected_without_gpu_work():
     lib = _lib.load()
     # null descriptors / bad sizes are rejected before any launch
-    assert lib.dwba_build_nodesets(None, 1, 10, 10, None, None, 5, None, None) == _lib.DWBA_ERR_INVALID_ARG
+    assert lib.dwba_build_nodesets(None, 1, 10, None, None, 5, None, None) == _lib.DWBA_ERR_INVALID_ARG
     assert lib.dwba_fold(None, 1, 10, None) == _lib.DWBA_ERR_INVALID_ARG
     assert lib.dwba_bilinear_semisep_fp64(None, 1, 4, None, 1e-5, 200.0, None, None) == _lib.DWBA_ERR_INVALID_ARG
     ds = np.ones(70)

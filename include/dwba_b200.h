@@ -124,6 +124,24 @@ int dwba_bilinear_dense_fp64(const dwba_form_t* forms_dev, int n_forms, int L_ma
                              const int64_t* chunk_prefix_dev, int64_t n_cta, double* partial_dev,
                              int64_t partial_cap, double* out_dev, dwba_stream_t stream);
 
+/* Allocation-free variant of dwba_bilinear_dense_fp64. No counterpart in the
+ * reference. For callers that cannot give this library scratch memory: their
+ * device memory is owned by another allocator (a framework's caching pool, a
+ * pool sized at start-up), or their loop must not call cudaMalloc/cudaFree,
+ * which synchronise the device. Inputs and the output are still the caller's;
+ * the partial sums live in a fixed array of DWBA_NOALLOC_SCRATCH_DOUBLES doubles
+ * (8 MiB) inside the library, held by every GPU that loads it until exit.
+ * max_m must be >= max(n_rows, n_cols) of every form (a form above it gets NaN);
+ * requests needing more than the array, n_forms * ceil(ceil(max_m/128)/2) *
+ * (L_max+1) doubles, return DWBA_ERR_WORKSPACE. The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture. All calls share the array: calls that overlap on
+ * the GPU race and must be ordered by the caller (e.g. one stream). Results
+ * equal dwba_bilinear_dense_fp64's (same tiles and summation order). */
+#define DWBA_NOALLOC_SCRATCH_DOUBLES (1 << 20)
+int dwba_bilinear_dense_fp64_noalloc(const dwba_form_t* forms_dev, int n_forms, int max_m, int L_max,
+                                     const double* diag_scale_host, double* out_dev, dwba_stream_t stream);
+
 /* Semiseparable form (exact in FP64, O(n L) per form): uses
  * K_L(r_i, r_j) = r_j^L / r_i^(L+1) for j < i. Returns DWBA_ERR_UNSUPPORTED if
  * r^-(L_max+1) or r^L could leave the normal FP64 range on [r_min_all, r_max_all]. */

@@ -72,9 +72,15 @@ def make_grid(N=N_GRID, r_min=1e-5, r_max=R_MAX):
     return _Grid(r, np.append(dr, dr[-1]), wt, ws)
 
 
-def make_workload(N=N_GRID, n_cont=N_CONT, n_bound=N_BOUND, seed_shift=0):
+def make_workload(N=N_GRID, n_cont=N_CONT, n_bound=N_BOUND, seed_shift=0, pinned=False):
+    """Seeded workload; the continuum waves are rows of one (2*n_cont, N) host matrix (pinned on request)."""
     g = make_grid(N)
     r = g.r
+    if pinned:
+        import torch
+        chi_block = torch.empty((2 * n_cont, N), dtype=torch.float64, pin_memory=True).numpy()
+    else:
+        chi_block = np.empty((2 * n_cont, N))
     rng0 = np.random.default_rng(0 + seed_shift)
     bounds = []
     for _ in range(n_bound):
@@ -88,14 +94,16 @@ def make_workload(N=N_GRID, n_cont=N_CONT, n_bound=N_BOUND, seed_shift=0):
         bounds.append((_Bound(0, us[0]), _Bound(1, us[1])))
     rng1 = np.random.default_rng(1 + seed_shift)
     pairs = []
-    for _ in range(n_cont):
+    for i in range(n_cont):
         w = []
-        for _ in range(2):
+        for j in range(2):
             k = float(rng1.uniform(0.5, 8.0))
             d = float(rng1.uniform(0.0, np.pi))
             l = int(rng1.integers(0, 64))
             r0 = (l + 1) / k
-            w.append(_Wave(l, k, d, np.sin(k * r - 0.5 * l * np.pi + d) * (1.0 - np.exp(-(r / r0) ** (l + 1)))))
+            row = chi_block[2 * i + j]
+            row[:] = np.sin(k * r - 0.5 * l * np.pi + d) * (1.0 - np.exp(-(r / r0) ** (l + 1)))
+            w.append(_Wave(l, k, d, row))
         pairs.append((w[0], w[1]))
     zeros = np.zeros(N)
     return g, zeros, bounds, pairs
@@ -233,7 +241,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--engine", default=os.environ.get("DWBA_BENCH_ENGINE", "semisep"),
-                    choices=["dense", "semisep"])
+                    choices=["dense", "semisep", "tc_bf16x3", "tc_bf16x6"])
     ap.add_argument("--n-cont", type=int, default=N_CONT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -254,15 +262,16 @@ def main():
     dev = torch.device("cuda", local)
 
     # each rank owns its shard of independent continuum pairs (weak scaling: fixed work per GPU)
-    g, zeros, bounds, pairs = make_workload(n_cont=args.n_cont, seed_shift=1000 * rank)
+    g, zeros, bounds, pairs = make_workload(n_cont=args.n_cont, seed_shift=1000 * rank, pinned=True)
     n_int = len(pairs) * len(bounds) * (L_MAX + 1) * 2
     cache = GPUCache.from_grid(g)
     kw = dict(use_oscillatory_quadrature=True, oscillatory_method="advanced", CC_nodes=5, phase_increment=1.5708,
               min_grid_fraction=0.10, k_threshold=0.5)
-    preps = []
-    for bi, bf in bounds:
-        job = _make_job(g, zeros, zeros, bi, bf, pairs, L_MAX, zeros, kw, cache)
-        preps.append(PreparedJob(job, cache.dg, args.engine, rebuild_nodesets=True))
+    b_i = [b[0] for b in bounds]
+    b_f = [b[1] for b in bounds]
+    # one job: the 4 bound transitions share the continuum waves and the 2048 node sets
+    job = _make_job(g, zeros, zeros, b_i, b_f, pairs, L_MAX, zeros, kw, cache)
+    preps = [PreparedJob(job, cache.dg, args.engine, rebuild_nodesets=True)]
     st = torch.cuda.current_stream()
 
     def step():
@@ -286,12 +295,24 @@ def main():
     for p in preps:
         p.launch_folds()
     ev[2].record(st)
-    for p in preps:
-        p.launch_forms()
+    tc = args.engine.startswith("tc_")
+    if tc:
+        ev_tc = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        for p in preps:
+            p.launch_forms_direct()
+        ev_tc[0].record(st)
+        for p in preps:
+            p.launch_forms_exchange()
+        ev_tc[1].record(st)
+    else:
+        for p in preps:
+            p.launch_forms()
     ev[3].record(st)
     barrier()
     split = {"nodesets_ms": ev[0].elapsed_time(ev[1]), "folds_ms": ev[1].elapsed_time(ev[2]),
              "forms_ms": ev[2].elapsed_time(ev[3])}
+    if tc:
+        split["forms_exchange_tensor_ms"] = ev_tc[0].elapsed_time(ev_tc[1])
     # timed region
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
@@ -310,19 +331,30 @@ def main():
     # results of the last step, checked for finiteness
     outs = [p.collect() for p in preps]
     finite = all(np.isfinite(d).all() and np.isfinite(e).all() for d, e in outs)
+    nonzero = all(np.abs(d).max() > 0 and np.abs(e).max() > 0 for d, e in outs)
 
     # dominant kernel roofline
     forms_ms = split["forms_ms"]
     flops = sum(p.algorithmic_flops() for p in preps)
-    fb = sum(float(np.sum(8.0 * (p.forms_host["n_rows"].astype(np.float64) + p.forms_host["n_cols"] +
-                                 np.maximum(p.forms_host["n_rows"], p.forms_host["n_cols"])))) for p in preps)
+    fb = sum(p.algorithmic_bytes() for p in preps)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    if args.engine == "semisep":
+    if tc:
+        t_ms = split["forms_exchange_tensor_ms"]
+        useful = sum(p.tensor_flops()[0] for p in preps)
+        executed = sum(p.tensor_flops()[1] for p in preps)
+        bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+        ach = executed / (t_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": ach, "peak": bf16_peak, "unit": "TFLOP/s", "frac": ach / bf16_peak,
+                "traffic": None, "kernel": "tc_exchange_kernel",
+                "useful_tflops": useful / (t_ms * 1e-3) / 1e12,
+                "note": "achieved = executed bf16 MMA flops (2*M*N*K per product, 3 or 6 products of the split) / "
+                        "kernel time; useful = dense-equivalent 2*n_rows*n_cols per exchange integral"}
+    elif args.engine == "semisep":
         ach = fb / (forms_ms * 1e-3) / 1e9
         roof = {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
                 "traffic": None, "kernel": "semisep_kernel",
@@ -336,11 +368,9 @@ def main():
     e2e = None
     if not args.no_e2e:
         def e2e_step():
-            h2d = 0
-            for bi, bf in bounds:
-                res = radial_ME_all_L_batch(g, zeros, zeros, bi, bf, pairs, L_MAX, U_f_array=zeros,
-                                            gpu_cache=cache, engine=args.engine)
-            return res
+            cache.clear()  # every step rebuilds its quadrature operators and re-uploads its inputs
+            return radial_ME_all_L_batch(g, zeros, zeros, b_i, b_f, pairs, L_MAX, U_f_array=zeros,
+                                         gpu_cache=cache, engine=args.engine)
         e2e_step()
         barrier()
         t0 = time.perf_counter()
@@ -354,11 +384,11 @@ def main():
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             e_ms = float(tt.item())
         uniq_waves = len({id(w) for pr in pairs for w in pr})
-        h2d = len(bounds) * (uniq_waves + 2) * N_GRID * 8
+        h2d = (uniq_waves + 2 * len(bounds)) * N_GRID * 8
         d2h = len(bounds) * len(pairs) * 2 * (L_MAX + 1) * 8
         e2e = {"value": world * n_int / (e_ms * 1e-3), "unit": "integrals/s", "ms_per_step": e_ms,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "path": "radial_ME_all_L_batch per bound pair from host NumPy inputs"}
+               "path": "radial_ME_all_L_batch (4 transitions x 2048 pairs) from pinned host NumPy inputs"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -372,17 +402,17 @@ def main():
         except Exception:
             pass
     if rank == 0:
-        n_launch = sum((1 if p.nodesets.n else 0) * 2 + (p.n_folds + 65534) // 65535 +
-                       (2 if args.engine == "dense" else (L_MAX + 16) // 16) for p in preps)
+        per_forms = {"dense": 2, "semisep": 1, "tc_bf16x3": 5, "tc_bf16x6": 5}[args.engine]
+        n_launch = sum((1 if p.nodesets.n else 0) + (p.n_folds + 65534) // 65535 + per_forms for p in preps)
         line = {"metric": METRIC, "value": value, "unit": "integrals/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "vs_baseline": None, "dtype": "bf16 split (x3/x6) + f64" if tc else "f64", "data": "synthetic",
                 "config": {"workload": "synthetic kernel batch: N=15000 exp grid r in [1e-5,400], "
                                        "2048 continuum pairs x 4 bound pairs per GPU, L=0..8, direct+exchange",
                            "engine": args.engine, "integrals_per_step_per_gpu": n_int,
                            "l2": "inputs larger than L2 (operands ~1 GB/step)", "parallelism": f"dp{world}"},
                 "split_ms": split, "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
-                "gpu_launches": n_launch * args.steps, "results_finite": bool(finite), "clocks": clk.summary()}
+                "gpu_launches": n_launch * args.steps, "results_finite": bool(finite and nonzero), "clocks": clk.summary()}
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

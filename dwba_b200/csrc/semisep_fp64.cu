@@ -80,24 +80,52 @@ semisep_kernel(const dwba_form_t* __restrict__ forms, int L0, int n_ltot, DiagSc
     B[l] = scan[NL + l][tid];
     acc[l] = 0.0;
   }
-  // pass 2: sweep with running prefixes
-  for (int p = p0; p < p1; ++p) {
+  // pass 2: sweep with running prefixes; two elements per iteration so their power chains
+  // overlap. The diagonal term sum_p X_p Y_p / r_p is collected once and scaled per L at the end.
+  double dsum = 0.0;
+  int p = p0;
+  for (; p + 1 < p1; p += 2) {
+    const double X0 = p < F.n_rows ? F.a_dev[p] : 0.0, X1 = p + 1 < F.n_rows ? F.a_dev[p + 1] : 0.0;
+    const double Y0 = p < F.n_cols ? F.b_dev[p] : 0.0, Y1 = p + 1 < F.n_cols ? F.b_dev[p + 1] : 0.0;
+    const double r0 = F.r_dev[p], r1 = F.r_dev[p + 1];
+    const double i0 = 1.0 / r0, i1 = 1.0 / r1;
+    double pw0 = L0 > 0 ? ipow(r0, L0) : 1.0, pw1 = L0 > 0 ? ipow(r1, L0) : 1.0;
+    double ip0 = L0 > 0 ? ipow(i0, L0 + 1) : i0, ip1 = L0 > 0 ? ipow(i1, L0 + 1) : i1;
+    dsum += X0 * Y0 * i0;
+    dsum += X1 * Y1 * i1;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+      acc[l] += ip0 * fma(X0, B[l], Y0 * A[l]);
+      A[l] += X0 * pw0;
+      B[l] += Y0 * pw0;
+      acc[l] += ip1 * fma(X1, B[l], Y1 * A[l]);
+      A[l] += X1 * pw1;
+      B[l] += Y1 * pw1;
+      pw0 *= r0;
+      pw1 *= r1;
+      ip0 *= i0;
+      ip1 *= i1;
+    }
+  }
+  for (; p < p1; ++p) {
     const double X = p < F.n_rows ? F.a_dev[p] : 0.0;
     const double Y = p < F.n_cols ? F.b_dev[p] : 0.0;
     const double r = F.r_dev[p];
     const double inv = 1.0 / r;
     double pw = L0 > 0 ? ipow(r, L0) : 1.0;
     double ipw = L0 > 0 ? ipow(inv, L0 + 1) : inv;
-    const double xy = X * Y;
+    dsum += X * Y * inv;
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
-      acc[l] += ipw * fma(X, B[l], Y * A[l]) + xy * inv * ds.v[L0 + l];
+      acc[l] += ipw * fma(X, B[l], Y * A[l]);
       A[l] += X * pw;
       B[l] += Y * pw;
       pw *= r;
       ipw *= inv;
     }
   }
+#pragma unroll
+  for (int l = 0; l < NL; ++l) acc[l] += dsum * ds.v[L0 + l];
   const int lane = tid & 31, warp = tid >> 5;
 #pragma unroll
   for (int l = 0; l < NL; ++l) {

@@ -1,0 +1,590 @@
+// Split-BF16 tensor-core form of the exchange integrals:
+//     Z_L = K_L B   (tcgen05.mma, FP32 accumulators in TMEM),   I_f,L = sum_i a_f[i] Z_L[i, f]  (FP64)
+//
+// Reference: the exchange contraction of oscillatory_integrals.py:2745-2770 (CPU) and
+// dwba_matrix_elements.py:1469-1560 (CuPy), with the CC quadrature folded into b_f.
+//
+// K_L and B are split into NT bfloat16 terms (NT = 2: hi + lo, products hh, hl, lh;
+// NT = 3: hi + mid + lo, products of total order <= 2). Each CTA owns a 128-row block of
+// the grid (i), BN forms (f) and one multipole L, and walks the grid in 64-wide blocks (j):
+//   * B tiles (BN forms x 64 j per term, K-major, 128-byte swizzle) arrive by TMA;
+//   * K_L tiles (128 x 64 per term) are generated in registers and stored to shared memory
+//     in the same swizzled layout. Off-diagonal blocks are exactly rank one,
+//     K_L(i,j) = U_i V_j (r_j^L / r_i^(L+1) below the diagonal, r_i^L / r_j^(L+1) above),
+//     with U, V scaled by the block's boundary radius so they stay in FP32 range; blocks
+//     that touch the diagonal use the full formula in FP64 (diagonal: (1-1e-12)^L / r);
+//   * one thread issues the tcgen05.mma products into a TMEM accumulator;
+//   * two shared-memory stages let generation of block k+1 overlap the MMAs of block k.
+// The epilogue reads the accumulator with tcgen05.ld, multiplies by a_f[i] in FP64 and
+// reduces over the 128 rows; partials per (L, row block, form) are summed in fixed order.
+// Every mbarrier wait is bounded: on timeout the CTA records an error, drains its own
+// in-flight copies (bounded), frees its TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr int BM = 128;  // rows (i) per CTA = TMEM lanes
+constexpr int BK = 64;   // j per block: 64 bf16 = one 128-byte swizzle row
+constexpr int THREADS = 256;
+constexpr int TC_BN2 = 256;  // forms per CTA with two terms (two 96 KB stages)
+constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz
+
+struct GemmParams {
+  const double* r;             // grid (n_grid)
+  const double* lg;            // log2(r) (n_grid)
+  const dwba_form_t* forms;    // a_f (rows) for the epilogue
+  double* partial;             // [n_L][n_iblk][f_pad]
+  const int* bexp;             // per form: b was scaled by 2^-bexp before the split
+  int* status;                 // error word
+  int n_grid, n_pad, f_pad, n_iblk, L_max, n_forms;
+  double diag[DWBA_MAX_L + 1];
+};
+
+// ---- PTX wrappers --------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait (about a second of SM clocks); returns false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+  const long long t0 = clock64();
+  while (true) {
+    if (mbar_try_wait(bar, phase)) return true;
+    if (clock64() - t0 > WAIT_CYCLES) return false;
+  }
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+// SMEM matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr & 0x3FFFF) >> 4);           // start address
+  d |= (uint64_t)1 << 16;                            // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;                  // stride byte offset
+  d |= (uint64_t)1 << 46;                            // descriptor version (sm100)
+  d |= (uint64_t)2 << 61;                            // SWIZZLE_128B
+  return d;
+}
+// Instruction descriptor, kind::f16: D f32, A/B bf16, both K-major, M = 128, N = bn.
+__host__ __device__ constexpr uint32_t instr_desc(int bn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int c = 0; c < 32; ++c) v[c] = __uint_as_float(r[c]);
+}
+
+// byte offset of element (row, k) in a K-major, 128-byte-swizzled tile with 64 bf16 per row
+__device__ __forceinline__ uint32_t sw128_offset(int row, int chunk16) {
+  return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((chunk16 ^ (row & 7)) << 4));
+}
+
+// Round-to-nearest-even to bfloat16 on the FP32 bit pattern (integer pipes, no conversion
+// unit): returns the rounded value as an FP32 bit pattern with the low 16 bits clear.
+__device__ __forceinline__ uint32_t bf16_rne_bits(float x) {
+  const uint32_t b = __float_as_uint(x);
+  return (b + 0x7FFFu + ((b >> 16) & 1u)) & 0xFFFF0000u;
+}
+
+template <int NT>
+__device__ __forceinline__ void split_store(uint8_t* a_base, int row, int chunk, const float* k8) {
+  // NT terms: t_0 = bf16(x), t_1 = bf16(x - t_0), t_2 = bf16(x - t_0 - t_1); x - t_0 is exact in FP32
+  float rem[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) rem[e] = k8[e];
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {
+    uint32_t w[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const uint32_t b0 = bf16_rne_bits(rem[2 * e]);
+      const uint32_t b1 = bf16_rne_bits(rem[2 * e + 1]);
+      rem[2 * e] -= __uint_as_float(b0);
+      rem[2 * e + 1] -= __uint_as_float(b1);
+      w[e] = (b0 >> 16) | b1;  // element 2e in the low half, 2e+1 in the high half
+    }
+    uint32_t addr = smem_u32(a_base + t * (BM * BK * 2) + sw128_offset(row, chunk));
+    asm volatile("st.shared.v4.b32 [%0], {%1,%2,%3,%4};" ::"r"(addr), "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3])
+                 : "memory");
+  }
+}
+
+// Far-to-near order of the j blocks of one row block: the blocks below and above the diagonal
+// merged by decreasing distance (ties: below first), then the blocks that touch the diagonal.
+struct BlockOrder {
+  int lo, hi, nd, kd0, kd1;
+  __device__ BlockOrder(int n_kb, int i0) : lo(0), hi(n_kb - 1), nd(i0 / BK), kd0(i0 / BK) {
+    kd1 = min(kd0 + BM / BK, n_kb);
+  }
+  __device__ int next() {
+    const int dl = lo < kd0 ? kd0 - lo : -1;       // distance of the next block below
+    const int dh = hi >= kd1 ? hi - kd1 + 1 : -1;  // and above
+    if (dl < 0 && dh < 0) return nd++;
+    if (dl >= dh) return lo++;
+    return hi--;
+  }
+};
+
+// Two shared-memory stages. Per j block t: all threads write K_L(t) into stage t%2 and the
+// column factors of block t+1; thread 0 then issues the MMAs of block t, waits for those of
+// block t-1 and fetches the B tiles of block t+1 into the other stage, which leaves a whole
+// block of MMA time for the copy to land.
+template <int NT, int BN>
+__global__ void __launch_bounds__(THREADS, 1)
+tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P) {
+  constexpr int A_BYTES = BM * BK * 2;            // one term
+  constexpr int B_BYTES = BN * BK * 2;            // one term
+  constexpr int STAGE = NT * (A_BYTES + B_BYTES);
+  constexpr int NPROD = NT == 2 ? 3 : 6;
+  constexpr int S = 2;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  __shared__ uint64_t bar_full[S], bar_done[S];
+  __shared__ uint32_t tmem_base_s;
+  __shared__ float sUb[BM], sUa[BM], sV[2][BK];
+  __shared__ double sRi[BM], sRj[2][BK];
+  __shared__ double sRed[4][BN];
+  __shared__ int s_abort;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int iblk = blockIdx.x, fblk = blockIdx.y, L = blockIdx.z;
+  const int i0 = iblk * BM, f0 = fblk * BN;
+  const int n_kb = P.n_pad / BK;
+  // a CTA that timed out already: skip the work (nothing allocated yet)
+  if (*(volatile int*)P.status != 0) return;
+
+  if (tid == 0) {
+    for (int q = 0; q < S; ++q) {
+      mbar_init(&bar_full[q], 1);
+      mbar_init(&bar_done[q], 1);
+    }
+    s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                 "r"((uint32_t)BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  // rank-one factors are scaled by the row block's smallest (c_lo) and largest (c_hi) radius:
+  //   below: U_i = (r_i/c_lo)^-(L+1) / c_lo, V_j = (r_j/c_lo)^L
+  //   above: U_i = (r_i/c_hi)^L,            V_j = (r_j/c_hi)^-(L+1) / c_hi
+  // evaluated as exp2 of FP64 differences of log2 r (no pow, no division)
+  const double lg_lo = P.lg[i0];
+  const double lg_hi = P.lg[min(i0 + BM, P.n_grid) - 1];
+  const double Lp1 = (double)(L + 1), Ld = (double)L;
+  for (int m = tid; m < BM; m += THREADS) {
+    const bool in = i0 + m < P.n_grid;
+    const double ri = in ? P.r[i0 + m] : 0.0;
+    const double li = in ? P.lg[i0 + m] : 0.0;
+    sRi[m] = ri;
+    sUb[m] = in ? (float)exp2(-Lp1 * (li - lg_lo) - lg_lo) : 0.0f;
+    sUa[m] = in ? (float)exp2(Ld * (li - lg_hi)) : 0.0f;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_s;
+  const uint32_t idesc = instr_desc(BN);
+
+  // barrier bookkeeping (thread 0 only)
+  uint32_t phase_full[S], phase_done[S];
+  bool full_pending[S], done_pending[S];
+#pragma unroll
+  for (int q = 0; q < S; ++q) {
+    phase_full[q] = phase_done[q] = 0;
+    full_pending[q] = done_pending[q] = false;
+  }
+  bool ok = true;
+
+  auto issue_tma = [&](int st_idx, int kb_t) {
+    uint8_t* b_dst = smem + st_idx * STAGE + NT * A_BYTES;
+    mbar_expect_tx(&bar_full[st_idx], NT * B_BYTES);
+#pragma unroll
+    for (int t = 0; t < NT; ++t) tma_load_2d(b_dst + t * B_BYTES, &bmap, &bar_full[st_idx], kb_t * BK, t * P.f_pad + f0);
+    full_pending[st_idx] = true;
+  };
+  auto kind_of = [&](int kb_t) {  // 0: below the diagonal, 1: above, 2: touches it
+    const int j0 = kb_t * BK;
+    return (j0 + BK - 1 < i0) ? 0 : ((j0 > i0 + BM - 1) ? 1 : 2);
+  };
+  // column radii and rank-one column factors of block kb_t (threads < BK)
+  auto column_factors = [&](int buf, int kb_t, double rj, double lj) {
+    const int kind = kind_of(kb_t);
+    const bool in = kb_t * BK + tid < P.n_grid;
+    sRj[buf][tid] = rj;
+    double v = 0.0;
+    if (in && kind != 2) v = kind == 0 ? exp2(Ld * (lj - lg_lo)) : exp2(-Lp1 * (lj - lg_hi) - lg_hi);
+    sV[buf][tid] = (float)v;
+  };
+
+  // visit the j blocks from the farthest to the nearest to this row block, so the FP32
+  // accumulator is still small while the many small far-field products are added
+  BlockOrder order(n_kb, i0);
+  int kb = order.next();
+  if (tid == 0) issue_tma(0, kb);
+  if (tid < BK) {
+    const int j = kb * BK + tid;
+    const bool in = j < P.n_grid;
+    column_factors(0, kb, in ? P.r[j] : 0.0, in ? P.lg[j] : 0.0);
+  }
+  __syncthreads();
+
+  for (int step = 0; step < n_kb; ++step) {
+    const int s = step & 1;
+    uint8_t* a_st = smem + s * STAGE;
+    uint8_t* b_st = a_st + NT * A_BYTES;
+    const int kb_next = step + 1 < n_kb ? order.next() : -1;
+    // start the loads of the next block's column data early
+    double rj_n = 0.0, lj_n = 0.0;
+    if (tid < BK && kb_next >= 0) {
+      const int j = kb_next * BK + tid;
+      if (j < P.n_grid) {
+        rj_n = P.r[j];
+        lj_n = P.lg[j];
+      }
+    }
+    // K_L tile in registers -> swizzled shared memory (stage s is free: MMAs of step-2 are done)
+    const int j0 = kb * BK;
+    const int kind = kind_of(kb);
+    {
+      // a warp covers 32 consecutive rows of one column half: the sV reads are broadcasts
+      const int row = tid & (BM - 1);
+      const int kh = (tid >> 7) * 32;
+      const int i = i0 + row;
+      const float u = kind == 0 ? sUb[row] : sUa[row];
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        float k8[8];
+        const int kk0 = kh + 8 * g;
+        if (kind != 2) {
+#pragma unroll
+          for (int e = 0; e < 8; ++e) k8[e] = u * sV[s][kk0 + e];
+        } else {
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const int j = j0 + kk0 + e;
+            double kv = 0.0;
+            if (i < P.n_grid && j < P.n_grid) {
+              const double ri = sRi[row], rj = sRj[s][kk0 + e];
+              if (i == j) {
+                kv = P.diag[L] / ri;
+              } else {
+                const double rl = fmin(ri, rj), rg = fmax(ri, rj);
+                const double inv = 1.0 / rg;
+                double ratio = rl * inv, pw = 1.0;
+                for (int e2 = L; e2 > 0; e2 >>= 1) {
+                  if (e2 & 1) pw *= ratio;
+                  ratio *= ratio;
+                }
+                kv = inv * pw;
+              }
+            }
+            k8[e] = (float)kv;
+          }
+        }
+        split_store<NT>(a_st, row, kk0 >> 3, k8);
+      }
+    }
+    // column data of the next block into the other buffer
+    if (tid < BK && kb_next >= 0) column_factors(s ^ 1, kb_next, rj_n, lj_n);
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      bool good = *(volatile int*)P.status == 0 && mbar_wait(&bar_full[s], phase_full[s]);
+      if (good) {
+        full_pending[s] = false;
+        phase_full[s] ^= 1;
+        tc_fence_after();
+        const uint32_t a0 = smem_u32(a_st), b0 = smem_u32(b_st);
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk) {
+#pragma unroll
+          for (int q = 0; q < NPROD; ++q) {
+            // (a term, b term) of product q, total order <= NT-1:
+            // NT=2: (0,0) (0,1) (1,0); NT=3: (0,0) (0,1) (1,0) (0,2) (1,1) (2,0)
+            const int ta = (q == 2 || q == 4) ? 1 : (q == 5 ? 2 : 0);
+            const int tb = (q == 1 || q == 4) ? 1 : (q == 3 ? 2 : 0);
+            const uint64_t ad = smem_desc(a0 + ta * A_BYTES + kk * 32);
+            const uint64_t bd = smem_desc(b0 + tb * B_BYTES + kk * 32);
+            mma_bf16(tmem, ad, bd, idesc, (step > 0 || kk > 0 || q > 0) ? 1u : 0u);
+          }
+        }
+        mma_commit(&bar_done[s]);
+        done_pending[s] = true;
+        // the other stage is free once the MMAs of the previous block completed
+        if (done_pending[s ^ 1]) {
+          good = mbar_wait(&bar_done[s ^ 1], phase_done[s ^ 1]);
+          phase_done[s ^ 1] ^= 1;
+          done_pending[s ^ 1] = false;
+        }
+        if (good && kb_next >= 0) issue_tma(s ^ 1, kb_next);
+      }
+      if (!good) s_abort = 1;
+    }
+    if (__syncthreads_or(s_abort)) { ok = false; break; }
+    kb = kb_next;
+  }
+  // drain (thread 0): every commit still outstanding and any copy in flight, bounded
+  if (tid == 0) {
+    for (int q = 0; q < S; ++q) {
+      if (done_pending[q] && !mbar_wait(&bar_done[q], phase_done[q])) s_abort = 1;
+      if (full_pending[q]) mbar_wait(&bar_full[q], phase_full[q]);
+    }
+    if (s_abort) ok = false;
+  }
+  if (__syncthreads_or(!ok)) ok = false;
+  if (!ok && tid == 0) atomicExch(P.status, 2);
+  tc_fence_after();
+  if (ok) {
+    // epilogue: warps w and w+4 share TMEM lanes 32*(w%4).., each takes half the columns
+    const int g = warp & 3, h = warp >> 2;
+    const int row = 32 * g + lane;
+    const int i = i0 + row;
+    for (int c0 = h * (BN / 2); c0 < (h + 1) * (BN / 2); c0 += 32) {
+      float z[32];
+      tmem_ld32(tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)c0, z);
+#pragma unroll
+      for (int c = 0; c < 32; ++c) {
+        // a_f[i] of column f: the lanes of a warp read 32 consecutive rows of one form
+        const int f = f0 + c0 + c;
+        double av = 0.0;
+        if (f < P.n_forms) {
+          const dwba_form_t F = P.forms[f];
+          if (i < F.n_rows) av = ldexp(F.a_dev[i], P.bexp[f]);
+        }
+        double v = av * (double)z[c];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) sRed[g][c0 + c] = v;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (ok) {
+    for (int c = tid; c < BN; c += THREADS) {
+      const double v = sRed[0][c] + sRed[1][c] + sRed[2][c] + sRed[3][c];
+      P.partial[((int64_t)L * P.n_iblk + iblk) * P.f_pad + f0 + c] = v;
+    }
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN));
+  }
+}
+
+// ---- operand preparation and reduction -----------------------------------------------
+// Per-form exponent e_f with 2^-e_f max|b_f| in [0.5, 1): the split then works at unit scale
+// whatever the magnitude of b_f (power-of-two scaling is exact).
+__global__ void tc_scale_kernel(const dwba_form_t* __restrict__ forms, int n_forms, int* __restrict__ bexp) {
+  __shared__ double red[8];
+  const int f = blockIdx.x;
+  const dwba_form_t F = forms[f];
+  double m = 0.0;
+  for (int j = threadIdx.x; j < F.n_cols; j += blockDim.x) m = fmax(m, fabs(F.b_dev[j]));
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mm = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) mm = fmax(mm, red[w]);
+    int e = 0;
+    if (mm > 0.0 && isfinite(mm)) frexp(mm, &e);
+    bexp[f] = e;
+  }
+}
+
+// b_f -> NT bf16 terms in [NT][f_pad][n_pad] (zero padded): t_0 = bf16(b'), t_1 = bf16(b' - t_0), ...,
+// b' = 2^-e_f b_f
+template <int NT>
+__global__ void tc_prepare_kernel(const dwba_form_t* __restrict__ forms, int n_forms, int n_pad, int f_pad,
+                                  const int* __restrict__ bexp, __nv_bfloat16* __restrict__ bterms) {
+  const int64_t total = (int64_t)f_pad * n_pad;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+    const int f = (int)(idx / n_pad), j = (int)(idx - (int64_t)f * n_pad);
+    double b = 0.0;
+    if (f < n_forms) {
+      const dwba_form_t F = forms[f];
+      if (j < F.n_cols) b = ldexp(F.b_dev[j], -bexp[f]);
+    }
+    float rem = (float)b;
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const __nv_bfloat16 q = __float2bfloat16_rn(rem);
+      rem -= __bfloat162float(q);
+      bterms[((int64_t)t * f_pad + f) * n_pad + j] = q;
+    }
+  }
+}
+
+__global__ void tc_log2_kernel(const double* __restrict__ r, int n, double* __restrict__ lg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) lg[i] = log2(r[i]);
+}
+
+__global__ void tc_reduce_kernel(const double* __restrict__ partial, int n_forms, int f_pad, int n_iblk, int n_L,
+                                 double* __restrict__ out) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n_forms * n_L) return;
+  const int f = (int)(idx / n_L), L = (int)(idx - (int64_t)f * n_L);
+  double s = 0.0;
+  for (int b = 0; b < n_iblk; ++b) s += partial[((int64_t)L * n_iblk + b) * f_pad + f];
+  out[idx] = s;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+template <int NT, int BN>
+int launch_tc(const GemmParams& P, const __nv_bfloat16* bterms, int n_L, cudaStream_t st) {
+  auto encode = get_encode();
+  if (!encode) return DWBA_ERR_CUDA;
+  CUtensorMap map;
+  cuuint64_t dims[2] = {(cuuint64_t)P.n_pad, (cuuint64_t)NT * (cuuint64_t)P.f_pad};
+  cuuint64_t strides[1] = {(cuuint64_t)P.n_pad * 2};
+  cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BN};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult cr = encode(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)bterms, dims, strides, box, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (cr != CUDA_SUCCESS) return DWBA_ERR_CUDA;
+  const int smem = 2 * NT * (BM * BK * 2 + BN * BK * 2) + 1024;
+  if (cudaFuncSetAttribute(tc_exchange_kernel<NT, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+      cudaSuccess)
+    return DWBA_ERR_CUDA;
+  dim3 grid(P.n_iblk, P.f_pad / BN, n_L);
+  tc_exchange_kernel<NT, BN><<<grid, THREADS, smem, st>>>(map, P);
+  DWBA_CHECK_LAUNCH();
+  return DWBA_OK;
+}
+
+}  // namespace
+
+extern "C" int64_t dwba_tc_workspace_bytes(int n_forms, int n_grid, int L_max, int n_terms) {
+  if (n_forms < 0 || n_grid < 2 || L_max < 0 || L_max > DWBA_MAX_L || (n_terms != 2 && n_terms != 3)) return -1;
+  const int bn = n_terms == 2 ? TC_BN2 : 128;
+  const int64_t n_pad = ((int64_t)n_grid + BK - 1) / BK * BK;
+  const int64_t f_pad = ((int64_t)n_forms + bn - 1) / bn * bn;
+  const int64_t n_iblk = ((int64_t)n_grid + BM - 1) / BM;
+  const int64_t b = (int64_t)n_terms * f_pad * n_pad * 2;
+  const int64_t p = (int64_t)(L_max + 1) * n_iblk * f_pad * 8;
+  const int64_t e = f_pad * 4;
+  const int64_t lgb = n_pad * 8;
+  return ((b + 255) / 256 * 256) + ((p + 255) / 256 * 256) + ((e + 255) / 256 * 256) + lgb;
+}
+
+extern "C" int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, const double* r_dev, int n_grid,
+                                     int L_max, int n_terms, const double* diag_scale_host, void* workspace,
+                                     int64_t workspace_bytes, int* status_dev, double* out_dev,
+                                     dwba_stream_t stream) {
+  if (n_forms <= 0) return DWBA_OK;
+  if (!forms_dev || !r_dev || !diag_scale_host || !workspace || !status_dev || !out_dev || n_grid < 2 || L_max < 0 ||
+      L_max > DWBA_MAX_L || (n_terms != 2 && n_terms != 3) || n_grid > (1 << 24))
+    return DWBA_ERR_INVALID_ARG;
+  const int64_t need = dwba_tc_workspace_bytes(n_forms, n_grid, L_max, n_terms);
+  if (need < 0 || workspace_bytes < need) return DWBA_ERR_WORKSPACE;
+  if (((uintptr_t)workspace & 255) != 0) return DWBA_ERR_INVALID_ARG;
+  const int bn = n_terms == 2 ? TC_BN2 : 128;
+  GemmParams P;
+  P.n_grid = n_grid;
+  P.n_pad = (n_grid + BK - 1) / BK * BK;
+  P.f_pad = (n_forms + bn - 1) / bn * bn;
+  P.n_iblk = (n_grid + BM - 1) / BM;
+  P.L_max = L_max;
+  P.r = r_dev;
+  P.forms = forms_dev;
+  P.n_forms = n_forms;
+  P.status = status_dev;
+  for (int l = 0; l <= DWBA_MAX_L; ++l) P.diag[l] = l <= L_max ? diag_scale_host[l] : 0.0;
+  uint8_t* ws = (uint8_t*)workspace;
+  const int64_t bbytes = (int64_t)n_terms * P.f_pad * P.n_pad * 2;
+  __nv_bfloat16* bterms = (__nv_bfloat16*)ws;
+  P.partial = (double*)(ws + (bbytes + 255) / 256 * 256);
+  const int64_t pbytes = (int64_t)(L_max + 1) * P.n_iblk * P.f_pad * 8;
+  int* bexp = (int*)((uint8_t*)P.partial + (pbytes + 255) / 256 * 256);
+  P.bexp = bexp;
+  double* lg = (double*)((uint8_t*)bexp + ((int64_t)P.f_pad * 4 + 255) / 256 * 256);
+  P.lg = lg;
+  if (P.f_pad / bn > 65535) return DWBA_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t total = (int64_t)P.f_pad * P.n_pad;
+  tc_scale_kernel<<<n_forms, 256, 0, st>>>(forms_dev, n_forms, bexp);
+  DWBA_CHECK_LAUNCH();
+  tc_log2_kernel<<<dwba_grid_1d(n_grid, 256), 256, 0, st>>>(r_dev, n_grid, lg);
+  DWBA_CHECK_LAUNCH();
+  if (n_terms == 2)
+    tc_prepare_kernel<2><<<dwba_grid_1d(total, 256, 65535), 256, 0, st>>>(forms_dev, n_forms, P.n_pad, P.f_pad,
+                                                                          bexp, bterms);
+  else
+    tc_prepare_kernel<3><<<dwba_grid_1d(total, 256, 65535), 256, 0, st>>>(forms_dev, n_forms, P.n_pad, P.f_pad,
+                                                                          bexp, bterms);
+  DWBA_CHECK_LAUNCH();
+  const int n_L = L_max + 1;
+  int rc = n_terms == 2 ? launch_tc<2, TC_BN2>(P, bterms, n_L, st) : launch_tc<3, 128>(P, bterms, n_L, st);
+  if (rc != DWBA_OK) return rc;
+  tc_reduce_kernel<<<dwba_grid_1d((int64_t)n_forms * n_L, 256), 256, 0, st>>>(P.partial, n_forms, P.f_pad,
+                                                                            P.n_iblk, n_L, out_dev);
+  DWBA_CHECK_LAUNCH();
+  return DWBA_OK;
+}

@@ -62,8 +62,8 @@ def check_cupy_runtime() -> bool:
 
 def _engine_name(engine: Optional[str]) -> str:
     e = engine or os.environ.get("DWBA_B200_ENGINE", "dense")
-    if e not in ("dense", "semisep"):
-        raise ValueError(f"unknown engine {e!r} (dense | semisep)")
+    if e not in ("dense", "semisep", "tc_bf16x3", "tc_bf16x6"):
+        raise ValueError(f"unknown engine {e!r} (dense | semisep | tc_bf16x3 | tc_bf16x6)")
     return e
 
 
@@ -148,7 +148,8 @@ class _WaveView:
 
 
 def _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, cache):
-    from .engine import Job
+    """Job for one or several transitions: bound_i/bound_f are single objects or equal-length sequences."""
+    from .engine import Job, Transition
     from .plan import is_excitation
     if L_max < 0:
         raise ValueError("radial_ME_all_L: L_max must be >= 0.")
@@ -156,8 +157,12 @@ def _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f
     V = _fit(V_core_array, N, "V_core")
     Ui = _fit(U_i_array, N, "U_i")
     Uf = _fit(U_f_array, N, "U_f") if U_f_array is not None else None
-    u_i = _fit(bound_i.u_of_r, N, "Bound state u_i")
-    u_f = _fit(bound_f.u_of_r, N, "u_f")
+    bis = list(bound_i) if isinstance(bound_i, (list, tuple)) else [bound_i]
+    bfs = list(bound_f) if isinstance(bound_f, (list, tuple)) else [bound_f]
+    if len(bis) != len(bfs):
+        raise ValueError("bound_i and bound_f must have the same number of transitions")
+    trans = [Transition(u_i=_fit(bi.u_of_r, N, "Bound state u_i"), u_f=_fit(bf.u_of_r, N, "u_f"),
+                        excitation=is_excitation(bf)) for bi, bf in zip(bis, bfs)]
     wp = []
     cache_w: Dict[int, _WaveView] = {}
     for ci, cf in pairs:
@@ -167,8 +172,8 @@ def _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f
     meth = kw.get("oscillatory_method", "advanced")
     if meth not in ("legacy", "advanced", "full_split"):
         meth = "advanced"  # the reference treats any other value as "advanced" (dwba_matrix_elements.py:1183)
-    return Job(grid=cache.info, V_core=V, U_i=Ui, U_f=Uf, u_i=u_i, u_f=u_f, excitation=is_excitation(bound_f),
-               pairs=wp, L_max=int(L_max), use_oscillatory_quadrature=bool(kw.get("use_oscillatory_quadrature", True)),
+    return Job(grid=cache.info, V_core=V, U_i=Ui, U_f=Uf, transitions=trans, pairs=wp, L_max=int(L_max),
+               use_oscillatory_quadrature=bool(kw.get("use_oscillatory_quadrature", True)),
                oscillatory_method=meth, CC_nodes=int(kw.get("CC_nodes", 5)),
                phase_increment=float(kw.get("phase_increment", 1.5708)),
                min_grid_fraction=float(kw.get("min_grid_fraction", 0.10)),
@@ -176,6 +181,7 @@ def _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f
 
 
 def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, gpu_cache, engine):
+    """Evaluate a job; returns results[t][p] (a list of RadialDWBAIntegrals per transition)."""
     if not HAS_CUPY:
         raise RuntimeError("dwba_b200 engine library is not available (build it with python -m dwba_b200.build)")
     import torch
@@ -186,9 +192,9 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
     job = _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, cache)
     with torch.cuda.device(cache.device):
         I_dir, I_exc = run_job(job, cache.dg, engine=_engine_name(engine))
-    return [RadialDWBAIntegrals(I_L_direct={L: float(I_dir[p, L]) for L in range(L_max + 1)},
-                                I_L_exchange={L: float(I_exc[p, L]) for L in range(L_max + 1)})
-            for p in range(len(pairs))]
+    return [[RadialDWBAIntegrals(I_L_direct={L: float(I_dir[t, p, L]) for L in range(L_max + 1)},
+                                 I_L_exchange={L: float(I_exc[t, p, L]) for L in range(L_max + 1)})
+             for p in range(len(pairs))] for t in range(I_dir.shape[0])]
 
 
 def radial_ME_all_L(grid, V_core_array, U_i_array, bound_i, bound_f, cont_i, cont_f, L_max: int,
@@ -201,7 +207,7 @@ def radial_ME_all_L(grid, V_core_array, U_i_array, bound_i, bound_f, cont_i, con
               CC_nodes=CC_nodes, phase_increment=phase_increment, min_grid_fraction=min_grid_fraction,
               k_threshold=k_threshold)
     return _run(grid, V_core_array, U_i_array, bound_i, bound_f, [(cont_i, cont_f)], L_max, U_f_array, kw, None,
-                engine)[0]
+                engine)[0][0]
 
 
 def radial_ME_all_L_gpu(grid, V_core_array, U_i_array, bound_i, bound_f, cont_i, cont_f, L_max: int,
@@ -217,7 +223,7 @@ def radial_ME_all_L_gpu(grid, V_core_array, U_i_array, bound_i, bound_f, cont_i,
               CC_nodes=CC_nodes, phase_increment=phase_increment, min_grid_fraction=min_grid_fraction,
               k_threshold=k_threshold)
     return _run(grid, V_core_array, U_i_array, bound_i, bound_f, [(cont_i, cont_f)], L_max, U_f_array, kw,
-                gpu_cache, engine)[0]
+                gpu_cache, engine)[0][0]
 
 
 def radial_ME_all_L_batch(grid, V_core_array, U_i_array, bound_i, bound_f,
@@ -227,11 +233,16 @@ def radial_ME_all_L_batch(grid, V_core_array, U_i_array, bound_i, bound_f,
                           k_threshold: float = 0.5, U_f_array: Optional[np.ndarray] = None,
                           gpu_cache: Optional[GPUCache] = None,
                           engine: Optional[str] = None) -> List[RadialDWBAIntegrals]:
-    """Batched entry point (new): one result per (cont_i, cont_f) pair, same values as calling
-    ``radial_ME_all_L`` per pair; all pairs share one grid, potentials and bound transition."""
+    """Batched entry point (new): the same values as calling ``radial_ME_all_L`` per pair.
+
+    All pairs share one grid and the potentials. With single ``bound_i``/``bound_f`` objects the
+    result is one ``RadialDWBAIntegrals`` per pair; with equal-length sequences of them (several
+    transitions, e.g. one per ejected wave in ionization) it is a list per transition."""
     kw = dict(use_oscillatory_quadrature=use_oscillatory_quadrature, oscillatory_method=oscillatory_method,
               CC_nodes=CC_nodes, phase_increment=phase_increment, min_grid_fraction=min_grid_fraction,
               k_threshold=k_threshold)
+    multi = isinstance(bound_i, (list, tuple))
     if len(pairs) == 0:
-        return []
-    return _run(grid, V_core_array, U_i_array, bound_i, bound_f, list(pairs), L_max, U_f_array, kw, gpu_cache, engine)
+        return [[] for _ in bound_i] if multi else []
+    res = _run(grid, V_core_array, U_i_array, bound_i, bound_f, list(pairs), L_max, U_f_array, kw, gpu_cache, engine)
+    return res if multi else res[0]

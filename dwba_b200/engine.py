@@ -21,7 +21,8 @@ from . import _lib
 from .plan import (GridInfo, NodeSetKey, NodeSetPlan, OVERLAP_TOL, adaptive_dphi, cc_reference, diag_scale,
                    idx_limit, is_excitation, multipole_moments, plan_nodeset, safe_float, tail_limits)
 
-ENGINES = ("dense", "semisep")
+ENGINES = ("dense", "semisep", "tc_bf16x3", "tc_bf16x6")
+TC_TERMS = {"tc_bf16x3": 2, "tc_bf16x6": 3}
 
 
 def _ptr(t: Optional[torch.Tensor]) -> int:
@@ -132,15 +133,26 @@ class PairPlan:
 
 
 @dataclass
+class Transition:
+    """One (bound_i, bound_f) pair: u_f is a bound orbital (excitation) or an ejected wave (ionization)."""
+    u_i: np.ndarray
+    u_f: np.ndarray
+    excitation: bool
+
+
+@dataclass
 class Job:
-    """One energy point: shared grid/potentials/transition, many continuum pairs."""
+    """Work sharing one grid and potentials: every transition with every (cont_i, cont_f) pair.
+
+    One energy point of the reference's excitation driver is one transition with all its
+    (l_i, l_f) pairs (``driver.py:907-1029``); one ejected energy of its ionization loop is a
+    set of transitions (one per ejected wave) (``ionization.py:526-608``).
+    """
     grid: GridInfo
     V_core: np.ndarray
     U_i: np.ndarray
     U_f: Optional[np.ndarray]
-    u_i: np.ndarray
-    u_f: np.ndarray
-    excitation: bool
+    transitions: List[Transition]
     pairs: List[Tuple[object, object]]
     L_max: int
     use_oscillatory_quadrature: bool = True
@@ -151,86 +163,246 @@ class Job:
     k_threshold: float = 0.5
 
 
-def plan_job(job: Job) -> List[PairPlan]:
-    """Host planning of every pair (integration limit, branch, node set, L=0 corrections, tails)."""
+def _pair_arrays(pairs):
+    def col(get):
+        return np.array([get(c) for c in pairs])
+    return dict(
+        k_i=col(lambda p: float(p[0].k_au)), k_f=col(lambda p: float(p[1].k_au)),
+        l_i=col(lambda p: int(p[0].l)), l_f=col(lambda p: int(p[1].l)),
+        im_i=col(lambda p: int(getattr(p[0], "idx_match", -1))), im_f=col(lambda p: int(getattr(p[1], "idx_match", -1))),
+        e_i=col(lambda p: float(getattr(p[0], "eta", 0.0))), e_f=col(lambda p: float(getattr(p[1], "eta", 0.0))),
+        d_i=col(lambda p: float(getattr(p[0], "phase_shift", 0.0))),
+        d_f=col(lambda p: float(getattr(p[1], "phase_shift", 0.0))),
+        s_i=col(lambda p: float(getattr(p[0], "sigma_l", 0.0))), s_f=col(lambda p: float(getattr(p[1], "sigma_l", 0.0))))
+
+
+def _idx_limits(job: Job, pa, t: Transition) -> np.ndarray:
+    """Vectorised ``idx_limit`` (dwba_matrix_elements.py:909-1022) for every pair of one transition."""
     g = job.grid
-    N = g.N
-    r, w = g.r, g.w
-    V_diff = job.V_core - job.U_i
-    moments = None
-    max_seg, max_dphi = tail_limits()
-    plans = []
-    for ci, cf in job.pairs:
-        k_i, k_f, l_i, l_f = float(ci.k_au), float(cf.k_au), int(ci.l), int(cf.l)
-        n1 = idx_limit(g, job.U_i, job.U_f, job.u_i, job.u_f, k_i, k_f, l_i, l_f,
-                       int(getattr(ci, "idx_match", -1)), int(getattr(cf, "idx_match", -1)), job.min_grid_fraction)
-        e_i, e_f = float(getattr(ci, "eta", 0.0)), float(getattr(cf, "eta", 0.0))
-        k_total, eta_total = k_i + k_f, e_i + e_f
-        osc = bool(job.use_oscillatory_quadrature and k_total > job.k_threshold)
-        ns = None
-        if osc and n1 >= 2:
-            d = adaptive_dphi(g, n1, k_total, job.phase_increment, eta_total)
-            ns = plan_nodeset(g, NodeSetKey(id(g), n1, k_total, d, eta_total, int(job.CC_nodes)))
-        pp = PairPlan(n1=n1, osc=osc, nodeset=ns)
-        # L=0 corrections with the limited Simpson weights (dwba_matrix_elements.py:1028-1046, :1249-1296)
-        wl = w.copy()
-        wl[n1:] = 0.0
-        chi_i, chi_f = ci.chi_of_r[:N], cf.chi_of_r[:N]
-        s2 = np.sum(wl * job.u_f * job.u_i)
-        if abs(s2) > OVERLAP_TOL:
-            pp.corr_dir = float(np.dot(wl * chi_f * chi_i, V_diff) * s2)
-        s2e = np.sum(wl * chi_f * job.u_i)
-        if abs(s2e) > OVERLAP_TOL:
-            pp.corr_ex = float(np.dot(wl * job.u_f * chi_i, V_diff) * s2e)
-        # outer tails of the direct term (dwba_matrix_elements.py:1213-1241 advanced/full_split; :1256-1267 legacy)
-        legacy = job.oscillatory_method == "legacy"
-        want = job.L_max >= 1 and n1 < N - 10 and job.excitation and (
-            (legacy and job.use_oscillatory_quadrature) or (not legacy and osc))
-        if want:
-            if moments is None:
-                moments = multipole_moments(g, job.u_i, job.u_f, job.L_max)
-            wave = [k_i, l_i, float(getattr(ci, "phase_shift", 0.0)), e_i, float(getattr(ci, "sigma_l", 0.0)),
-                    k_f, l_f, float(getattr(cf, "phase_shift", 0.0)), e_f, float(getattr(cf, "sigma_l", 0.0))]
-            pp.tail = _lib.outer_tails(wave, float(r[n1 - 1]), float(r[-1]), job.L_max, moments, 1 if legacy else 0,
-                                       max_seg, max_dphi)
-        plans.append(pp)
-    return plans
+    N, r = g.N, g.r
+    n1 = np.full(len(pa["k_i"]), N, dtype=np.int64)
+    for im in (pa["im_i"], pa["im_f"]):
+        m = (im > 0) & (im < N)
+        n1 = np.where(m, np.minimum(n1, im + 1), n1)
+    kmin = np.minimum(pa["k_i"], pa["k_f"])
+    kmax = np.maximum(pa["k_i"], pa["k_f"])
+    k_eff = np.where(kmin > 0.1, kmin, kmax)
+    lmax = np.maximum(pa["l_i"], pa["l_f"])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r_turn = (lmax + 0.5) / k_eff
+    idx_turn = np.minimum(np.searchsorted(r, np.where(k_eff > 1e-3, r_turn, 0.0)), N - 20)
+    mgf = int(N * job.min_grid_fraction)
+    min_idx = np.where(k_eff > 1e-3, np.minimum(np.maximum(idx_turn + 20, mgf), N), max(1, mgf))
+    n1 = np.where(n1 < min_idx, min_idx, n1)
+    idx99 = max(0, g.extent99(t.u_i), g.extent99(t.u_f))
+    n1 = np.where(idx99 > n1, idx99 + 1, n1)
+    ke = 0.5 * kmin ** 2
+    uabs = np.abs(job.U_i) if job.U_f is None else np.maximum(np.abs(job.U_i), np.abs(job.U_f))
+    cent = lmax * (lmax + 1)
+    i0 = np.maximum(0, n1 - 1)
+    veff0 = uabs[i0] + cent / (2.0 * r[i0] ** 2)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        sel = np.nonzero((ke > 1e-10) & (veff0 / ke > 0.03))[0]
+    if len(sel):
+        T = n1[sel, None] + np.arange(500)[None, :]
+        valid = T < N
+        Tc = np.minimum(T, N - 1)
+        veff = uabs[Tc] + cent[sel, None] / (2.0 * r[Tc] ** 2)
+        ok = valid & (veff / ke[sel, None] < 0.03)
+        has = ok.any(axis=1)
+        first = np.argmax(ok, axis=1)
+        n1[sel] = np.where(has, T[np.arange(len(sel)), first] + 1, n1[sel])
+    return n1
 
 
-class _Pool:
-    """Device copies of the distinct 1-D functions of a job (dedup by host buffer)."""
+def _dphis(job: Job, n1: np.ndarray, k_total: np.ndarray, eta_total: np.ndarray) -> np.ndarray:
+    """Vectorised adaptive phase step (oscillatory_integrals.py:1716-1755, :1456-1509)."""
+    g = job.grid
+    d0 = min(max(np.pi / 16, float(job.phase_increment)), np.pi / 4)
+    mx = np.zeros(len(n1))
+    neutral = np.abs(eta_total) <= 1e-10
+    idx = np.maximum(n1 - 2, 0)
+    mx[neutral] = np.abs(k_total[neutral] * g.dr_prefix_max[idx[neutral]])
+    if (~neutral).any():
+        rm = np.maximum(0.5 * (g.r[:-1] + g.r[1:]), 1e-10)
+        for key in set(zip(k_total[~neutral].tolist(), eta_total[~neutral].tolist())):
+            sel = (~neutral) & (k_total == key[0]) & (eta_total == key[1])
+            cm = np.maximum.accumulate(np.abs((key[0] + key[1] / rm) * g.dr))
+            mx[sel] = cm[idx[sel]]
+    d = np.full(len(n1), d0)
+    under = (mx > np.pi / 4) & (k_total >= 1e-10) & (n1 >= 2)
+    scale = np.pi / 4 / np.maximum(mx, 1e-12)
+    d_eff = d0 * np.maximum(0.25, np.minimum(1.0, scale))
+    d = np.where(under, np.clip(d_eff, np.pi / 16, np.pi / 4), d)
+    return d
 
-    def __init__(self, device, N):
-        self.device = device
+
+class WaveMatrix:
+    """Distinct 1-D functions of a job as rows of one host matrix (dedup by host buffer)."""
+
+    def __init__(self, N):
         self.N = N
-        self.idx: Dict[int, int] = {}
-        self.host: List[np.ndarray] = []
+        self.idx: Dict[Tuple[int, int], int] = {}
+        self.arrays: List[np.ndarray] = []
 
     def add(self, arr: np.ndarray) -> int:
-        a = np.ascontiguousarray(arr[: self.N], dtype=np.float64)
-        key = arr.__array_interface__["data"][0]
+        a = np.asarray(arr)
+        key = (a.__array_interface__["data"][0], a.strides[0] if a.ndim else 0)
         i = self.idx.get(key)
         if i is None:
-            i = len(self.host)
+            i = len(self.arrays)
             self.idx[key] = i
-            self.host.append(a)
+            self.arrays.append(a[: self.N])
         return i
 
-    def upload(self) -> torch.Tensor:
-        stacked = np.stack(self.host) if self.host else np.zeros((1, self.N))
-        pinned = torch.from_numpy(stacked).pin_memory()
-        return pinned.to(self.device, non_blocking=True)
+    def matrix(self) -> np.ndarray:
+        if not hasattr(self, "_m"):
+            self._m = np.stack([np.asarray(a, dtype=np.float64) for a in self.arrays]) if self.arrays \
+                else np.zeros((1, self.N))
+        return self._m
+
+    def upload(self, device) -> torch.Tensor:
+        """Copy every row to the device. Rows that are consecutive rows of one C-contiguous
+        host block are copied as one block (pinned when the caller's memory is pinned)."""
+        N = self.N
+        out = torch.empty((max(1, len(self.arrays)), N), dtype=torch.float64, device=device)
+        i = 0
+        n = len(self.arrays)
+        while i < n:
+            a = self.arrays[i]
+            p0 = a.__array_interface__["data"][0]
+            j = i + 1
+            ok = a.flags.c_contiguous and a.dtype == np.float64 and len(a) == N
+            while ok and j < n:
+                b = self.arrays[j]
+                if not (b.flags.c_contiguous and b.dtype == np.float64 and len(b) == N and
+                        b.__array_interface__["data"][0] == p0 + 8 * N * (j - i)):
+                    break
+                j += 1
+            if ok and j - i > 1 and a.base is not None:
+                block = np.lib.stride_tricks.as_strided(a, shape=(j - i, N), strides=(8 * N, 8))
+                src = torch.from_numpy(block)
+            else:
+                j = i + 1
+                src = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).reshape(1, N)
+            out[i:j].copy_(src, non_blocking=src.is_pinned())
+            i = j
+        return out
+
+
+@dataclass
+class JobPlan:
+    """Host plan of a job, as arrays over (transition, pair).
+
+    n1: integration limit; osc: oscillatory branch (per pair); ns_index: node set of the pair
+    (index into ``nodesets``, -1 when there is none); corr_dir/corr_ex: L=0 corrections;
+    tails: outer tails of the direct term, keyed by (t, p)."""
+    n1: np.ndarray
+    osc: np.ndarray
+    ns_index: np.ndarray
+    nodesets: List[NodeSetPlan]
+    corr_dir: np.ndarray
+    corr_ex: np.ndarray
+    tails: Dict[Tuple[int, int], np.ndarray]
+
+    def pair(self, t: int, p: int) -> PairPlan:
+        k = int(self.ns_index[t, p])
+        return PairPlan(n1=int(self.n1[t, p]), osc=bool(self.osc[p]), nodeset=self.nodesets[k] if k >= 0 else None,
+                        corr_dir=float(self.corr_dir[t, p]), corr_ex=float(self.corr_ex[t, p]),
+                        tail=self.tails.get((t, p)))
+
+
+def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
+    """Host planning (vectorised over pairs): integration limit, branch, node set, L=0
+    corrections and outer tails for every (transition, pair)."""
+    g = job.grid
+    N, r, w = g.N, g.r, g.w
+    P, T = len(job.pairs), len(job.transitions)
+    pa = _pair_arrays(job.pairs)
+    k_total = pa["k_i"] + pa["k_f"]
+    eta_total = pa["e_i"] + pa["e_f"]
+    osc = np.asarray(job.use_oscillatory_quadrature & (k_total > job.k_threshold), dtype=bool)
+    V_diff = job.V_core - job.U_i
+    v_live = bool(np.any(V_diff))
+    max_seg, max_dphi = tail_limits()
+    legacy = job.oscillatory_method == "legacy"
+    if waves is None:
+        waves = WaveMatrix(N)
+    wi_idx = np.array([waves.add(ci.chi_of_r) for ci, _ in job.pairs], dtype=np.int64)
+    wf_idx = np.array([waves.add(cf.chi_of_r) for _, cf in job.pairs], dtype=np.int64)
+    n1_all = np.zeros((T, P), dtype=np.int64)
+    ns_index = np.full((T, P), -1, dtype=np.int64)
+    corr_dir = np.zeros((T, P))
+    corr_ex = np.zeros((T, P))
+    tails: Dict[Tuple[int, int], np.ndarray] = {}
+    nodesets: List[NodeSetPlan] = []
+    ns_pos: Dict[NodeSetKey, int] = {}
+    for ti, t in enumerate(job.transitions):
+        n1 = _idx_limits(job, pa, t)
+        n1_all[ti] = n1
+        d = _dphis(job, n1, k_total, eta_total)
+        # distinct node sets of this transition (pairs of one energy share k_total and eta)
+        cand = np.nonzero(osc & (n1 >= 2))[0]
+        if len(cand):
+            keys = np.rec.fromarrays([n1[cand], k_total[cand], d[cand], eta_total[cand]])
+            uk, inv = np.unique(keys, return_inverse=True)
+            pos = np.empty(len(uk), dtype=np.int64)
+            for u, rec in enumerate(uk):
+                key = NodeSetKey(id(g), int(rec[0]), float(rec[1]), float(rec[2]), float(rec[3]), int(job.CC_nodes))
+                q = ns_pos.get(key)
+                if q is None:
+                    nsp = plan_nodeset(g, key)
+                    q = -1 if nsp is None else len(nodesets)
+                    if nsp is not None:
+                        nodesets.append(nsp)
+                    ns_pos[key] = q
+                pos[u] = q
+            ns_index[ti, cand] = pos[np.ravel(inv)]
+        # L=0 corrections with the limited Simpson weights (dwba_matrix_elements.py:1028-1046, :1249-1296)
+        if v_live:
+            # per pair with the reference's own expressions (np.dot of rho_w and V_diff), so the
+            # rounding does not depend on how many pairs share the call
+            W = waves.matrix()
+            for nv in np.unique(n1):
+                sel = np.nonzero(n1 == nv)[0]
+                wl = w.copy()
+                wl[nv:] = 0.0
+                s2 = np.sum(wl * t.u_f * t.u_i)
+                wl_uf = wl * t.u_f
+                for p in sel:
+                    chi_i, chi_f = W[wi_idx[p]], W[wf_idx[p]]
+                    wl_cf = wl * chi_f
+                    if abs(s2) > OVERLAP_TOL:
+                        corr_dir[ti, p] = np.dot(wl_cf * chi_i, V_diff) * s2
+                    s2e = np.sum(wl_cf * t.u_i)
+                    if abs(s2e) > OVERLAP_TOL:
+                        corr_ex[ti, p] = np.dot(wl_uf * chi_i, V_diff) * s2e
+        # outer tails of the direct term (dwba_matrix_elements.py:1213-1241 advanced/full_split; :1256-1267 legacy)
+        want = (job.L_max >= 1) & (n1 < N - 10) & t.excitation & (
+            (legacy & job.use_oscillatory_quadrature) | ((not legacy) & osc))
+        if want.any():
+            moments = multipole_moments(g, t.u_i, t.u_f, job.L_max)
+            for p in np.nonzero(want)[0]:
+                wave = [pa["k_i"][p], pa["l_i"][p], pa["d_i"][p], pa["e_i"][p], pa["s_i"][p],
+                        pa["k_f"][p], pa["l_f"][p], pa["d_f"][p], pa["e_f"][p], pa["s_f"][p]]
+                tails[(ti, int(p))] = _lib.outer_tails(wave, float(r[n1[p] - 1]), float(r[-1]), job.L_max, moments,
+                                                       1 if legacy else 0, max_seg, max_dphi)
+    job._waves = waves
+    job._wave_idx = (wi_idx, wf_idx)
+    return JobPlan(n1=n1_all, osc=osc, ns_index=ns_index, nodesets=nodesets, corr_dir=corr_dir, corr_ex=corr_ex,
+                   tails=tails)
 
 
 class PreparedJob:
     """A job planned on the host with its inputs and descriptors resident on the device.
 
-    ``launch()`` enqueues every kernel on the current stream (node sets are built in
-    ``__init__`` and cached per grid); ``collect()`` copies the results back once
-    and adds the host-side L=0 corrections and outer tails.
+    ``launch()`` enqueues every kernel on the current stream: node-set operators (those not
+    yet cached for the grid, or all of them with ``rebuild_nodesets``), operand folds and the
+    bilinear forms. ``collect()`` copies the results back once and adds the host-side L=0
+    corrections and outer tails. Results are indexed [transition, pair, L].
     """
 
-    def __init__(self, job: Job, dg: DeviceGrid, engine: str = "dense", plans: Optional[List[PairPlan]] = None,
+    def __init__(self, job: Job, dg: DeviceGrid, engine: str = "dense", plans=None,
                  rebuild_nodesets: bool = False):
         if engine not in ENGINES:
             raise ValueError(f"unknown engine {engine!r}; choose from {ENGINES}")
@@ -245,86 +417,118 @@ class PreparedJob:
         N = g.N
         self.nl = nl = job.L_max + 1
         self.plans = plans = plan_job(job) if plans is None else plans
+        T, P = len(job.transitions), len(job.pairs)
+        self.T, self.P = T, P
         # 1. node sets (operators cached per grid and key; rebuilt every launch when rebuild_nodesets)
-        uniq = {}
-        for p in plans:
-            if p.nodeset is not None:
-                uniq.setdefault(p.nodeset.key, p.nodeset)
-        self.nodesets = NodeSetBatch(dg, list(uniq.values()), job.CC_nodes, rebuild=rebuild_nodesets)
-        # 2. functions on the device
-        pool = _Pool(dev, N)
-        iu_i, iu_f = pool.add(job.u_i), pool.add(job.u_f)
-        fidx = [(pool.add(ci.chi_of_r), pool.add(cf.chi_of_r)) for ci, cf in job.pairs]
-        self.F = F = pool.upload()
-        self.h2d_bytes = int(F.numel()) * 8
-        fptr = lambda i: _ptr(F) + 8 * N * i  # noqa: E731
-        # 3. operand folds: per pair a_dir, a_ex, b_ex, b_dir(standard path); the filon b_dir is shared
-        n_p = len(job.pairs)
+        self.nodesets = NodeSetBatch(dg, plans.nodesets, job.CC_nodes, rebuild=rebuild_nodesets)
+        # 2. functions on the device: continuum waves (planner order) + bound functions
+        waves = getattr(job, "_waves", None) or WaveMatrix(N)
+        wi_idx, wf_idx = getattr(job, "_wave_idx", (None, None))
+        if wi_idx is None:
+            wi_idx = np.array([waves.add(ci.chi_of_r) for ci, _ in job.pairs], dtype=np.int64)
+            wf_idx = np.array([waves.add(cf.chi_of_r) for _, cf in job.pairs], dtype=np.int64)
+        tidx = [(waves.add(t.u_i), waves.add(t.u_f)) for t in job.transitions]
+        self.F = F = waves.upload(dev)
+        self.h2d_bytes = len(waves.arrays) * N * 8
+        Fp = np.uint64(_ptr(F))
+        row = np.uint64(8 * N)
+        fptr = lambda i: Fp + row * np.asarray(i, dtype=np.uint64)  # noqa: E731
+        # 3. operand folds: per (t, p) a_dir, a_ex, b_ex, b_dir(standard); one full-grid b_dir per transition
         SL = 4
-        ops = torch.empty((SL * n_p + 1, N), dtype=torch.float64, device=dev)
-        op_ptr = lambda k: _ptr(ops) + 8 * N * k  # noqa: E731
-        folds = np.zeros(SL * n_p + 1, dtype=_lib.FOLD_DTYPE)
-        forms = np.zeros(2 * n_p, dtype=_lib.FORM_DTYPE)
-        w_ptr = _ptr(dg.w)
-        r_ptr = _ptr(dg.r)
+        n_slots = SL * T * P + T
+        ops = torch.empty((n_slots, N), dtype=torch.float64, device=dev)
+        Op = np.uint64(_ptr(ops))
         wl_cache: Dict[int, torch.Tensor] = {}
 
-        def wl(n1):  # Simpson weights zeroed past n1 (dwba_matrix_elements.py:1025-1026)
-            t = wl_cache.get(n1)
-            if t is None:
-                t = dg.w.clone()
-                t[n1:] = 0.0
-                wl_cache[n1] = t
-            return t
+        def wl_ptr(n1):  # Simpson weights zeroed past n1 (dwba_matrix_elements.py:1025-1026)
+            t_ = wl_cache.get(n1)
+            if t_ is None:
+                t_ = dg.w.clone()
+                t_[n1:] = 0.0
+                wl_cache[n1] = t_
+            return t_.data_ptr()
 
-        b_dir_full = op_ptr(SL * n_p)  # full-grid Simpson weights: the filon inner integral runs over all N
-        nf = 0
-        folds[nf] = (w_ptr, fptr(iu_f), fptr(iu_i), b_dir_full, 0, N, N, N)
-        nf += 1
-        for p_i, (pp, (ic_i, ic_f)) in enumerate(zip(plans, fidx)):
-            a_dir, a_ex, b_ex, b_dir = (op_ptr(SL * p_i + k) for k in range(SL))
-            n1 = pp.n1
-            if pp.osc and pp.nodeset is not None:
-                ns = dg.nodesets[pp.nodeset.key]
-                nb = min(N, n1 + 2)
-                folds[nf] = (_ptr(ns.ta), fptr(ic_f), fptr(ic_i), a_dir, 1, n1, n1, n1)
-                folds[nf + 1] = (_ptr(ns.ta), fptr(iu_f), fptr(ic_i), a_ex, 1, n1, n1, n1)
-                folds[nf + 2] = (_ptr(ns.bx), fptr(ic_f), fptr(iu_i), b_ex, 2, nb, N, nb)
-                nf += 3
-                forms[2 * p_i] = (r_ptr, a_dir, b_dir_full, n1, N)
-                forms[2 * p_i + 1] = (r_ptr, a_ex, b_ex, n1, nb)
-            elif pp.osc:
+        ta_ptr = np.array([dg.nodesets[ns.key].ta.data_ptr() for ns in plans.nodesets] + [0], dtype=np.uint64)
+        bx_ptr = np.array([dg.nodesets[ns.key].bx.data_ptr() for ns in plans.nodesets] + [0], dtype=np.uint64)
+        w_ptr, r_ptr = np.uint64(_ptr(dg.w)), np.uint64(_ptr(dg.r))
+        fold_parts, forms = [], np.zeros(2 * T * P, dtype=_lib.FORM_DTYPE)
+        pidx = np.arange(P, dtype=np.int64)
+        ci_p, cf_p = fptr(wi_idx), fptr(wf_idx)
+
+        def mk(op, f, g_, out, h, n_out, n_src, n_clear):
+            a = np.zeros(len(out), dtype=_lib.FOLD_DTYPE)
+            a["op"], a["f"], a["g"], a["out"] = op, f, g_, out
+            a["half_band"], a["n_out"], a["n_src"], a["n_clear"] = h, n_out, n_src, n_clear
+            return a
+
+        for ti, (iu_i, iu_f) in enumerate(tidx):
+            ui_p, uf_p = fptr(iu_i), fptr(iu_f)
+            b_full = Op + row * np.uint64(SL * T * P + ti)  # filon inner integral runs over all N
+            fold_parts.append(mk(w_ptr, uf_p, ui_p, np.array([b_full]), 0, N, N, N))
+            n1 = plans.n1[ti]
+            k = plans.ns_index[ti]
+            base = (SL * (ti * P + pidx)).astype(np.uint64)
+            a_dir, a_ex, b_ex, b_dir = (Op + row * (base + np.uint64(q)) for q in range(SL))
+            fo = 2 * (ti * P + pidx)
+            nb = np.minimum(N, n1 + 2)
+            A = plans.osc & (k >= 0)
+            B = plans.osc & (k < 0)
+            C = ~plans.osc
+            if A.any():
+                fold_parts.append(mk(ta_ptr[k[A]], cf_p[A], ci_p[A], a_dir[A], 1, n1[A], n1[A], n1[A]))
+                fold_parts.append(mk(ta_ptr[k[A]], uf_p, ci_p[A], a_ex[A], 1, n1[A], n1[A], n1[A]))
+                fold_parts.append(mk(bx_ptr[k[A]], cf_p[A], ui_p, b_ex[A], 2, nb[A], N, nb[A]))
+                forms["r"][fo[A]], forms["a"][fo[A]], forms["b"][fo[A]] = r_ptr, a_dir[A], b_full
+                forms["n_rows"][fo[A]], forms["n_cols"][fo[A]] = n1[A], N
+                forms["r"][fo[A] + 1], forms["a"][fo[A] + 1], forms["b"][fo[A] + 1] = r_ptr, a_ex[A], b_ex[A]
+                forms["n_rows"][fo[A] + 1], forms["n_cols"][fo[A] + 1] = n1[A], nb[A]
+            if B.any():
                 # no valid phase interval: weighted dot products over r[:n1] x r[:N]
                 # (oscillatory_integrals.py:2580-2587, :2694-2699)
-                folds[nf] = (w_ptr, fptr(ic_f), fptr(ic_i), a_dir, 0, n1, N, n1)
-                folds[nf + 1] = (w_ptr, fptr(iu_f), fptr(ic_i), a_ex, 0, n1, N, n1)
-                folds[nf + 2] = (w_ptr, fptr(ic_f), fptr(iu_i), b_ex, 0, N, N, N)
-                nf += 3
-                forms[2 * p_i] = (r_ptr, a_dir, b_dir_full, n1, N)
-                forms[2 * p_i + 1] = (r_ptr, a_ex, b_ex, n1, N)
-            else:
+                fold_parts.append(mk(w_ptr, cf_p[B], ci_p[B], a_dir[B], 0, n1[B], N, n1[B]))
+                fold_parts.append(mk(w_ptr, uf_p, ci_p[B], a_ex[B], 0, n1[B], N, n1[B]))
+                fold_parts.append(mk(w_ptr, cf_p[B], ui_p, b_ex[B], 0, N, N, N))
+                forms["r"][fo[B]], forms["a"][fo[B]], forms["b"][fo[B]] = r_ptr, a_dir[B], b_full
+                forms["n_rows"][fo[B]], forms["n_cols"][fo[B]] = n1[B], N
+                forms["r"][fo[B] + 1], forms["a"][fo[B] + 1], forms["b"][fo[B] + 1] = r_ptr, a_ex[B], b_ex[B]
+                forms["n_rows"][fo[B] + 1], forms["n_cols"][fo[B] + 1] = n1[B], N
+            if C.any():
                 # standard Simpson path with limited weights (dwba_matrix_elements.py:1242-1245, :1287-1289)
-                wlp = _ptr(wl(n1))
-                folds[nf] = (wlp, fptr(ic_f), fptr(ic_i), a_dir, 0, n1, N, n1)
-                folds[nf + 1] = (wlp, fptr(iu_f), fptr(ic_i), a_ex, 0, n1, N, n1)
-                folds[nf + 2] = (wlp, fptr(ic_f), fptr(iu_i), b_ex, 0, n1, N, n1)
-                folds[nf + 3] = (wlp, fptr(iu_f), fptr(iu_i), b_dir, 0, n1, N, n1)
-                nf += 4
-                forms[2 * p_i] = (r_ptr, a_dir, b_dir, n1, n1)
-                forms[2 * p_i + 1] = (r_ptr, a_ex, b_ex, n1, n1)
+                wl = np.array([wl_ptr(int(v)) for v in n1[C]], dtype=np.uint64)
+                fold_parts.append(mk(wl, cf_p[C], ci_p[C], a_dir[C], 0, n1[C], N, n1[C]))
+                fold_parts.append(mk(wl, uf_p, ci_p[C], a_ex[C], 0, n1[C], N, n1[C]))
+                fold_parts.append(mk(wl, cf_p[C], ui_p, b_ex[C], 0, n1[C], N, n1[C]))
+                fold_parts.append(mk(wl, uf_p, ui_p, b_dir[C], 0, n1[C], N, n1[C]))
+                forms["r"][fo[C]], forms["a"][fo[C]], forms["b"][fo[C]] = r_ptr, a_dir[C], b_dir[C]
+                forms["n_rows"][fo[C]], forms["n_cols"][fo[C]] = n1[C], n1[C]
+                forms["r"][fo[C] + 1], forms["a"][fo[C] + 1], forms["b"][fo[C] + 1] = r_ptr, a_ex[C], b_ex[C]
+                forms["n_rows"][fo[C] + 1], forms["n_cols"][fo[C] + 1] = n1[C], n1[C]
+        folds = np.concatenate(fold_parts)
+        nf = len(folds)
         self.n_folds = nf
-        self.folds_d = _dev(folds[:nf].view(np.uint8), dev)
+        self.folds_d = _dev(folds.view(np.uint8), dev)
         self.ops, self.wl_cache = ops, wl_cache
         # 4. bilinear form descriptors
-        self.n_forms = 2 * n_p
+        self.n_forms = 2 * T * P
         self.forms_d = _dev(forms.view(np.uint8), dev)
-        self.out = torch.empty((2 * n_p, nl), dtype=torch.float64, device=dev)
+        self.out = torch.empty((self.n_forms, nl), dtype=torch.float64, device=dev)
         self.ds = diag_scale(job.L_max)
         self.forms_host = forms
+        if engine in TC_TERMS:
+            # direct forms share b per transition: exact FP64 O(N L); exchange forms: tensor cores
+            self.forms_dir_d = _dev(np.ascontiguousarray(forms[0::2]).view(np.uint8), dev)
+            self.forms_ex_d = _dev(np.ascontiguousarray(forms[1::2]).view(np.uint8), dev)
+            self.out_dir = torch.empty((T * P, nl), dtype=torch.float64, device=dev)
+            self.out_ex = torch.empty((T * P, nl), dtype=torch.float64, device=dev)
+            ws = int(lib.dwba_tc_workspace_bytes(T * P, N, job.L_max, TC_TERMS[engine]))
+            if ws < 0:
+                raise ValueError("invalid tensor-core form sizes")
+            self.tc_ws = torch.empty(max(ws, 256), dtype=torch.uint8, device=dev)
+            self.tc_status = torch.zeros(1, dtype=torch.int32, device=dev)
         if engine == "dense":
             m = np.maximum(forms["n_rows"], forms["n_cols"]).astype(np.int32)
-            prefix = np.zeros(2 * n_p + 1, dtype=np.int64)
-            n_cta = lib.dwba_dense_chunk_prefix(m.ctypes.data, 2 * n_p, prefix.ctypes.data)
+            prefix = np.zeros(self.n_forms + 1, dtype=np.int64)
+            n_cta = lib.dwba_dense_chunk_prefix(m.ctypes.data, self.n_forms, prefix.ctypes.data)
             if n_cta < 0:
                 raise ValueError("invalid form sizes")
             self.n_cta = int(n_cta)
@@ -338,8 +542,40 @@ class PreparedJob:
             _lib.check(lib.dwba_fold(_ptr(self.folds_d) + s0 * _lib.FOLD_DTYPE.itemsize, n, self.job.grid.N,
                                      _stream()), "dwba_fold")
 
+    def launch_forms_direct(self) -> None:
+        """Tensor-core engines: the direct forms share b per transition and use the exact FP64 O(N L) form."""
+        job, g = self.job, self.job.grid
+        _lib.check(self.lib.dwba_bilinear_semisep_fp64(_ptr(self.forms_dir_d), self.T * self.P, job.L_max,
+                                                       self.ds.ctypes.data, float(g.r[0]), float(g.r[-1]),
+                                                       _ptr(self.out_dir), _stream()), "dwba_bilinear_semisep_fp64")
+
+    def launch_forms_exchange(self) -> None:
+        """Tensor-core engines: exchange forms on tcgen05 (split bf16 K_L B, FP64 epilogue)."""
+        job, g = self.job, self.job.grid
+        _lib.check(self.lib.dwba_bilinear_tc_bf16(_ptr(self.forms_ex_d), self.T * self.P, _ptr(self.dg.r), g.N,
+                                                  job.L_max, TC_TERMS[self.engine], self.ds.ctypes.data,
+                                                  _ptr(self.tc_ws), self.tc_ws.numel(), _ptr(self.tc_status),
+                                                  _ptr(self.out_ex), _stream()), "dwba_bilinear_tc_bf16")
+
+    def tensor_flops(self) -> Tuple[float, float]:
+        """(dense-equivalent, executed) tensor flops of the exchange forms per launch."""
+        N = self.job.grid.N
+        n_pad = (N + 63) // 64 * 64
+        bn = 256 if TC_TERMS[self.engine] == 2 else 128
+        f_pad = (self.T * self.P + bn - 1) // bn * bn
+        n_iblk = (N + 127) // 128
+        prods = 3 if TC_TERMS[self.engine] == 2 else 6
+        useful = float(np.sum(2.0 * self.forms_host["n_rows"][1::2].astype(np.float64) *
+                              self.forms_host["n_cols"][1::2])) * self.nl
+        executed = 2.0 * (n_iblk * 128) * n_pad * f_pad * self.nl * prods
+        return useful, executed
+
     def launch_forms(self) -> None:
         lib, job = self.lib, self.job
+        if self.engine in TC_TERMS:
+            self.launch_forms_direct()
+            self.launch_forms_exchange()
+            return
         if self.engine == "dense":
             _lib.check(lib.dwba_bilinear_dense_fp64(_ptr(self.forms_d), self.n_forms, job.L_max, self.ds.ctypes.data,
                                                     _ptr(self.prefix_d), self.n_cta, _ptr(self.partial),
@@ -361,23 +597,36 @@ class PreparedJob:
         f = self.forms_host
         return float(np.sum(2.0 * f["n_rows"].astype(np.float64) * f["n_cols"])) * self.nl
 
+    def algorithmic_bytes(self) -> float:
+        """Operand bytes of the semiseparable evaluation: a, b and r read once per form."""
+        f = self.forms_host
+        m = np.maximum(f["n_rows"], f["n_cols"]).astype(np.float64)
+        return float(np.sum(8.0 * (f["n_rows"].astype(np.float64) + f["n_cols"] + m)))
+
     def collect(self):
+        """(I_dir, I_exc) as (T, P, L_max+1) float64 arrays."""
+        if self.engine in TC_TERMS:
+            self.out[0::2] = self.out_dir
+            self.out[1::2] = self.out_ex
         res = self.out.cpu().numpy()  # single device->host transfer (synchronises)
         self.nodesets.check()
-        I_dir = res[0::2].copy()
-        I_exc = res[1::2].copy()
-        for p_i, pp in enumerate(self.plans):
-            if pp.tail is not None:
-                I_dir[p_i] += pp.tail
-            I_dir[p_i, 0] += pp.corr_dir
-            I_exc[p_i, 0] += pp.corr_ex
+        if self.engine in TC_TERMS and int(self.tc_status.item()) != 0:
+            raise _lib.DWBAError(_lib.DWBA_ERR_RANGE, "dwba_bilinear_tc_bf16: a bounded wait expired")
+        T, P, nl = self.T, self.P, self.nl
+        I_dir = res[0::2].reshape(T, P, nl).copy()
+        I_exc = res[1::2].reshape(T, P, nl).copy()
+        pl = self.plans
+        for (ti, p_i), tail in pl.tails.items():
+            I_dir[ti, p_i] += tail
+        I_dir[:, :, 0] += pl.corr_dir
+        I_exc[:, :, 0] += pl.corr_ex
         I_dir[~np.isfinite(I_dir)] = 0.0
         I_exc[~np.isfinite(I_exc)] = 0.0
         return I_dir, I_exc
 
 
-def run_job(job: Job, dg: DeviceGrid, engine: str = "dense", plans: Optional[List[PairPlan]] = None):
-    """Evaluate every pair of a job. Returns (I_dir, I_exc) as (n_pairs, L_max+1) float64 arrays."""
-    pj = PreparedJob(job, dg, engine, plans)
+def run_job(job: Job, dg: DeviceGrid, engine: str = "dense"):
+    """Evaluate every (transition, pair) of a job: (I_dir, I_exc) of shape (T, P, L_max+1)."""
+    pj = PreparedJob(job, dg, engine)
     pj.launch()
     return pj.collect()

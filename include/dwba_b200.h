@@ -149,6 +149,20 @@ int dwba_bilinear_semisep_fp64(const dwba_form_t* forms_dev, int n_forms, int L_
                                const double* diag_scale_host, double r_min_all, double r_max_all,
                                double* out_dev, dwba_stream_t stream);
 
+/* Split-BF16 tensor-core form (tcgen05.mma, TMEM accumulators, TMA-loaded operands):
+ * for every form of one grid, I_L = sum_i a_i (K_L B)_i with K_L generated on the fly and
+ * split into n_terms bf16 terms (2: hi+lo, three products; 3: hi+mid+lo, six products),
+ * FP32 accumulation per 64-column block in TMEM and FP64 epilogue sums. Replaces the
+ * exchange contraction of oscillatory_integrals.py:2745-2770 / dwba_matrix_elements.py:1469-1560
+ * at reduced precision (the error is measured against the FP64 forms). All forms must share
+ * r_dev (n_grid points). workspace: dwba_tc_workspace_bytes(...) bytes, 256-byte aligned.
+ * status_dev: one int, zero on entry; set to 2 if a bounded wait expired (the call's
+ * results are then invalid). */
+int64_t dwba_tc_workspace_bytes(int n_forms, int n_grid, int L_max, int n_terms);
+int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, const double* r_dev, int n_grid, int L_max,
+                          int n_terms, const double* diag_scale_host, void* workspace, int64_t workspace_bytes,
+                          int* status_dev, double* out_dev, dwba_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Host helpers (no GPU work)
  * ------------------------------------------------------------------------- */

@@ -27,22 +27,23 @@ def _model_eval(call):
     kw = dict(call["kwargs"])
     Uf = kw.pop("U_f_array")
     job = dme._make_job(grid, V, Ui, bi, bf, [(ci, cf)], L_max, Uf, kw, _Cache(grid))
-    pp = plan_job(job)[0]
+    pp = plan_job(job).pair(0, 0)
     g, N, r = job.grid, job.grid.N, job.grid.r
     (wi, wf), = job.pairs
+    tr = job.transitions[0]
     n1 = pp.n1
     if pp.osc and pp.nodeset is not None:
         ns = pp.nodeset
         ta, bx = km.bands(r, n1, ns.n_breaks, ns.breaks, job.CC_nodes, ns.log1, ns.log2)
         a_dir = km.fold(ta, 1, wf.chi_of_r, wi.chi_of_r, n1, n1, N)
-        a_ex = km.fold(ta, 1, job.u_f, wi.chi_of_r, n1, n1, N)
-        b_ex = km.fold(bx, 2, wf.chi_of_r, job.u_i, min(N, n1 + 2), N, N)
-        b_dir = g.w * job.u_f * job.u_i
+        a_ex = km.fold(ta, 1, tr.u_f, wi.chi_of_r, n1, n1, N)
+        b_ex = km.fold(bx, 2, wf.chi_of_r, tr.u_i, min(N, n1 + 2), N, N)
+        b_dir = g.w * tr.u_f * tr.u_i
     else:
         wl = g.w.copy()
         wl[n1:] = 0
-        a_dir, a_ex = wl * wf.chi_of_r * wi.chi_of_r, wl * job.u_f * wi.chi_of_r
-        b_ex, b_dir = wl * wf.chi_of_r * job.u_i, wl * job.u_f * job.u_i
+        a_dir, a_ex = wl * wf.chi_of_r * wi.chi_of_r, wl * tr.u_f * wi.chi_of_r
+        b_ex, b_dir = wl * wf.chi_of_r * tr.u_i, wl * tr.u_f * tr.u_i
     Id, Ie = folded_eval(r, a_dir, b_dir, L_max), folded_eval(r, a_ex, b_ex, L_max)
     Sd = folded_eval(r, np.abs(a_dir), np.abs(b_dir), L_max)
     Se = folded_eval(r, np.abs(a_ex), np.abs(b_ex), L_max)
@@ -92,6 +93,24 @@ def test_cc_tables_match_reference():
         x, w = cc_reference(n)
         np.testing.assert_array_equal(x, UNIT[f"cc_x_{n}"])
         np.testing.assert_array_equal(w, UNIT[f"cc_w_{n}"])
+
+
+def test_vectorised_planner_matches_scalar_idx_limit():
+    """The vectorised planner against the scalar restatement of dwba_matrix_elements.py:909-1022."""
+    from dwba_b200.plan import idx_limit
+    for name in gc.case_names():
+        common, calls = gc.load_case(name)
+        grid = common["grid"]
+        pairs = [(a, b) for a in common["waves_i"].values() for b in common["waves_f"].values()]
+        job = dme._make_job(grid, common["V_core"], common["U_i"], common["bound_i"], common["bound_f"], pairs, 4,
+                            common["U_f"], {}, _Cache(grid))
+        jp = plan_job(job)
+        tr = job.transitions[0]
+        for p_i, (ci, cf) in enumerate(job.pairs):
+            pp = jp.pair(0, p_i)
+            n1 = idx_limit(job.grid, job.U_i, job.U_f, tr.u_i, tr.u_f, ci.k_au, cf.k_au, ci.l, cf.l, ci.idx_match,
+                           cf.idx_match)
+            assert pp.n1 == n1, (name, ci.l, cf.l)
 
 
 def test_invalid_arguments_raise_value_error():

@@ -28,6 +28,8 @@ NODESET_DTYPE = np.dtype([(n, "<u8") for n in ("r", "logr", "breaks", "ta", "bx"
 FOLD_DTYPE = np.dtype([(n, "<u8") for n in ("op", "f", "g", "out")]
                       + [(n, "<i4") for n in ("half_band", "n_out", "n_src", "n_clear")])
 FORM_DTYPE = np.dtype([("r", "<u8"), ("a", "<u8"), ("b", "<u8"), ("n_rows", "<i4"), ("n_cols", "<i4")])
+TAIL_DTYPE = np.dtype([("wave", "<f8", (10,)), ("r_m", "<f8"), ("r_max", "<f8"), ("moments", "<u8"), ("out", "<u8"),
+                       ("mode", "<i4"), ("pad", "<i4")])
 
 
 class DWBAError(RuntimeError):
@@ -60,6 +62,8 @@ def _declare(lib):
         "dwba_phase_breaks_coulomb": (c_int, [c_dbl, c_dbl, c_dbl, c_dbl, c_dbl, c_vp, c_int,
                                               ctypes.POINTER(c_int)]),
         "dwba_outer_tails": (c_int, [c_vp, c_dbl, c_dbl, c_int, c_vp, c_int, c_int, c_dbl, c_vp]),
+        "dwba_outer_tails_batch": (c_int, [c_vp, c_int, c_int, c_int, c_dbl, c_vp]),
+        "dwba_outer_tail_on_device": (c_int, [c_vp, c_dbl, c_dbl]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -79,9 +83,9 @@ def load():
     lib = _declare(ctypes.CDLL(LIB_PATH))
     if lib.dwba_abi_version() != 1:
         raise ImportError("libdwba_b200.so ABI version mismatch")
-    sizes = (ctypes.c_int64 * 3)()
-    lib.dwba_struct_sizes(sizes, 3)
-    want = (NODESET_DTYPE.itemsize, FOLD_DTYPE.itemsize, FORM_DTYPE.itemsize)
+    sizes = (ctypes.c_int64 * 4)()
+    lib.dwba_struct_sizes(sizes, 4)
+    want = (NODESET_DTYPE.itemsize, FOLD_DTYPE.itemsize, FORM_DTYPE.itemsize, TAIL_DTYPE.itemsize)
     if tuple(sizes) != want:
         raise ImportError(f"struct layout mismatch: library {tuple(sizes)} vs binding {want}")
     _lib = lib
@@ -114,6 +118,11 @@ def phase_breaks_coulomb(r_start, r_end, k_total, dphi, eta_total):
     check(lib.dwba_phase_breaks_coulomb(float(r_start), float(r_end), float(k_total), float(dphi), float(eta_total),
                                         out.ctypes.data, cap, ctypes.byref(n)), "dwba_phase_breaks_coulomb")
     return out[:n.value].copy()
+
+
+def tail_on_device(wave, r_m, r_max) -> bool:
+    w = np.ascontiguousarray(wave, dtype=np.float64)
+    return bool(load().dwba_outer_tail_on_device(w.ctypes.data, float(r_m), float(r_max)))
 
 
 def outer_tails(wave, r_m, r_max, L_max, moments, mode, max_filon_segments, max_effective_dphi):

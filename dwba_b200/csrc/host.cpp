@@ -456,5 +456,18 @@ extern "C" int dwba_struct_sizes(int64_t* sizes, int n) {
   sizes[0] = (int64_t)sizeof(dwba_nodeset_t);
   sizes[1] = (int64_t)sizeof(dwba_fold_t);
   sizes[2] = (int64_t)sizeof(dwba_form_t);
+  if (n >= 4) sizes[3] = (int64_t)sizeof(dwba_tail_t);
   return DWBA_OK;
+}
+
+// 1 when both phase branches of a pair take the Filon/Levin path (the device kernel's domain),
+// 0 when one of them falls into the adaptive-quadrature branch (mid-interval frequency < 1e-10).
+extern "C" int dwba_outer_tail_on_device(const double* wave_host, double r_m, double r_max) {
+  if (!wave_host) return 0;
+  const Wave wi = {wave_host[0], wave_host[2], wave_host[3], wave_host[4], (int)wave_host[1]};
+  const Wave wf = {wave_host[5], wave_host[7], wave_host[8], wave_host[9], (int)wave_host[6]};
+  const double mid = (r_m + r_max) / 2;
+  for (int sgn = -1; sgn <= 1; sgn += 2)
+    if (std::fabs(Phase(wi, wf, sgn).d1(mid)) < 1e-10) return 0;
+  return 1;
 }

@@ -30,7 +30,7 @@ namespace {
 
 constexpr int BM = 128;  // rows (i) per CTA = TMEM lanes
 constexpr int BK = 64;   // j per block: 64 bf16 = one 128-byte swizzle row
-constexpr int THREADS = 256;
+constexpr int THREADS = 512;  // 16 warps: 4 x 32 rows x 4 column quarters during generation
 constexpr int TC_BN2 = 256;  // forms per CTA with two terms (two 96 KB stages)
 constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz
 
@@ -155,9 +155,8 @@ __device__ __forceinline__ void split_store(uint8_t* a_base, int row, int chunk,
       rem[2 * e + 1] -= __uint_as_float(b1);
       w[e] = (b0 >> 16) | b1;  // element 2e in the low half, 2e+1 in the high half
     }
-    uint32_t addr = smem_u32(a_base + t * (BM * BK * 2) + sw128_offset(row, chunk));
-    asm volatile("st.shared.v4.b32 [%0], {%1,%2,%3,%4};" ::"r"(addr), "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3])
-                 : "memory");
+    *reinterpret_cast<uint4*>(a_base + t * (BM * BK * 2) + sw128_offset(row, chunk)) =
+        make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
@@ -300,13 +299,13 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
     const int j0 = kb * BK;
     const int kind = kind_of(kb);
     {
-      // a warp covers 32 consecutive rows of one column half: the sV reads are broadcasts
+      // a warp covers 32 consecutive rows of one column quarter: the sV reads are broadcasts
       const int row = tid & (BM - 1);
-      const int kh = (tid >> 7) * 32;
+      const int kh = (tid >> 7) * 16;
       const int i = i0 + row;
       const float u = kind == 0 ? sUb[row] : sUa[row];
 #pragma unroll
-      for (int g = 0; g < 4; ++g) {
+      for (int g = 0; g < 2; ++g) {
         float k8[8];
         const int kk0 = kh + 8 * g;
         if (kind != 2) {
@@ -343,7 +342,7 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
-      bool good = *(volatile int*)P.status == 0 && mbar_wait(&bar_full[s], phase_full[s]);
+      bool good = mbar_wait(&bar_full[s], phase_full[s]);
       if (good) {
         full_pending[s] = false;
         phase_full[s] ^= 1;
@@ -389,11 +388,11 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
   if (!ok && tid == 0) atomicExch(P.status, 2);
   tc_fence_after();
   if (ok) {
-    // epilogue: warps w and w+4 share TMEM lanes 32*(w%4).., each takes half the columns
+    // epilogue: warps w, w+4, w+8, w+12 share TMEM lanes 32*(w%4).., each takes a quarter of the columns
     const int g = warp & 3, h = warp >> 2;
     const int row = 32 * g + lane;
     const int i = i0 + row;
-    for (int c0 = h * (BN / 2); c0 < (h + 1) * (BN / 2); c0 += 32) {
+    for (int c0 = h * (BN / 4); c0 < (h + 1) * (BN / 4); c0 += 32) {
       float z[32];
       tmem_ld32(tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)c0, z);
 #pragma unroll

@@ -177,7 +177,8 @@ def _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f
                oscillatory_method=meth, CC_nodes=int(kw.get("CC_nodes", 5)),
                phase_increment=float(kw.get("phase_increment", 1.5708)),
                min_grid_fraction=float(kw.get("min_grid_fraction", 0.10)),
-               k_threshold=float(kw.get("k_threshold", 0.5)))
+               k_threshold=float(kw.get("k_threshold", 0.5)),
+               tails_on_device=os.environ.get("DWBA_B200_TAILS", "device").strip().lower() != "host")
 
 
 def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, gpu_cache, engine):
@@ -246,3 +247,50 @@ def radial_ME_all_L_batch(grid, V_core_array, U_i_array, bound_i, bound_f,
         return [[] for _ in bound_i] if multi else []
     res = _run(grid, V_core_array, U_i_array, bound_i, bound_f, list(pairs), L_max, U_f_array, kw, gpu_cache, engine)
     return res if multi else res[0]
+
+
+def radial_ME_all_L_sweep(points: Sequence[dict], L_max: int, engine: Optional[str] = None, graph: bool = False,
+                          replays: int = 0, **options):
+    """Many energy points in shared launches (new entry point; the reference loops over energies).
+
+    ``points``: one dict per energy point with the arguments of ``radial_ME_all_L_batch``:
+    ``grid``, ``V_core_array``, ``U_i_array``, ``bound_i``, ``bound_f`` (objects or equal-length
+    sequences), ``pairs`` and optionally ``U_f_array``. Every point keeps its own grid (LOCAL
+    adaptive grids of any size); all node sets, operand folds and bilinear forms of all points
+    are evaluated in one launch each. With ``graph=True`` the launch sequence is captured once
+    in a CUDA graph and replayed (``replays`` extra replays, e.g. for timing).
+    Returns, per point, what ``radial_ME_all_L_batch`` returns for it.
+    """
+    if not HAS_CUPY:
+        raise RuntimeError("dwba_b200 engine library is not available (build it with python -m dwba_b200.build)")
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("radial_ME_all_L_sweep: no CUDA device available (the B200 engine has no CPU fallback)")
+    from .engine import MultiPrepared, PreparedJob
+    kw = dict(use_oscillatory_quadrature=options.get("use_oscillatory_quadrature", True),
+              oscillatory_method=options.get("oscillatory_method", "advanced"),
+              CC_nodes=options.get("CC_nodes", 5), phase_increment=options.get("phase_increment", 1.5708),
+              min_grid_fraction=options.get("min_grid_fraction", 0.10), k_threshold=options.get("k_threshold", 0.5))
+    eng = _engine_name(engine)
+    parts, shapes = [], []
+    for pt in points:
+        cache = pt.get("gpu_cache") or GPUCache(pt["grid"])
+        job = _make_job(pt["grid"], pt["V_core_array"], pt["U_i_array"], pt["bound_i"], pt["bound_f"],
+                        list(pt["pairs"]), L_max, pt.get("U_f_array"), kw, cache)
+        parts.append(PreparedJob(job, cache.dg, eng, rebuild_nodesets=True))
+        shapes.append(isinstance(pt["bound_i"], (list, tuple)))
+    mp = MultiPrepared(parts)
+    if graph:
+        mp.capture()
+        for _ in range(max(0, int(replays)) + 1):
+            mp.replay()
+    else:
+        mp.launch()
+    outs = mp.collect()
+    results = []
+    for (I_dir, I_exc), multi, pt in zip(outs, shapes, points):
+        per_t = [[RadialDWBAIntegrals(I_L_direct={L: float(I_dir[t, p, L]) for L in range(L_max + 1)},
+                                      I_L_exchange={L: float(I_exc[t, p, L]) for L in range(L_max + 1)})
+                  for p in range(I_dir.shape[1])] for t in range(I_dir.shape[0])]
+        results.append(per_t if multi else per_t[0])
+    return results

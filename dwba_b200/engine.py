@@ -103,6 +103,7 @@ class NodeSetBatch:
             recs[i] = (_ptr(dg.r), _ptr(dg.logr), _ptr(br), _ptr(ta), _ptr(bx), N, p.key.n1, p.n_breaks,
                        int(p.log1), int(p.log2), 0)
             dg.nodesets[p.key] = DeviceNodeSet(p, ta, bx, 8 * (3 * p.key.n1 + 5 * N))
+        self.recs = recs
         self.recs_d = _dev(recs.view(np.uint8), dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
 
@@ -161,6 +162,7 @@ class Job:
     phase_increment: float = 1.5708
     min_grid_fraction: float = 0.10
     k_threshold: float = 0.5
+    tails_on_device: bool = True
 
 
 def _pair_arrays(pairs):
@@ -296,7 +298,9 @@ class JobPlan:
 
     n1: integration limit; osc: oscillatory branch (per pair); ns_index: node set of the pair
     (index into ``nodesets``, -1 when there is none); corr_dir/corr_ex: L=0 corrections;
-    tails: outer tails of the direct term, keyed by (t, p)."""
+    tails: outer tails of the direct term evaluated on the host, keyed by (t, p);
+    tail_tp/tail_wave/tail_rm/tail_rmax/tail_mode: the tails left to the device kernel (one
+    record per (t, p)); moments: multipole moments M_L of each transition (T, L_max+1)."""
     n1: np.ndarray
     osc: np.ndarray
     ns_index: np.ndarray
@@ -304,6 +308,17 @@ class JobPlan:
     corr_dir: np.ndarray
     corr_ex: np.ndarray
     tails: Dict[Tuple[int, int], np.ndarray]
+    tail_tp: np.ndarray = None
+    tail_wave: np.ndarray = None
+    tail_rm: np.ndarray = None
+    tail_rmax: np.ndarray = None
+    tail_mode: np.ndarray = None
+    moments: np.ndarray = None
+    tail_limits: Tuple[int, float] = (4096, np.pi / 2)
+
+    @property
+    def n_tail_dev(self) -> int:
+        return 0 if self.tail_tp is None else len(self.tail_tp)
 
     def pair(self, t: int, p: int) -> PairPlan:
         k = int(self.ns_index[t, p])
@@ -335,6 +350,8 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
     corr_dir = np.zeros((T, P))
     corr_ex = np.zeros((T, P))
     tails: Dict[Tuple[int, int], np.ndarray] = {}
+    dev_tp, dev_wave, dev_rm, dev_rmax = [], [], [], []
+    moments_all = np.zeros((T, job.L_max + 1))
     nodesets: List[NodeSetPlan] = []
     ns_pos: Dict[NodeSetKey, int] = {}
     for ti, t in enumerate(job.transitions):
@@ -382,15 +399,30 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
             (legacy & job.use_oscillatory_quadrature) | ((not legacy) & osc))
         if want.any():
             moments = multipole_moments(g, t.u_i, t.u_f, job.L_max)
+            moments_all[ti] = moments
             for p in np.nonzero(want)[0]:
-                wave = [pa["k_i"][p], pa["l_i"][p], pa["d_i"][p], pa["e_i"][p], pa["s_i"][p],
-                        pa["k_f"][p], pa["l_f"][p], pa["d_f"][p], pa["e_f"][p], pa["s_f"][p]]
-                tails[(ti, int(p))] = _lib.outer_tails(wave, float(r[n1[p] - 1]), float(r[-1]), job.L_max, moments,
-                                                       1 if legacy else 0, max_seg, max_dphi)
+                wave = np.array([pa["k_i"][p], pa["l_i"][p], pa["d_i"][p], pa["e_i"][p], pa["s_i"][p],
+                                 pa["k_f"][p], pa["l_f"][p], pa["d_f"][p], pa["e_f"][p], pa["s_f"][p]])
+                r_m, r_end = float(r[n1[p] - 1]), float(r[-1])
+                # the device kernel covers the Filon/Levin branches; pairs whose mid-interval
+                # frequency selects the adaptive-quadrature branch stay on the host
+                if job.tails_on_device and (legacy or _lib.tail_on_device(wave, r_m, r_end)):
+                    dev_tp.append((ti, int(p)))
+                    dev_wave.append(wave)
+                    dev_rm.append(r_m)
+                    dev_rmax.append(r_end)
+                else:
+                    tails[(ti, int(p))] = _lib.outer_tails(wave, r_m, r_end, job.L_max, moments,
+                                                           1 if legacy else 0, max_seg, max_dphi)
     job._waves = waves
     job._wave_idx = (wi_idx, wf_idx)
+    nd = len(dev_tp)
     return JobPlan(n1=n1_all, osc=osc, ns_index=ns_index, nodesets=nodesets, corr_dir=corr_dir, corr_ex=corr_ex,
-                   tails=tails)
+                   tails=tails, tail_tp=np.array(dev_tp, dtype=np.int64).reshape(nd, 2),
+                   tail_wave=np.array(dev_wave, dtype=np.float64).reshape(nd, 10),
+                   tail_rm=np.array(dev_rm, dtype=np.float64), tail_rmax=np.array(dev_rmax, dtype=np.float64),
+                   tail_mode=np.full(nd, 1 if legacy else 0, dtype=np.int32), moments=moments_all,
+                   tail_limits=(max_seg, max_dphi))
 
 
 class PreparedJob:
@@ -506,12 +538,18 @@ class PreparedJob:
         folds = np.concatenate(fold_parts)
         nf = len(folds)
         self.n_folds = nf
+        self.folds_host = folds
         self.folds_d = _dev(folds.view(np.uint8), dev)
         self.ops, self.wl_cache = ops, wl_cache
         # 4. bilinear form descriptors
         self.n_forms = 2 * T * P
         self.forms_d = _dev(forms.view(np.uint8), dev)
-        self.out = torch.empty((self.n_forms, nl), dtype=torch.float64, device=dev)
+        self.n_tail = plans.n_tail_dev
+        # rows [0, n_forms): bilinear forms (direct, exchange interleaved); then one row per device tail
+        self.out = torch.empty((self.n_forms + self.n_tail, nl), dtype=torch.float64, device=dev)
+        if self.n_tail:
+            self.moments_d = _dev(np.ascontiguousarray(plans.moments), dev)
+            self.tails_d = _dev(self.tail_records(_ptr(self.out), self.n_forms).view(np.uint8), dev)
         self.ds = diag_scale(job.L_max)
         self.forms_host = forms
         if engine in TC_TERMS:
@@ -534,6 +572,36 @@ class PreparedJob:
             self.n_cta = int(n_cta)
             self.prefix_d = _dev(prefix, dev)
             self.partial = torch.empty(self.n_cta * nl, dtype=torch.float64, device=dev)
+
+    def tail_records(self, out_ptr: int, row0: int) -> np.ndarray:
+        """Device tail records writing rows row0.. of a (rows, L_max+1) float64 buffer at out_ptr."""
+        pl, nl = self.plans, self.nl
+        n = pl.n_tail_dev
+        rec = np.zeros(n, dtype=_lib.TAIL_DTYPE)
+        if n:
+            rec["wave"] = pl.tail_wave
+            rec["r_m"], rec["r_max"], rec["mode"] = pl.tail_rm, pl.tail_rmax, pl.tail_mode
+            rec["moments"] = np.uint64(_ptr(self.moments_d)) + np.uint64(8 * nl) * pl.tail_tp[:, 0].astype(np.uint64)
+            rec["out"] = np.uint64(out_ptr) + np.uint64(8 * nl) * (np.uint64(row0) + np.arange(n, dtype=np.uint64))
+        return rec
+
+    def launch_tails(self) -> None:
+        if self.n_tail and self.job.L_max >= 1:
+            seg, dphi = self.plans.tail_limits
+            _lib.check(self.lib.dwba_outer_tails_batch(_ptr(self.tails_d), self.n_tail, self.job.L_max, seg, dphi,
+                                                       _stream()), "dwba_outer_tails_batch")
+
+    def add_host_terms(self, I_dir, I_exc, tail_rows) -> None:
+        """Outer tails (host- and device-evaluated) and L=0 corrections, then the non-finite guard."""
+        pl = self.plans
+        for (ti, p_i), tail in pl.tails.items():
+            I_dir[ti, p_i] += tail
+        if self.n_tail:
+            I_dir[pl.tail_tp[:, 0], pl.tail_tp[:, 1], 1:] += tail_rows[:, 1:]
+        I_dir[:, :, 0] += pl.corr_dir
+        I_exc[:, :, 0] += pl.corr_ex
+        I_dir[~np.isfinite(I_dir)] = 0.0
+        I_exc[~np.isfinite(I_exc)] = 0.0
 
     def launch_folds(self) -> None:
         lib, nf = self.lib, self.n_folds
@@ -591,6 +659,7 @@ class PreparedJob:
         self.nodesets.launch()
         self.launch_folds()
         self.launch_forms()
+        self.launch_tails()
 
     def algorithmic_flops(self) -> float:
         """Dense-equivalent work: 2 n_rows n_cols flops per (form, L)."""
@@ -605,23 +674,18 @@ class PreparedJob:
 
     def collect(self):
         """(I_dir, I_exc) as (T, P, L_max+1) float64 arrays."""
+        nf = self.n_forms
         if self.engine in TC_TERMS:
-            self.out[0::2] = self.out_dir
-            self.out[1::2] = self.out_ex
+            self.out[0:nf:2] = self.out_dir
+            self.out[1:nf:2] = self.out_ex
         res = self.out.cpu().numpy()  # single device->host transfer (synchronises)
         self.nodesets.check()
         if self.engine in TC_TERMS and int(self.tc_status.item()) != 0:
             raise _lib.DWBAError(_lib.DWBA_ERR_RANGE, "dwba_bilinear_tc_bf16: a bounded wait expired")
         T, P, nl = self.T, self.P, self.nl
-        I_dir = res[0::2].reshape(T, P, nl).copy()
-        I_exc = res[1::2].reshape(T, P, nl).copy()
-        pl = self.plans
-        for (ti, p_i), tail in pl.tails.items():
-            I_dir[ti, p_i] += tail
-        I_dir[:, :, 0] += pl.corr_dir
-        I_exc[:, :, 0] += pl.corr_ex
-        I_dir[~np.isfinite(I_dir)] = 0.0
-        I_exc[~np.isfinite(I_exc)] = 0.0
+        I_dir = res[0:nf:2].reshape(T, P, nl).copy()
+        I_exc = res[1:nf:2].reshape(T, P, nl).copy()
+        self.add_host_terms(I_dir, I_exc, res[nf:])
         return I_dir, I_exc
 
 
@@ -630,3 +694,129 @@ def run_job(job: Job, dg: DeviceGrid, engine: str = "dense"):
     pj = PreparedJob(job, dg, engine)
     pj.launch()
     return pj.collect()
+
+
+class MultiPrepared:
+    """Several prepared jobs (typically one per energy point, each with its own grid) evaluated
+    with shared launches: one node-set launch, one fold launch and one bilinear-form launch for
+    all of them (every descriptor carries its own grid pointer and sizes). The launch sequence
+    does no host synchronisation and no allocation, so it can be captured in a CUDA graph and
+    replayed (``capture()`` / ``replay()``). Tensor-core engines need one grid per launch and
+    launch their exchange forms per job."""
+
+    def __init__(self, parts: List[PreparedJob]):
+        if not parts:
+            raise ValueError("no jobs")
+        self.parts = parts
+        self.engine = parts[0].engine
+        if any(p.engine != self.engine for p in parts):
+            raise ValueError("all jobs of a batch use one engine")
+        dev = parts[0].dg.device
+        self.lib = _lib.load()
+        self.L_max = max(p.job.L_max for p in parts)
+        if any(p.job.L_max != self.L_max for p in parts):
+            raise ValueError("all jobs of a batch share L_max")
+        self.nl = self.L_max + 1
+        # node sets of every part (each record names its own grid)
+        recs = [p.nodesets.recs for p in parts if p.nodesets.n]
+        self.n_sets = int(sum(len(r) for r in recs))
+        self.max_grid = max(p.job.grid.N for p in parts)
+        if self.n_sets:
+            self.recs_d = _dev(np.concatenate(recs).view(np.uint8), dev)
+            cc = {p.nodesets.n_cc for p in parts if p.nodesets.n}
+            if len(cc) != 1:
+                raise ValueError("all jobs of a batch share CC_nodes")
+            self.n_cc = cc.pop()
+            self.ccx, self.ccw = CCTables.get(self.n_cc, dev)
+            self.ns_status = torch.zeros(1, dtype=torch.int32, device=dev)
+        folds = np.concatenate([p.folds_host for p in parts])
+        self.n_folds = len(folds)
+        self.folds_d = _dev(folds.view(np.uint8), dev)
+        forms = np.concatenate([p.forms_host for p in parts])
+        self.n_forms = len(forms)
+        self.forms_host = forms
+        self.forms_d = _dev(forms.view(np.uint8), dev)
+        self.n_tail = int(sum(p.n_tail for p in parts))
+        self.out = torch.empty((self.n_forms + self.n_tail, self.nl), dtype=torch.float64, device=dev)
+        self.ds = diag_scale(self.L_max)
+        self.offsets = np.cumsum([0] + [p.n_forms for p in parts])
+        self.tail_offsets = self.n_forms + np.cumsum([0] + [p.n_tail for p in parts])
+        if self.n_tail:
+            trec = np.concatenate([p.tail_records(_ptr(self.out), int(self.tail_offsets[k]))
+                                   for k, p in enumerate(parts)])
+            self.tails_d = _dev(trec.view(np.uint8), dev)
+            self.tail_limits = parts[0].plans.tail_limits
+        self.r_min = min(float(p.job.grid.r[0]) for p in parts)
+        self.r_max = max(float(p.job.grid.r[-1]) for p in parts)
+        if self.engine == "dense":
+            m = np.maximum(forms["n_rows"], forms["n_cols"]).astype(np.int32)
+            prefix = np.zeros(self.n_forms + 1, dtype=np.int64)
+            self.n_cta = int(self.lib.dwba_dense_chunk_prefix(m.ctypes.data, self.n_forms, prefix.ctypes.data))
+            if self.n_cta < 0:
+                raise ValueError("invalid form sizes")
+            self.prefix_d = _dev(prefix, dev)
+            self.partial = torch.empty(self.n_cta * self.nl, dtype=torch.float64, device=dev)
+        self.graph = None
+
+    def launch(self) -> None:
+        lib = self.lib
+        st = _stream()
+        if self.n_sets:
+            for s0 in range(0, self.n_sets, 65535):
+                n = min(65535, self.n_sets - s0)
+                _lib.check(lib.dwba_build_nodesets(_ptr(self.recs_d) + s0 * _lib.NODESET_DTYPE.itemsize, n,
+                                                   self.max_grid, _ptr(self.ccx), _ptr(self.ccw), self.n_cc,
+                                                   _ptr(self.ns_status), st), "dwba_build_nodesets")
+        for s0 in range(0, self.n_folds, 65535):
+            n = min(65535, self.n_folds - s0)
+            _lib.check(lib.dwba_fold(_ptr(self.folds_d) + s0 * _lib.FOLD_DTYPE.itemsize, n, self.max_grid, st),
+                       "dwba_fold")
+        if self.engine == "dense":
+            _lib.check(lib.dwba_bilinear_dense_fp64(_ptr(self.forms_d), self.n_forms, self.L_max, self.ds.ctypes.data,
+                                                    _ptr(self.prefix_d), self.n_cta, _ptr(self.partial),
+                                                    self.partial.numel(), _ptr(self.out), st),
+                       "dwba_bilinear_dense_fp64")
+        elif self.engine == "semisep":
+            _lib.check(lib.dwba_bilinear_semisep_fp64(_ptr(self.forms_d), self.n_forms, self.L_max, self.ds.ctypes.data,
+                                                      self.r_min, self.r_max, _ptr(self.out), st),
+                       "dwba_bilinear_semisep_fp64")
+        else:
+            for p in self.parts:
+                p.launch_forms()
+                p.launch_tails()
+            return
+        if self.n_tail and self.L_max >= 1:
+            seg, dphi = self.tail_limits
+            _lib.check(lib.dwba_outer_tails_batch(_ptr(self.tails_d), self.n_tail, self.L_max, seg, dphi, st),
+                       "dwba_outer_tails_batch")
+
+    def capture(self) -> None:
+        """Record the launch sequence once in a CUDA graph (warm-up launch first)."""
+        self.launch()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.launch()
+        self.graph = g
+
+    def replay(self) -> None:
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
+
+    def collect(self):
+        """[(I_dir, I_exc) per part], each (T, P, L_max+1)."""
+        if self.engine in TC_TERMS:
+            return [p.collect() for p in self.parts]
+        res = self.out.cpu().numpy()
+        if self.n_sets and int(self.ns_status.item()) != 0:
+            raise _lib.DWBAError(_lib.DWBA_ERR_RANGE, "dwba_build_nodesets")
+        outs = []
+        for k, p in enumerate(self.parts):
+            part = res[self.offsets[k]:self.offsets[k + 1]]
+            T, P, nl = p.T, p.P, p.nl
+            I_dir = part[0::2].reshape(T, P, nl).copy()
+            I_exc = part[1::2].reshape(T, P, nl).copy()
+            p.add_host_terms(I_dir, I_exc, res[self.tail_offsets[k]:self.tail_offsets[k + 1]])
+            outs.append((I_dir, I_exc))
+        return outs

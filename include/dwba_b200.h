@@ -182,11 +182,29 @@ int dwba_phase_breaks_coulomb(double r_start, double r_end, double k_total, doub
 int dwba_outer_tails(const double* wave_host, double r_m, double r_max, int L_max, const double* moments_host,
                      int mode, int max_filon_segments, double max_effective_dphi, double* tail_host);
 
+/* Outer tails on the GPU, one warp per (record, L): the same quantity and formulas as
+ * dwba_outer_tails (Filon / Levin segments split across the lanes, compensated lane sums).
+ * Records whose mid-interval frequency is below 1e-10 take the reference's adaptive-quadrature
+ * branch and must go to dwba_outer_tails instead: dwba_outer_tail_on_device returns 0 for them.
+ * out_dev[L] of each record receives tail[L] for L = 0..L_max (tail[0] = 0). */
+typedef struct {
+  double wave[10];            /* k_i, l_i, delta_i, eta_i, sigma_i, k_f, l_f, delta_f, eta_f, sigma_f */
+  double r_m, r_max;
+  const double* moments_dev;  /* M_L, L = 0..L_max */
+  double* out_dev;            /* tail[L], L = 0..L_max */
+  int32_t mode;               /* 0: advanced/full_split, 1: legacy */
+  int32_t pad;
+} dwba_tail_t;
+
+int dwba_outer_tails_batch(const dwba_tail_t* tails_dev, int n, int L_max, int max_filon_segments,
+                           double max_effective_dphi, dwba_stream_t stream);
+int dwba_outer_tail_on_device(const double* wave_host, double r_m, double r_max);
+
 /* Library identity and device probe (the check_cupy_runtime analogue, dwba_matrix_elements.py:178-193). */
 int dwba_abi_version(void);
 const char* dwba_status_string(int status);
 int dwba_device_probe(int* n_devices, int* cc_major, int* cc_minor);
-/* sizeof(dwba_nodeset_t), sizeof(dwba_fold_t), sizeof(dwba_form_t) into sizes[0..2]. */
+/* sizeof(dwba_nodeset_t), sizeof(dwba_fold_t), sizeof(dwba_form_t), sizeof(dwba_tail_t) into sizes[0..3]. */
 int dwba_struct_sizes(int64_t* sizes, int n);
 
 #ifdef __cplusplus

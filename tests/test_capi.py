@@ -27,9 +27,10 @@ def test_library_exports_every_declared_symbol():
 def test_abi_version_and_struct_layout():
     lib = _lib.load()
     assert lib.dwba_abi_version() == 1
-    sizes = (ctypes.c_int64 * 3)()
-    assert lib.dwba_struct_sizes(sizes, 3) == 0
-    assert tuple(sizes) == (_lib.NODESET_DTYPE.itemsize, _lib.FOLD_DTYPE.itemsize, _lib.FORM_DTYPE.itemsize)
+    sizes = (ctypes.c_int64 * 4)()
+    assert lib.dwba_struct_sizes(sizes, 4) == 0
+    assert tuple(sizes) == (_lib.NODESET_DTYPE.itemsize, _lib.FOLD_DTYPE.itemsize, _lib.FORM_DTYPE.itemsize,
+                            _lib.TAIL_DTYPE.itemsize)
 
 
 def test_status_strings():

@@ -27,6 +27,7 @@ def _model_eval(call):
     kw = dict(call["kwargs"])
     Uf = kw.pop("U_f_array")
     job = dme._make_job(grid, V, Ui, bi, bf, [(ci, cf)], L_max, Uf, kw, _Cache(grid))
+    job.tails_on_device = False  # every tail through the native host path here
     pp = plan_job(job).pair(0, 0)
     g, N, r = job.grid, job.grid.N, job.grid.r
     (wi, wf), = job.pairs
@@ -73,6 +74,14 @@ def test_coulomb_breaks_bit_exact():
         rr = r[: int(n)]
         br = _lib.phase_breaks_coulomb(rr[0], rr[-1], k, d, eta)
         np.testing.assert_array_equal(br, UNIT[f"phase_nodes_{i}"])
+
+
+def test_tail_device_routing():
+    """Pairs reach the device tail kernel unless a phase branch has ~zero mid-interval frequency."""
+    w = np.array([1.2, 2, 0.3, 0.0, 0.0, 0.9, 3, 0.1, 0.0, 0.0])
+    assert _lib.tail_on_device(w, 50.0, 200.0)
+    same = np.array([1.0, 0, 0.3, 0.0, 0.0, 1.0, 0, 0.1, 0.0, 0.0])  # k_i = k_f, l = 0: Phi' of the minus branch = 0
+    assert not _lib.tail_on_device(same, 50.0, 200.0)
 
 
 def test_outer_tails_native():

@@ -13,7 +13,8 @@
 //     K_L(i,j) = U_i V_j (r_j^L / r_i^(L+1) below the diagonal, r_i^L / r_j^(L+1) above),
 //     with U, V scaled by the block's boundary radius so they stay in FP32 range; blocks
 //     that touch the diagonal use the full formula in FP64 (diagonal: (1-1e-12)^L / r);
-//   * one thread issues the tcgen05.mma products into a TMEM accumulator;
+//   * one thread of a dedicated warp issues the TMA copies and the tcgen05.mma products into a
+//     TMEM accumulator;
 //   * two shared-memory stages let generation of block k+1 overlap the MMAs of block k.
 // The epilogue reads the accumulator with tcgen05.ld, multiplies by a_f[i] in FP64 and
 // reduces over the 128 rows; partials per (L, row block, form) are summed in fixed order.
@@ -30,7 +31,9 @@ namespace {
 
 constexpr int BM = 128;  // rows (i) per CTA = TMEM lanes
 constexpr int BK = 64;   // j per block: 64 bf16 = one 128-byte swizzle row
-constexpr int THREADS = 512;  // 16 warps: 4 x 32 rows x 4 column quarters during generation
+constexpr int GEN_WARPS = 16;  // K_L tile generators: 4 x 32 rows x 4 column quarters
+constexpr int GEN_THREADS = 32 * GEN_WARPS;
+constexpr int THREADS = 32 + GEN_THREADS;  // + warp 0: TMA and MMA issue
 constexpr int TC_BN2 = 256;  // forms per CTA with two terms (two 96 KB stages)
 constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz
 
@@ -131,16 +134,10 @@ __device__ __forceinline__ uint32_t sw128_offset(int row, int chunk16) {
   return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((chunk16 ^ (row & 7)) << 4));
 }
 
-// Round-to-nearest-even to bfloat16 on the FP32 bit pattern (integer pipes, no conversion
-// unit): returns the rounded value as an FP32 bit pattern with the low 16 bits clear.
-__device__ __forceinline__ uint32_t bf16_rne_bits(float x) {
-  const uint32_t b = __float_as_uint(x);
-  return (b + 0x7FFFu + ((b >> 16) & 1u)) & 0xFFFF0000u;
-}
-
 template <int NT>
 __device__ __forceinline__ void split_store(uint8_t* a_base, int row, int chunk, const float* k8) {
-  // NT terms: t_0 = bf16(x), t_1 = bf16(x - t_0), t_2 = bf16(x - t_0 - t_1); x - t_0 is exact in FP32
+  // NT terms: t_0 = bf16(x), t_1 = bf16(x - t_0), t_2 = bf16(x - t_0 - t_1); x - t_0 is exact in FP32.
+  // cvt.rn.bf16x2.f32 rounds two values to nearest-even and packs them (first value in the low half).
   float rem[8];
 #pragma unroll
   for (int e = 0; e < 8; ++e) rem[e] = k8[e];
@@ -149,11 +146,12 @@ __device__ __forceinline__ void split_store(uint8_t* a_base, int row, int chunk,
     uint32_t w[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-      const uint32_t b0 = bf16_rne_bits(rem[2 * e]);
-      const uint32_t b1 = bf16_rne_bits(rem[2 * e + 1]);
-      rem[2 * e] -= __uint_as_float(b0);
-      rem[2 * e + 1] -= __uint_as_float(b1);
-      w[e] = (b0 >> 16) | b1;  // element 2e in the low half, 2e+1 in the high half
+      const __nv_bfloat162 q = __floats2bfloat162_rn(rem[2 * e], rem[2 * e + 1]);
+      w[e] = *reinterpret_cast<const uint32_t*>(&q);
+      if (t + 1 < NT) {
+        rem[2 * e] -= __uint_as_float(w[e] << 16);
+        rem[2 * e + 1] -= __uint_as_float(w[e] & 0xFFFF0000u);
+      }
     }
     *reinterpret_cast<uint4*>(a_base + t * (BM * BK * 2) + sw128_offset(row, chunk)) =
         make_uint4(w[0], w[1], w[2], w[3]);
@@ -176,10 +174,32 @@ struct BlockOrder {
   }
 };
 
-// Two shared-memory stages. Per j block t: all threads write K_L(t) into stage t%2 and the
-// column factors of block t+1; thread 0 then issues the MMAs of block t, waits for those of
-// block t-1 and fetches the B tiles of block t+1 into the other stage, which leaves a whole
-// block of MMA time for the copy to land.
+// Named barrier 1 over the generator warps, OR-reducing a predicate (barrier 0 is __syncthreads).
+__device__ __forceinline__ bool gen_barrier_or(bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "n"(GEN_THREADS)
+      : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Warp-specialised pipeline over two shared-memory stages, synchronised by mbarriers only:
+//   warp 0, lane 0 (issuer): waits for K_L(t) (bar_a) and the B tiles of block t (bar_b), issues the
+//     tcgen05.mma products of block t and commits them to bar_mma; then waits for the products of
+//     block t-1 (bar_mma of the other stage) and fetches the B tiles of block t+1 into that stage.
+//   warps 1..16 (generators): wait for the products of block t-2 (stage free), write K_L(t) into the
+//     stage in the swizzled layout and arrive on bar_a (one arrival per warp); the rank-one column
+//     factors of block t+1 are staged through a named barrier among the generator warps, which also
+//     spreads an abort decision.
+// Generation of block t+1 and the copy of its B tiles overlap the products of block t.
 template <int NT, int BN>
 __global__ void __launch_bounds__(THREADS, 1)
 tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P) {
@@ -190,28 +210,32 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
   constexpr int S = 2;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  __shared__ uint64_t bar_full[S], bar_done[S];
+  __shared__ uint64_t bar_b[S], bar_a[S], bar_mma[S];
   __shared__ uint32_t tmem_base_s;
   __shared__ float sUb[BM], sUa[BM], sV[2][BK];
   __shared__ double sRi[BM], sRj[2][BK];
   __shared__ double sRed[4][BN];
-  __shared__ int s_abort;
+  __shared__ volatile int s_abort;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int gtid = tid - 32;  // generator thread index (warps 1..16)
   const int iblk = blockIdx.x, fblk = blockIdx.y, L = blockIdx.z;
   const int i0 = iblk * BM, f0 = fblk * BN;
   const int n_kb = P.n_pad / BK;
-  // a CTA that timed out already: skip the work (nothing allocated yet)
-  if (*(volatile int*)P.status != 0) return;
 
   if (tid == 0) {
+    // a CTA that starts after another one timed out skips the work (the decision is shared
+    // through shared memory so that every thread of the CTA takes the same path)
+    s_abort = *(volatile int*)P.status != 0 ? 1 : 0;
     for (int q = 0; q < S; ++q) {
-      mbar_init(&bar_full[q], 1);
-      mbar_init(&bar_done[q], 1);
+      mbar_init(&bar_b[q], 1);
+      mbar_init(&bar_a[q], GEN_WARPS);
+      mbar_init(&bar_mma[q], 1);
     }
-    s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  __syncthreads();
+  if (s_abort) return;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
                  "r"((uint32_t)BN));
@@ -232,122 +256,61 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
     sUb[m] = in ? (float)exp2(-Lp1 * (li - lg_lo) - lg_lo) : 0.0f;
     sUa[m] = in ? (float)exp2(Ld * (li - lg_hi)) : 0.0f;
   }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = tmem_base_s;
-  const uint32_t idesc = instr_desc(BN);
-
-  // barrier bookkeeping (thread 0 only)
-  uint32_t phase_full[S], phase_done[S];
-  bool full_pending[S], done_pending[S];
-#pragma unroll
-  for (int q = 0; q < S; ++q) {
-    phase_full[q] = phase_done[q] = 0;
-    full_pending[q] = done_pending[q] = false;
-  }
-  bool ok = true;
-
-  auto issue_tma = [&](int st_idx, int kb_t) {
-    uint8_t* b_dst = smem + st_idx * STAGE + NT * A_BYTES;
-    mbar_expect_tx(&bar_full[st_idx], NT * B_BYTES);
-#pragma unroll
-    for (int t = 0; t < NT; ++t) tma_load_2d(b_dst + t * B_BYTES, &bmap, &bar_full[st_idx], kb_t * BK, t * P.f_pad + f0);
-    full_pending[st_idx] = true;
-  };
   auto kind_of = [&](int kb_t) {  // 0: below the diagonal, 1: above, 2: touches it
     const int j0 = kb_t * BK;
     return (j0 + BK - 1 < i0) ? 0 : ((j0 > i0 + BM - 1) ? 1 : 2);
   };
-  // column radii and rank-one column factors of block kb_t (threads < BK)
+  // column radii and rank-one column factors of block kb_t (generator threads < BK)
   auto column_factors = [&](int buf, int kb_t, double rj, double lj) {
     const int kind = kind_of(kb_t);
-    const bool in = kb_t * BK + tid < P.n_grid;
-    sRj[buf][tid] = rj;
+    const bool in = kb_t * BK + gtid < P.n_grid;
+    sRj[buf][gtid] = rj;
     double v = 0.0;
     if (in && kind != 2) v = kind == 0 ? exp2(Ld * (lj - lg_lo)) : exp2(-Lp1 * (lj - lg_hi) - lg_hi);
-    sV[buf][tid] = (float)v;
+    sV[buf][gtid] = (float)v;
   };
-
-  // visit the j blocks from the farthest to the nearest to this row block, so the FP32
-  // accumulator is still small while the many small far-field products are added
-  BlockOrder order(n_kb, i0);
-  int kb = order.next();
-  if (tid == 0) issue_tma(0, kb);
-  if (tid < BK) {
-    const int j = kb * BK + tid;
+  if (gtid >= 0 && gtid < BK) {
+    BlockOrder o(n_kb, i0);
+    const int kb = o.next();
+    const int j = kb * BK + gtid;
     const bool in = j < P.n_grid;
     column_factors(0, kb, in ? P.r[j] : 0.0, in ? P.lg[j] : 0.0);
   }
+  tc_fence_before();
   __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_s;
 
-  for (int step = 0; step < n_kb; ++step) {
-    const int s = step & 1;
-    uint8_t* a_st = smem + s * STAGE;
-    uint8_t* b_st = a_st + NT * A_BYTES;
-    const int kb_next = step + 1 < n_kb ? order.next() : -1;
-    // start the loads of the next block's column data early
-    double rj_n = 0.0, lj_n = 0.0;
-    if (tid < BK && kb_next >= 0) {
-      const int j = kb_next * BK + tid;
-      if (j < P.n_grid) {
-        rj_n = P.r[j];
-        lj_n = P.lg[j];
-      }
-    }
-    // K_L tile in registers -> swizzled shared memory (stage s is free: MMAs of step-2 are done)
-    const int j0 = kb * BK;
-    const int kind = kind_of(kb);
-    {
-      // a warp covers 32 consecutive rows of one column quarter: the sV reads are broadcasts
-      const int row = tid & (BM - 1);
-      const int kh = (tid >> 7) * 16;
-      const int i = i0 + row;
-      const float u = kind == 0 ? sUb[row] : sUa[row];
+  // issuer bookkeeping (warp 0, lane 0): per stage the step of the last B copy issued into it and
+  // whether it is still in flight; the last step whose products were committed
+  int b_step[S] = {-1, -1};
+  bool b_pending[S] = {false, false};
+  int last_commit = -1;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      const uint32_t idesc = instr_desc(BN);
+      auto issue_tma = [&](int st_idx, int kb_t, int step_t) {
+        uint8_t* b_dst = smem + st_idx * STAGE + NT * A_BYTES;
+        mbar_expect_tx(&bar_b[st_idx], NT * B_BYTES);
 #pragma unroll
-      for (int g = 0; g < 2; ++g) {
-        float k8[8];
-        const int kk0 = kh + 8 * g;
-        if (kind != 2) {
-#pragma unroll
-          for (int e = 0; e < 8; ++e) k8[e] = u * sV[s][kk0 + e];
-        } else {
-#pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const int j = j0 + kk0 + e;
-            double kv = 0.0;
-            if (i < P.n_grid && j < P.n_grid) {
-              const double ri = sRi[row], rj = sRj[s][kk0 + e];
-              if (i == j) {
-                kv = P.diag[L] / ri;
-              } else {
-                const double rl = fmin(ri, rj), rg = fmax(ri, rj);
-                const double inv = 1.0 / rg;
-                double ratio = rl * inv, pw = 1.0;
-                for (int e2 = L; e2 > 0; e2 >>= 1) {
-                  if (e2 & 1) pw *= ratio;
-                  ratio *= ratio;
-                }
-                kv = inv * pw;
-              }
-            }
-            k8[e] = (float)kv;
-          }
-        }
-        split_store<NT>(a_st, row, kk0 >> 3, k8);
-      }
-    }
-    // column data of the next block into the other buffer
-    if (tid < BK && kb_next >= 0) column_factors(s ^ 1, kb_next, rj_n, lj_n);
-    fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      bool good = mbar_wait(&bar_full[s], phase_full[s]);
-      if (good) {
-        full_pending[s] = false;
-        phase_full[s] ^= 1;
+        for (int t = 0; t < NT; ++t)
+          tma_load_2d(b_dst + t * B_BYTES, &bmap, &bar_b[st_idx], kb_t * BK, t * P.f_pad + f0);
+        b_step[st_idx] = step_t;
+        b_pending[st_idx] = true;
+      };
+      BlockOrder order(n_kb, i0);
+      issue_tma(0, order.next(), 0);
+      bool good = true;
+      for (int step = 0; step < n_kb; ++step) {
+        const int s = step & 1;
+        const uint32_t par = (uint32_t)((step >> 1) & 1);
+        good = mbar_wait(&bar_a[s], par) && !s_abort;
+        if (good) good = mbar_wait(&bar_b[s], par);
+        if (!good) break;
+        b_pending[s] = false;
         tc_fence_after();
-        const uint32_t a0 = smem_u32(a_st), b0 = smem_u32(b_st);
+        const uint32_t a0 = smem_u32(smem + s * STAGE), b0 = a0 + NT * A_BYTES;
 #pragma unroll
         for (int kk = 0; kk < BK / 16; ++kk) {
 #pragma unroll
@@ -361,35 +324,108 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
             mma_bf16(tmem, ad, bd, idesc, (step > 0 || kk > 0 || q > 0) ? 1u : 0u);
           }
         }
-        mma_commit(&bar_done[s]);
-        done_pending[s] = true;
-        // the other stage is free once the MMAs of the previous block completed
-        if (done_pending[s ^ 1]) {
-          good = mbar_wait(&bar_done[s ^ 1], phase_done[s ^ 1]);
-          phase_done[s ^ 1] ^= 1;
-          done_pending[s ^ 1] = false;
+        mma_commit(&bar_mma[s]);
+        last_commit = step;
+        if (step + 1 < n_kb) {
+          // the other stage is free once the products of block step-1 completed
+          if (step >= 1) good = mbar_wait(&bar_mma[s ^ 1], (uint32_t)(((step - 1) >> 1) & 1));
+          if (!good) break;
+          issue_tma(s ^ 1, order.next(), step + 1);
         }
-        if (good && kb_next >= 0) issue_tma(s ^ 1, kb_next);
       }
       if (!good) s_abort = 1;
     }
-    if (__syncthreads_or(s_abort)) { ok = false; break; }
-    kb = kb_next;
-  }
-  // drain (thread 0): every commit still outstanding and any copy in flight, bounded
-  if (tid == 0) {
-    for (int q = 0; q < S; ++q) {
-      if (done_pending[q] && !mbar_wait(&bar_done[q], phase_done[q])) s_abort = 1;
-      if (full_pending[q]) mbar_wait(&bar_full[q], phase_full[q]);
+    __syncwarp();
+  } else {
+    // generator warps
+    BlockOrder order(n_kb, i0);
+    int kb = order.next();
+    const int row = gtid & (BM - 1);
+    const int kh = (gtid >> 7) * 16;  // a warp covers 32 consecutive rows of one column quarter
+    const int i = i0 + row;
+    bool good = true;
+    for (int step = 0; step < n_kb; ++step) {
+      const int s = step & 1;
+      const int kb_next = step + 1 < n_kb ? order.next() : -1;
+      double rj_n = 0.0, lj_n = 0.0;
+      if (gtid < BK && kb_next >= 0) {
+        const int j = kb_next * BK + gtid;
+        if (j < P.n_grid) {
+          rj_n = P.r[j];
+          lj_n = P.lg[j];
+        }
+      }
+      // stage s is free once the products of block step-2 completed
+      if (step >= 2) good = mbar_wait(&bar_mma[s], (uint32_t)(((step - 2) >> 1) & 1));
+      good = __all_sync(0xffffffffu, good);  // warp-uniform, so the warp's arrival below is all or none
+      if (good) {
+        uint8_t* a_st = smem + s * STAGE;
+        const int j0 = kb * BK;
+        const int kind = kind_of(kb);
+        const float u = kind == 0 ? sUb[row] : sUa[row];
+#pragma unroll
+        for (int g = 0; g < 2; ++g) {
+          float k8[8];
+          const int kk0 = kh + 8 * g;
+          if (kind != 2) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) k8[e] = u * sV[s][kk0 + e];
+          } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+              const int j = j0 + kk0 + e;
+              double kv = 0.0;
+              if (i < P.n_grid && j < P.n_grid) {
+                const double ri = sRi[row], rj = sRj[s][kk0 + e];
+                if (i == j) {
+                  kv = P.diag[L] / ri;
+                } else {
+                  const double rl = fmin(ri, rj), rg = fmax(ri, rj);
+                  const double inv = 1.0 / rg;
+                  double ratio = rl * inv, pw = 1.0;
+                  for (int e2 = L; e2 > 0; e2 >>= 1) {
+                    if (e2 & 1) pw *= ratio;
+                    ratio *= ratio;
+                  }
+                  kv = inv * pw;
+                }
+              }
+              k8[e] = (float)kv;
+            }
+          }
+          split_store<NT>(a_st, row, kk0 >> 3, k8);
+        }
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&bar_a[s]);
+      }
+      // column data of the next block into the other buffer (read in the next step only)
+      if (gtid < BK && kb_next >= 0) column_factors(s ^ 1, kb_next, rj_n, lj_n);
+      if (gen_barrier_or(!good || s_abort)) {
+        good = false;
+        break;
+      }
+      kb = kb_next;
     }
-    if (s_abort) ok = false;
+    // every product has completed once the last commit arrived (commits track all prior MMAs)
+    if (good) good = mbar_wait(&bar_mma[(n_kb - 1) & 1], (uint32_t)(((n_kb - 1) >> 1) & 1));
+    if (!good) s_abort = 1;
   }
-  if (__syncthreads_or(!ok)) ok = false;
-  if (!ok && tid == 0) atomicExch(P.status, 2);
+  __syncthreads();
+  // error path (thread 0): wait, bounded, for the copies still in flight and the last commit
+  if (tid == 0 && s_abort) {
+    for (int q = 0; q < S; ++q)
+      if (b_pending[q]) mbar_wait(&bar_b[q], (uint32_t)((b_step[q] >> 1) & 1));
+    if (last_commit >= 0) mbar_wait(&bar_mma[last_commit & 1], (uint32_t)((last_commit >> 1) & 1));
+    atomicExch(P.status, 2);
+  }
+  __syncthreads();
+  const bool ok = !s_abort;
   tc_fence_after();
-  if (ok) {
-    // epilogue: warps w, w+4, w+8, w+12 share TMEM lanes 32*(w%4).., each takes a quarter of the columns
-    const int g = warp & 3, h = warp >> 2;
+  if (ok && warp >= 1) {
+    // epilogue: warp w reads TMEM lanes 32*(w%4).. (its lane quarter); the four warps of a quarter
+    // split the columns
+    const int g = warp & 3, h = (warp - 1) >> 2;
     const int row = 32 * g + lane;
     const int i = i0 + row;
     for (int c0 = h * (BN / 4); c0 < (h + 1) * (BN / 4); c0 += 32) {

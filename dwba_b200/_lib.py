@@ -28,6 +28,10 @@ NODESET_DTYPE = np.dtype([(n, "<u8") for n in ("r", "logr", "breaks", "ta", "bx"
 FOLD_DTYPE = np.dtype([(n, "<u8") for n in ("op", "f", "g", "out")]
                       + [(n, "<i4") for n in ("half_band", "n_out", "n_src", "n_clear")])
 FORM_DTYPE = np.dtype([("r", "<u8"), ("a", "<u8"), ("b", "<u8"), ("n_rows", "<i4"), ("n_cols", "<i4")])
+FORM_GRAD_DTYPE = np.dtype([("r", "<u8"), ("a", "<u8"), ("b", "<u8"), ("ga", "<u8"), ("gb", "<u8"),
+                            ("n_rows", "<i4"), ("n_cols", "<i4")])
+FOLD_ADJ_DTYPE = np.dtype([("op", "<u8"), ("y", "<u8"), ("z", "<u8"), ("half_band", "<i4"), ("n_out", "<i4"),
+                           ("n_src", "<i4"), ("pad", "<i4")])
 TAIL_DTYPE = np.dtype([("wave", "<f8", (10,)), ("r_m", "<f8"), ("r_max", "<f8"), ("moments", "<u8"), ("out", "<u8"),
                        ("mode", "<i4"), ("pad", "<i4")])
 
@@ -63,6 +67,8 @@ def _declare(lib):
                                               ctypes.POINTER(c_int)]),
         "dwba_outer_tails": (c_int, [c_vp, c_dbl, c_dbl, c_int, c_vp, c_int, c_int, c_dbl, c_vp]),
         "dwba_outer_tails_batch": (c_int, [c_vp, c_int, c_int, c_int, c_dbl, c_vp]),
+        "dwba_bilinear_semisep_backward_fp64": (c_int, [c_vp, c_int, c_int, c_vp, c_vp, c_dbl, c_dbl, c_vp]),
+        "dwba_fold_adjoint": (c_int, [c_vp, c_int, c_int, c_vp]),
         "dwba_outer_tail_on_device": (c_int, [c_vp, c_dbl, c_dbl]),
     }
     for name, (res, args) in sig.items():
@@ -83,9 +89,10 @@ def load():
     lib = _declare(ctypes.CDLL(LIB_PATH))
     if lib.dwba_abi_version() != 1:
         raise ImportError("libdwba_b200.so ABI version mismatch")
-    sizes = (ctypes.c_int64 * 4)()
-    lib.dwba_struct_sizes(sizes, 4)
-    want = (NODESET_DTYPE.itemsize, FOLD_DTYPE.itemsize, FORM_DTYPE.itemsize, TAIL_DTYPE.itemsize)
+    sizes = (ctypes.c_int64 * 6)()
+    lib.dwba_struct_sizes(sizes, 6)
+    want = (NODESET_DTYPE.itemsize, FOLD_DTYPE.itemsize, FORM_DTYPE.itemsize, TAIL_DTYPE.itemsize,
+            FORM_GRAD_DTYPE.itemsize, FOLD_ADJ_DTYPE.itemsize)
     if tuple(sizes) != want:
         raise ImportError(f"struct layout mismatch: library {tuple(sizes)} vs binding {want}")
     _lib = lib

@@ -163,6 +163,9 @@ class Job:
     min_grid_fraction: float = 0.10
     k_threshold: float = 0.5
     tails_on_device: bool = True
+    # tails per unit multipole moment (t_L / M_L) instead of the tails themselves, for callers that
+    # apply the moments themselves (the differentiable path)
+    tails_per_unit_moment: bool = False
 
 
 def _pair_arrays(pairs):
@@ -399,6 +402,8 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
             (legacy & job.use_oscillatory_quadrature) | ((not legacy) & osc))
         if want.any():
             moments = multipole_moments(g, t.u_i, t.u_f, job.L_max)
+            if job.tails_per_unit_moment:
+                moments = np.ones(job.L_max + 1)
             moments_all[ti] = moments
             for p in np.nonzero(want)[0]:
                 wave = np.array([pa["k_i"][p], pa["l_i"][p], pa["d_i"][p], pa["e_i"][p], pa["s_i"][p],
@@ -406,7 +411,8 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
                 r_m, r_end = float(r[n1[p] - 1]), float(r[-1])
                 # the device kernel covers the Filon/Levin branches; pairs whose mid-interval
                 # frequency selects the adaptive-quadrature branch stay on the host
-                if job.tails_on_device and (legacy or _lib.tail_on_device(wave, r_m, r_end)):
+                if job.tails_on_device and not job.tails_per_unit_moment and (
+                        legacy or _lib.tail_on_device(wave, r_m, r_end)):
                     dev_tp.append((ti, int(p)))
                     dev_wave.append(wave)
                     dev_rm.append(r_m)
@@ -460,6 +466,7 @@ class PreparedJob:
             wi_idx = np.array([waves.add(ci.chi_of_r) for ci, _ in job.pairs], dtype=np.int64)
             wf_idx = np.array([waves.add(cf.chi_of_r) for _, cf in job.pairs], dtype=np.int64)
         tidx = [(waves.add(t.u_i), waves.add(t.u_f)) for t in job.transitions]
+        self.wave_rows = (np.asarray(wi_idx), np.asarray(wf_idx), tidx)
         self.F = F = waves.upload(dev)
         self.h2d_bytes = len(waves.arrays) * N * 8
         Fp = np.uint64(_ptr(F))

@@ -182,6 +182,42 @@ int dwba_phase_breaks_coulomb(double r_start, double r_end, double k_total, doub
 int dwba_outer_tails(const double* wave_host, double r_m, double r_max, int L_max, const double* moments_host,
                      int mode, int max_filon_segments, double max_effective_dphi, double* tail_host);
 
+/* ---------------------------------------------------------------------------
+ * Backward (no reference counterpart: the reference computes no gradients).
+ * For each form with upstream gradients g[f*(L_max+1) + L] = dLoss/dI_f,L of the forward
+ * I_f,L = a_f^T K_L b_f (dwba_bilinear_semisep_fp64 / dwba_bilinear_dense_fp64):
+ *   ga_f = K_g b_f  (n_rows values),  gb_f = K_g a_f  (n_cols values),  K_g = sum_L g_L K_L,
+ * i.e. dLoss/da_f and dLoss/db_f (K_L is symmetric). Exact O(n L) FP64; the same range rule as
+ * dwba_bilinear_semisep_fp64 (DWBA_ERR_UNSUPPORTED when r^L or r^-(L+1) would leave FP64).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  const double* r_dev;
+  const double* a_dev;
+  const double* b_dev;
+  double* ga_dev;       /* out, n_rows values */
+  double* gb_dev;       /* out, n_cols values */
+  int32_t n_rows;
+  int32_t n_cols;
+} dwba_form_grad_t;
+
+int dwba_bilinear_semisep_backward_fp64(const dwba_form_grad_t* forms_dev, int n_forms, int L_max,
+                                        const double* diag_scale_host, const double* grad_dev, double r_min_all,
+                                        double r_max_all, dwba_stream_t stream);
+
+/* Adjoint of dwba_fold: z = Op^T y for the banded operator of a fold (same op layout), i.e.
+ * dLoss/d(f .* g) for y = dLoss/d(out). z gets n_src values. No reference counterpart. */
+typedef struct {
+  const double* op_dev;
+  const double* y_dev;  /* >= n_out values */
+  double* z_dev;        /* out, n_src values */
+  int32_t half_band;
+  int32_t n_out;
+  int32_t n_src;
+  int32_t pad;
+} dwba_fold_adj_t;
+
+int dwba_fold_adjoint(const dwba_fold_adj_t* adj_dev, int n, int max_len, dwba_stream_t stream);
+
 /* Outer tails on the GPU, one warp per (record, L): the same quantity and formulas as
  * dwba_outer_tails (Filon / Levin segments split across the lanes, compensated lane sums).
  * Records whose mid-interval frequency is below 1e-10 take the reference's adaptive-quadrature
@@ -204,7 +240,8 @@ int dwba_outer_tail_on_device(const double* wave_host, double r_m, double r_max)
 int dwba_abi_version(void);
 const char* dwba_status_string(int status);
 int dwba_device_probe(int* n_devices, int* cc_major, int* cc_minor);
-/* sizeof(dwba_nodeset_t), sizeof(dwba_fold_t), sizeof(dwba_form_t), sizeof(dwba_tail_t) into sizes[0..3]. */
+/* sizeof(dwba_nodeset_t), sizeof(dwba_fold_t), sizeof(dwba_form_t), sizeof(dwba_tail_t),
+ * sizeof(dwba_form_grad_t), sizeof(dwba_fold_adj_t) into sizes[0..5] (the first n of them). */
 int dwba_struct_sizes(int64_t* sizes, int n);
 
 #ifdef __cplusplus

@@ -108,3 +108,27 @@ def test_hydrogen_slater_F0_known_answer():
     F0 = semiseparable_eval(r, a, a, 0)[0]
     F0d = folded_eval(r, a, a, 0)[0]
     assert abs(F0 - 0.625) < 2e-6 and abs(F0d - F0) < 1e-13
+
+
+def test_oracle_config1_sample():
+    """The folded oracle against the reference's own I_L for config 1 (H 1s->2p, 50 eV, N = 3000)
+    on 16 of its 128 pairs: 1e-12 relative or 1e-13 of the pair's largest multipole."""
+    import json
+    import os
+    z = np.load(os.path.join(gc.GOLDEN_DIR, "config1.npz"))
+    meta = json.loads(bytes(z["meta_json"]).decode())
+    grid = gc.Grid(r=z["r"], dr=z["dr"], w_trapz=z["w_trapz"], w_simpson=z["w_simpson"])
+    bi = gc.BoundOrbital(l=0, energy_au=-0.5, u_of_r=z["u_i"], n_index=1)
+    bf = gc.BoundOrbital(l=1, energy_au=-0.125, u_of_r=z["u_f"], n_index=1)
+    L = meta["L_max"]
+    for p in range(0, len(meta["pairs"]), 8):
+        li, lf = meta["pairs"][p]
+        ci = gc._wave(meta["waves_i"][str(li)], z["chi_i"][li])
+        cf = gc._wave(meta["waves_f"][str(lf)], z["chi_f"][lf])
+        fp = fold_pair(grid, z["V_core"], z["U_i"], bi, bf, ci, cf, L, U_f_array=z["U_f"])
+        Id = folded_eval(grid.r, fp["a_dir"], fp["b_dir"], L) + fp["tail"]
+        Ie = folded_eval(grid.r, fp["a_ex"], fp["b_ex"], L)
+        Id[0] += fp["corr_dir"]
+        Ie[0] += fp["corr_ex"]
+        for I, R in ((Id, z["I_dir"][p]), (Ie, z["I_exc"][p])):
+            assert np.all(np.abs(I - R) <= 1e-12 * np.abs(R) + 1e-13 * np.max(np.abs(R))), (li, lf, I, R)

@@ -34,7 +34,9 @@ constexpr int BK = 64;   // j per block: 64 bf16 = one 128-byte swizzle row
 constexpr int GEN_WARPS = 16;  // K_L tile generators: 4 x 32 rows x 4 column quarters
 constexpr int GEN_THREADS = 32 * GEN_WARPS;
 constexpr int THREADS = 32 + GEN_THREADS;  // + warp 0: TMA and MMA issue
-constexpr int TC_BN2 = 256;  // forms per CTA with two terms (two 96 KB stages)
+constexpr int TC_BN2 = 256;  // forms per CTA with two terms
+constexpr int TC_STAGES = 3;  // pipeline stages (B tiles in shared memory, K_L tiles in tensor memory)
+constexpr int TMEM_COLS = 512;  // accumulator (BN columns) + TC_STAGES x NT K_L terms of BK/2 columns
 constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz
 
 struct GemmParams {
@@ -43,8 +45,10 @@ struct GemmParams {
   const dwba_form_t* forms;    // a_f (rows) for the epilogue
   double* partial;             // [n_L][n_iblk][f_pad]
   const int* bexp;             // per form: b was scaled by 2^-bexp before the split
+  const float* vt;             // [2][n_L][n_pad] column factors within each j block (below, above)
+  const float* st;             // [n_L][n_iblk][n_kb] per (row block, j block) scale (0 where K is not rank one)
   int* status;                 // error word
-  int n_grid, n_pad, f_pad, n_iblk, L_max, n_forms;
+  int n_grid, n_pad, f_pad, n_iblk, L_max, n_forms, n_kb;
   double diag[DWBA_MAX_L + 1];
 };
 
@@ -84,7 +88,6 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
       : "memory");
 }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
@@ -102,14 +105,22 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
 __host__ __device__ constexpr uint32_t instr_desc(int bn) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 }
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                         uint32_t accumulate) {
+// A from tensor memory: row i of the 128 x 16 A slice in lane i, two bf16 per 32-bit column
+// (even k in the low half), 8 consecutive columns per K = 16.
+__device__ __forceinline__ void mma_bf16_tmem_a(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc,
+                                                uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
+      ::"r"(tmem_d), "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* v) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"
+               ::"r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+               : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
@@ -129,32 +140,25 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int c = 0; c < 32; ++c) v[c] = __uint_as_float(r[c]);
 }
 
-// byte offset of element (row, k) in a K-major, 128-byte-swizzled tile with 64 bf16 per row
-__device__ __forceinline__ uint32_t sw128_offset(int row, int chunk16) {
-  return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((chunk16 ^ (row & 7)) << 4));
-}
-
+// 16 consecutive K_L values of one row -> NT bfloat16 terms, 8 packed words each (element 2c in
+// the low half of word c): t_0 = bf16(x), t_1 = bf16(x - t_0), t_2 = bf16(x - t_0 - t_1); x - t_0 is
+// exact in FP32. cvt.rn.bf16x2.f32 rounds two values to nearest-even and packs them.
 template <int NT>
-__device__ __forceinline__ void split_store(uint8_t* a_base, int row, int chunk, const float* k8) {
-  // NT terms: t_0 = bf16(x), t_1 = bf16(x - t_0), t_2 = bf16(x - t_0 - t_1); x - t_0 is exact in FP32.
-  // cvt.rn.bf16x2.f32 rounds two values to nearest-even and packs them (first value in the low half).
-  float rem[8];
+__device__ __forceinline__ void split_terms(const float* k16, uint32_t (*w)[8]) {
+  float rem[16];
 #pragma unroll
-  for (int e = 0; e < 8; ++e) rem[e] = k8[e];
+  for (int e = 0; e < 16; ++e) rem[e] = k16[e];
 #pragma unroll
   for (int t = 0; t < NT; ++t) {
-    uint32_t w[4];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const __nv_bfloat162 q = __floats2bfloat162_rn(rem[2 * e], rem[2 * e + 1]);
-      w[e] = *reinterpret_cast<const uint32_t*>(&q);
+    for (int c = 0; c < 8; ++c) {
+      const __nv_bfloat162 q = __floats2bfloat162_rn(rem[2 * c], rem[2 * c + 1]);
+      w[t][c] = *reinterpret_cast<const uint32_t*>(&q);
       if (t + 1 < NT) {
-        rem[2 * e] -= __uint_as_float(w[e] << 16);
-        rem[2 * e + 1] -= __uint_as_float(w[e] & 0xFFFF0000u);
+        rem[2 * c] -= __uint_as_float(w[t][c] << 16);
+        rem[2 * c + 1] -= __uint_as_float(w[t][c] & 0xFFFF0000u);
       }
     }
-    *reinterpret_cast<uint4*>(a_base + t * (BM * BK * 2) + sw128_offset(row, chunk)) =
-        make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
@@ -174,54 +178,47 @@ struct BlockOrder {
   }
 };
 
-// Named barrier 1 over the generator warps, OR-reducing a predicate (barrier 0 is __syncthreads).
-__device__ __forceinline__ bool gen_barrier_or(bool pred) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.u32 p, %1, 0;\n\t"
-      "bar.red.or.pred q, 1, %2, p;\n\t"
-      "selp.u32 %0, 1, 0, q;\n\t}"
-      : "=r"(r)
-      : "r"((uint32_t)pred), "n"(GEN_THREADS)
-      : "memory");
-  return r != 0;
-}
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Warp-specialised pipeline over two shared-memory stages, synchronised by mbarriers only:
+// Warp-specialised pipeline over S stages, synchronised by mbarriers only. Stage s holds the
+// K_L terms of one j block in tensor memory (A operand of tcgen05.mma, written by the generator
+// warps with tcgen05.st) and the B terms in shared memory (written by TMA):
 //   warp 0, lane 0 (issuer): waits for K_L(t) (bar_a) and the B tiles of block t (bar_b), issues the
-//     tcgen05.mma products of block t and commits them to bar_mma; then waits for the products of
-//     block t-1 (bar_mma of the other stage) and fetches the B tiles of block t+1 into that stage.
-//   warps 1..16 (generators): wait for the products of block t-2 (stage free), write K_L(t) into the
-//     stage in the swizzled layout and arrive on bar_a (one arrival per warp); the rank-one column
-//     factors of block t+1 are staged through a named barrier among the generator warps, which also
-//     spreads an abort decision.
-// Generation of block t+1 and the copy of its B tiles overlap the products of block t.
+//     products of block t and commits them to bar_mma; then waits for the products of block t-1 and
+//     fetches the B tiles of block t+S-1 into that stage (S-1 blocks of copy lead).
+//   warps 1..16 (generators): wait for the products of block t-S (stage free), write K_L(t) and arrive
+//     on bar_a (one arrival per warp). Warp w owns tensor-memory lanes 32 (w mod 4) .. +31 (rows) and
+//     the 16-column quarter (w-1)/4 of the block. Off-diagonal tiles are U_i s(row block, j block) v_j
+//     with v_j from a precomputed table, prefetched one block ahead into registers.
+// Shared memory carries only the B tiles, so the tensor cores read one operand from it.
+// Rank-one factors, scaled so that every factor stays in FP32 range (c_lo, c_hi: smallest and
+// largest radius of the row block, c_b: first radius of the j block):
+//   below the diagonal: K = r_j^L / r_i^(L+1) = [c_lo^L / r_i^(L+1)] [(c_b/c_lo)^L] [(r_j/c_b)^L]
+//   above the diagonal: K = r_i^L / r_j^(L+1) = [(r_i/c_hi)^L] [c_hi^L / c_b^(L+1)] [(r_j/c_b)^-(L+1)]
 template <int NT, int BN>
 __global__ void __launch_bounds__(THREADS, 1)
 tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P) {
-  constexpr int A_BYTES = BM * BK * 2;            // one term
   constexpr int B_BYTES = BN * BK * 2;            // one term
-  constexpr int STAGE = NT * (A_BYTES + B_BYTES);
+  constexpr int STAGE = NT * B_BYTES;             // shared memory per stage
   constexpr int NPROD = NT == 2 ? 3 : 6;
-  constexpr int S = 2;
+  constexpr int S = TC_STAGES;
+  constexpr int A_COLS = BK / 2;                  // tensor-memory columns of one K_L term
+  static_assert(BN + S * NT * A_COLS <= TMEM_COLS, "tensor memory");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   __shared__ uint64_t bar_b[S], bar_a[S], bar_mma[S];
   __shared__ uint32_t tmem_base_s;
-  __shared__ float sUb[BM], sUa[BM], sV[2][BK];
-  __shared__ double sRi[BM], sRj[2][BK];
+  __shared__ float sUb[BM], sUa[BM];
+  __shared__ double sRi[BM];
   __shared__ double sRed[4][BN];
   __shared__ volatile int s_abort;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int gtid = tid - 32;  // generator thread index (warps 1..16)
   const int iblk = blockIdx.x, fblk = blockIdx.y, L = blockIdx.z;
   const int i0 = iblk * BM, f0 = fblk * BN;
-  const int n_kb = P.n_pad / BK;
+  const int n_kb = P.n_kb;
 
   if (tid == 0) {
     // a CTA that starts after another one timed out skips the work (the decision is shared
@@ -238,13 +235,11 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
   if (s_abort) return;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
-                 "r"((uint32_t)BN));
+                 "r"((uint32_t)TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  // rank-one factors are scaled by the row block's smallest (c_lo) and largest (c_hi) radius:
-  //   below: U_i = (r_i/c_lo)^-(L+1) / c_lo, V_j = (r_j/c_lo)^L
-  //   above: U_i = (r_i/c_hi)^L,            V_j = (r_j/c_hi)^-(L+1) / c_hi
-  // evaluated as exp2 of FP64 differences of log2 r (no pow, no division)
+  // row factors: U_i below the diagonal (c_lo^L / r_i^(L+1)) and above ((r_i/c_hi)^L), as exp2 of
+  // FP64 differences of log2 r
   const double lg_lo = P.lg[i0];
   const double lg_hi = P.lg[min(i0 + BM, P.n_grid) - 1];
   const double Lp1 = (double)(L + 1), Ld = (double)L;
@@ -260,38 +255,28 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
     const int j0 = kb_t * BK;
     return (j0 + BK - 1 < i0) ? 0 : ((j0 > i0 + BM - 1) ? 1 : 2);
   };
-  // column radii and rank-one column factors of block kb_t (generator threads < BK)
-  auto column_factors = [&](int buf, int kb_t, double rj, double lj) {
-    const int kind = kind_of(kb_t);
-    const bool in = kb_t * BK + gtid < P.n_grid;
-    sRj[buf][gtid] = rj;
-    double v = 0.0;
-    if (in && kind != 2) v = kind == 0 ? exp2(Ld * (lj - lg_lo)) : exp2(-Lp1 * (lj - lg_hi) - lg_hi);
-    sV[buf][gtid] = (float)v;
-  };
-  if (gtid >= 0 && gtid < BK) {
-    BlockOrder o(n_kb, i0);
-    const int kb = o.next();
-    const int j = kb * BK + gtid;
-    const bool in = j < P.n_grid;
-    column_factors(0, kb, in ? P.r[j] : 0.0, in ? P.lg[j] : 0.0);
-  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_base_s;
+  const uint32_t tmem_a = tmem + BN;  // K_L terms: stage s, term t at column BN + (s NT + t) A_COLS
 
   // issuer bookkeeping (warp 0, lane 0): per stage the step of the last B copy issued into it and
   // whether it is still in flight; the last step whose products were committed
-  int b_step[S] = {-1, -1};
-  bool b_pending[S] = {false, false};
+  int b_step[S];
+  bool b_pending[S];
+#pragma unroll
+  for (int q = 0; q < S; ++q) {
+    b_step[q] = -1;
+    b_pending[q] = false;
+  }
   int last_commit = -1;
 
   if (warp == 0) {
     if (lane == 0) {
       const uint32_t idesc = instr_desc(BN);
       auto issue_tma = [&](int st_idx, int kb_t, int step_t) {
-        uint8_t* b_dst = smem + st_idx * STAGE + NT * A_BYTES;
+        uint8_t* b_dst = smem + st_idx * STAGE;
         mbar_expect_tx(&bar_b[st_idx], NT * B_BYTES);
 #pragma unroll
         for (int t = 0; t < NT; ++t)
@@ -300,17 +285,20 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
         b_pending[st_idx] = true;
       };
       BlockOrder order(n_kb, i0);
-      issue_tma(0, order.next(), 0);
+      // prologue: B tiles of the first S-1 blocks (their stages are free)
+      int n_issued = 0;
+      for (; n_issued < S - 1 && n_issued < n_kb; ++n_issued) issue_tma(n_issued, order.next(), n_issued);
       bool good = true;
       for (int step = 0; step < n_kb; ++step) {
-        const int s = step & 1;
-        const uint32_t par = (uint32_t)((step >> 1) & 1);
+        const int s = step % S;
+        const uint32_t par = (uint32_t)((step / S) & 1);
         good = mbar_wait(&bar_a[s], par) && !s_abort;
         if (good) good = mbar_wait(&bar_b[s], par);
         if (!good) break;
         b_pending[s] = false;
         tc_fence_after();
-        const uint32_t a0 = smem_u32(smem + s * STAGE), b0 = a0 + NT * A_BYTES;
+        const uint32_t b0 = smem_u32(smem + s * STAGE);
+        const uint32_t a0 = tmem_a + (uint32_t)(s * NT * A_COLS);
 #pragma unroll
         for (int kk = 0; kk < BK / 16; ++kk) {
 #pragma unroll
@@ -319,18 +307,21 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
             // NT=2: (0,0) (0,1) (1,0); NT=3: (0,0) (0,1) (1,0) (0,2) (1,1) (2,0)
             const int ta = (q == 2 || q == 4) ? 1 : (q == 5 ? 2 : 0);
             const int tb = (q == 1 || q == 4) ? 1 : (q == 3 ? 2 : 0);
-            const uint64_t ad = smem_desc(a0 + ta * A_BYTES + kk * 32);
             const uint64_t bd = smem_desc(b0 + tb * B_BYTES + kk * 32);
-            mma_bf16(tmem, ad, bd, idesc, (step > 0 || kk > 0 || q > 0) ? 1u : 0u);
+            mma_bf16_tmem_a(tmem, a0 + (uint32_t)(ta * A_COLS + kk * 8), bd, idesc,
+                            (step > 0 || kk > 0 || q > 0) ? 1u : 0u);
           }
         }
         mma_commit(&bar_mma[s]);
         last_commit = step;
-        if (step + 1 < n_kb) {
-          // the other stage is free once the products of block step-1 completed
-          if (step >= 1) good = mbar_wait(&bar_mma[s ^ 1], (uint32_t)(((step - 1) >> 1) & 1));
+        if (n_issued < n_kb) {
+          // block n_issued = step + S - 1 goes into the stage of block step-1, free once its
+          // products completed
+          const int sp = n_issued % S;
+          if (step >= 1) good = mbar_wait(&bar_mma[sp], (uint32_t)(((step - 1) / S) & 1));
           if (!good) break;
-          issue_tma(s ^ 1, order.next(), step + 1);
+          issue_tma(sp, order.next(), n_issued);
+          ++n_issued;
         }
       }
       if (!good) s_abort = 1;
@@ -340,83 +331,95 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
     // generator warps
     BlockOrder order(n_kb, i0);
     int kb = order.next();
-    const int row = gtid & (BM - 1);
-    const int kh = (gtid >> 7) * 16;  // a warp covers 32 consecutive rows of one column quarter
+    const int quarter = warp & 3;              // tensor-memory lane quarter
+    const int row = 32 * quarter + lane;
+    const int kh = ((warp - 1) >> 2) * 16;     // first of this warp's 16 columns of the block
     const int i = i0 + row;
+    const uint32_t lane_off = (uint32_t)(32 * quarter) << 16;
+    const float* vt_b = P.vt + (int64_t)L * P.n_pad;                  // below the diagonal
+    const float* vt_a = P.vt + (int64_t)(P.L_max + 1 + L) * P.n_pad;  // above
+    const float* st = P.st + ((int64_t)L * P.n_iblk + iblk) * n_kb;
+    // column factors and block scale of a j block (rank-one blocks only), 16 columns per thread
+    auto load_factors = [&](int kb_t, float4* v, float& sc) {
+      const int kind = kind_of(kb_t);
+      if (kind == 2) {
+        sc = 0.0f;
+        return;
+      }
+      const float4* src = reinterpret_cast<const float4*>((kind == 0 ? vt_b : vt_a) + kb_t * BK + kh);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v[q] = __ldg(src + q);
+      sc = __ldg(st + kb_t);
+    };
+    float4 v_cur[4], v_nxt[4];
+    float s_cur = 0.0f, s_nxt = 0.0f;
+    load_factors(kb, v_cur, s_cur);
     bool good = true;
     for (int step = 0; step < n_kb; ++step) {
-      const int s = step & 1;
+      const int s = step % S;
       const int kb_next = step + 1 < n_kb ? order.next() : -1;
-      double rj_n = 0.0, lj_n = 0.0;
-      if (gtid < BK && kb_next >= 0) {
-        const int j = kb_next * BK + gtid;
-        if (j < P.n_grid) {
-          rj_n = P.r[j];
-          lj_n = P.lg[j];
-        }
-      }
-      // stage s is free once the products of block step-2 completed
-      if (step >= 2) good = mbar_wait(&bar_mma[s], (uint32_t)(((step - 2) >> 1) & 1));
-      good = __all_sync(0xffffffffu, good);  // warp-uniform, so the warp's arrival below is all or none
-      if (good) {
-        uint8_t* a_st = smem + s * STAGE;
-        const int j0 = kb * BK;
-        const int kind = kind_of(kb);
-        const float u = kind == 0 ? sUb[row] : sUa[row];
+      if (kb_next >= 0) load_factors(kb_next, v_nxt, s_nxt);  // in flight while this block is generated
+      // stage s is free once the products of block step-S completed
+      if (step >= S) good = mbar_wait(&bar_mma[s], (uint32_t)(((step - S) / S) & 1));
+      good = __all_sync(0xffffffffu, good && !s_abort);  // warp-uniform: the warp arrives all or none
+      if (!good) break;
+      tc_fence_after();
+      const int j0 = kb * BK;
+      const int kind = kind_of(kb);
+      float k16[16];
+      if (kind != 2) {
+        const float us = (kind == 0 ? sUb[row] : sUa[row]) * s_cur;
+        const float* vv = reinterpret_cast<const float*>(v_cur);
 #pragma unroll
-        for (int g = 0; g < 2; ++g) {
-          float k8[8];
-          const int kk0 = kh + 8 * g;
-          if (kind != 2) {
+        for (int e = 0; e < 16; ++e) k16[e] = us * vv[e];
+      } else {
+        const double ri = sRi[row];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) k8[e] = u * sV[s][kk0 + e];
-          } else {
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-              const int j = j0 + kk0 + e;
-              double kv = 0.0;
-              if (i < P.n_grid && j < P.n_grid) {
-                const double ri = sRi[row], rj = sRj[s][kk0 + e];
-                if (i == j) {
-                  kv = P.diag[L] / ri;
-                } else {
-                  const double rl = fmin(ri, rj), rg = fmax(ri, rj);
-                  const double inv = 1.0 / rg;
-                  double ratio = rl * inv, pw = 1.0;
-                  for (int e2 = L; e2 > 0; e2 >>= 1) {
-                    if (e2 & 1) pw *= ratio;
-                    ratio *= ratio;
-                  }
-                  kv = inv * pw;
-                }
+        for (int e = 0; e < 16; ++e) {
+          const int j = j0 + kh + e;
+          double kv = 0.0;
+          if (i < P.n_grid && j < P.n_grid) {
+            if (i == j) {
+              kv = P.diag[L] / ri;
+            } else {
+              const double rj = P.r[j];
+              const double rl = fmin(ri, rj), rg = fmax(ri, rj);
+              const double inv = 1.0 / rg;
+              double ratio = rl * inv, pw = 1.0;
+              for (int e2 = L; e2 > 0; e2 >>= 1) {
+                if (e2 & 1) pw *= ratio;
+                ratio *= ratio;
               }
-              k8[e] = (float)kv;
+              kv = inv * pw;
             }
           }
-          split_store<NT>(a_st, row, kk0 >> 3, k8);
+          k16[e] = (float)kv;
         }
-        fence_proxy_async();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&bar_a[s]);
       }
-      // column data of the next block into the other buffer (read in the next step only)
-      if (gtid < BK && kb_next >= 0) column_factors(s ^ 1, kb_next, rj_n, lj_n);
-      if (gen_barrier_or(!good || s_abort)) {
-        good = false;
-        break;
-      }
+      uint32_t w[NT][8];
+      split_terms<NT>(k16, w);
+#pragma unroll
+      for (int t = 0; t < NT; ++t)
+        tmem_st8(tmem_a + lane_off + (uint32_t)((s * NT + t) * A_COLS + (kh >> 1)), w[t]);
+      tmem_wait_st();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bar_a[s]);
       kb = kb_next;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v_cur[q] = v_nxt[q];
+      s_cur = s_nxt;
     }
     // every product has completed once the last commit arrived (commits track all prior MMAs)
-    if (good) good = mbar_wait(&bar_mma[(n_kb - 1) & 1], (uint32_t)(((n_kb - 1) >> 1) & 1));
+    if (good) good = mbar_wait(&bar_mma[(n_kb - 1) % S], (uint32_t)(((n_kb - 1) / S) & 1));
     if (!good) s_abort = 1;
   }
   __syncthreads();
   // error path (thread 0): wait, bounded, for the copies still in flight and the last commit
   if (tid == 0 && s_abort) {
     for (int q = 0; q < S; ++q)
-      if (b_pending[q]) mbar_wait(&bar_b[q], (uint32_t)((b_step[q] >> 1) & 1));
-    if (last_commit >= 0) mbar_wait(&bar_mma[last_commit & 1], (uint32_t)((last_commit >> 1) & 1));
+      if (b_pending[q]) mbar_wait(&bar_b[q], (uint32_t)((b_step[q] / S) & 1));
+    if (last_commit >= 0) mbar_wait(&bar_mma[last_commit % S], (uint32_t)((last_commit / S) & 1));
     atomicExch(P.status, 2);
   }
   __syncthreads();
@@ -456,7 +459,7 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
     }
   }
   if (warp == 0) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)TMEM_COLS));
   }
 }
 
@@ -509,6 +512,40 @@ __global__ void tc_log2_kernel(const double* __restrict__ r, int n, double* __re
   if (i < n) lg[i] = log2(r[i]);
 }
 
+// Rank-one factor tables (FP64 exp2 of log2 differences, rounded once to FP32):
+//   vt[0][L][j] = (r_j/c_b)^L, vt[1][L][j] = (r_j/c_b)^-(L+1), c_b = first radius of j's block;
+//   st[L][iblk][kb] = (c_b/c_lo)^L below the diagonal, c_hi^L / c_b^(L+1) above, 0 when the j block
+//   touches the row block.
+__global__ void tc_factors_kernel(const double* __restrict__ lg, int n_grid, int n_pad, int n_kb, int n_iblk,
+                                  int n_L, float* __restrict__ vt, float* __restrict__ st) {
+  const int64_t n_v = 2LL * n_L * n_pad, n_s = (int64_t)n_L * n_iblk * n_kb;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n_v + n_s;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    if (idx < n_v) {
+      const int j = (int)(idx % n_pad);
+      const int64_t tl = idx / n_pad;
+      const int L = (int)(tl % n_L), t = (int)(tl / n_L);
+      float v = 0.0f;
+      if (j < n_grid) {
+        const double d = lg[j] - lg[(j / BK) * BK];
+        v = (float)(t == 0 ? exp2((double)L * d) : exp2(-(double)(L + 1) * d));
+      }
+      vt[idx] = v;
+    } else {
+      const int64_t q = idx - n_v;
+      const int kb = (int)(q % n_kb);
+      const int64_t li = q / n_kb;
+      const int iblk = (int)(li % n_iblk), L = (int)(li / n_iblk);
+      const int i0 = iblk * BM, j0 = kb * BK;
+      const double lg_lo = lg[i0], lg_hi = lg[min(i0 + BM, n_grid) - 1], lgc = lg[j0];
+      float v = 0.0f;
+      if (j0 + BK - 1 < i0) v = (float)exp2((double)L * (lgc - lg_lo));
+      else if (j0 > i0 + BM - 1) v = (float)exp2((double)L * lg_hi - (double)(L + 1) * lgc);
+      st[q] = v;
+    }
+  }
+}
+
 __global__ void tc_reduce_kernel(const double* __restrict__ partial, int n_forms, int f_pad, int n_iblk, int n_L,
                                  double* __restrict__ out) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -544,7 +581,7 @@ int launch_tc(const GemmParams& P, const __nv_bfloat16* bterms, int n_L, cudaStr
                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) return DWBA_ERR_CUDA;
-  const int smem = 2 * NT * (BM * BK * 2 + BN * BK * 2) + 1024;
+  const int smem = TC_STAGES * NT * (BN * BK * 2) + 1024;
   if (cudaFuncSetAttribute(tc_exchange_kernel<NT, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
       cudaSuccess)
     return DWBA_ERR_CUDA;
@@ -566,7 +603,10 @@ extern "C" int64_t dwba_tc_workspace_bytes(int n_forms, int n_grid, int L_max, i
   const int64_t p = (int64_t)(L_max + 1) * n_iblk * f_pad * 8;
   const int64_t e = f_pad * 4;
   const int64_t lgb = n_pad * 8;
-  return ((b + 255) / 256 * 256) + ((p + 255) / 256 * 256) + ((e + 255) / 256 * 256) + lgb;
+  const int64_t vtb = 2LL * (L_max + 1) * n_pad * 4;
+  const int64_t stb = (int64_t)(L_max + 1) * n_iblk * (n_pad / BK) * 4;
+  return ((b + 255) / 256 * 256) + ((p + 255) / 256 * 256) + ((e + 255) / 256 * 256) + ((lgb + 255) / 256 * 256) +
+         ((vtb + 255) / 256 * 256) + stb;
 }
 
 extern "C" int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, const double* r_dev, int n_grid,
@@ -601,6 +641,11 @@ extern "C" int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, 
   P.bexp = bexp;
   double* lg = (double*)((uint8_t*)bexp + ((int64_t)P.f_pad * 4 + 255) / 256 * 256);
   P.lg = lg;
+  P.n_kb = P.n_pad / BK;
+  float* vt = (float*)((uint8_t*)lg + ((int64_t)P.n_pad * 8 + 255) / 256 * 256);
+  float* stab = (float*)((uint8_t*)vt + (2LL * (L_max + 1) * P.n_pad * 4 + 255) / 256 * 256);
+  P.vt = vt;
+  P.st = stab;
   if (P.f_pad / bn > 65535) return DWBA_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   const int64_t total = (int64_t)P.f_pad * P.n_pad;
@@ -608,6 +653,12 @@ extern "C" int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, 
   DWBA_CHECK_LAUNCH();
   tc_log2_kernel<<<dwba_grid_1d(n_grid, 256), 256, 0, st>>>(r_dev, n_grid, lg);
   DWBA_CHECK_LAUNCH();
+  {
+    const int64_t n_fac = 2LL * (L_max + 1) * P.n_pad + (int64_t)(L_max + 1) * P.n_iblk * P.n_kb;
+    tc_factors_kernel<<<dwba_grid_1d(n_fac, 256, 65535), 256, 0, st>>>(lg, n_grid, P.n_pad, P.n_kb, P.n_iblk,
+                                                                       L_max + 1, vt, stab);
+    DWBA_CHECK_LAUNCH();
+  }
   if (n_terms == 2)
     tc_prepare_kernel<2><<<dwba_grid_1d(total, 256, 65535), 256, 0, st>>>(forms_dev, n_forms, P.n_pad, P.f_pad,
                                                                           bexp, bterms);

@@ -69,7 +69,10 @@ __device__ __forceinline__ int interval_floor(const SetView& s, double x) {
   return m;
 }
 
-__global__ void nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets, const double* __restrict__ ccx_g,
+// One warp per CTA: 32 consecutive rows do similar work (their windows hold similar node counts),
+// and the small CTAs keep the SMs evenly loaded although the work per row grows with r.
+constexpr int ROWS_CTA = 32;
+__global__ void __launch_bounds__(ROWS_CTA, 24) nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets, const double* __restrict__ ccx_g,
                                     const double* __restrict__ ccw_g, int n_cc, int* status) {
   __shared__ double ccx[MAX_CC], ccw[MAX_CC];
   if (threadIdx.x < n_cc) {
@@ -97,8 +100,18 @@ __global__ void nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets, con
     const double wlo = k >= 1 ? r[k - 1] : -1.0e308;
     const double whi = k + 1 <= N - 1 ? r[k + 1] : 1.0e308;
     double t_lo = 0.0, t_di = 0.0, t_up = 0.0;
-    double band[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double band0 = 0.0, band1 = 0.0, band2 = 0.0, band3 = 0.0, band4 = 0.0;
     bool bad = false;
+    // the interpolation intervals a node of this row can use are j in {k-1, k, k+1}: their
+    // reciprocal widths (log r or r) and the reciprocal kernel-column spacings, once per row
+    auto recip = [&](int j, bool lg) -> double {
+      if (j < 0 || j + 1 > N - 1) return 0.0;
+      return lg ? 1.0 / (s.lr[j + 1] - s.lr[j]) : 1.0 / (r[j + 1] - r[j]);
+    };
+    const double iT0 = recip(k - 1, s.log1), iT1 = recip(k, s.log1);
+    const double iB0 = recip(k - 1, s.log2), iB1 = recip(k, s.log2), iB2 = recip(k + 1, s.log2);
+    const double iW0 = k >= 1 ? 1.0 / (r[k] - r[k - 1] + 1e-30) : 0.0;          // il = k-1
+    const double iW1 = k + 1 <= N - 1 ? 1.0 / (r[k + 1] - r[k] + 1e-30) : 0.0;  // il = k
     // nodes never leave [r0, r[n1-1]]; rows past n1+1 have none
     if (k <= n1 + 1) {
       // one interval earlier too: its top node can coincide with the window's lower end
@@ -129,7 +142,12 @@ __global__ void nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets, con
             else if (x >= r[n1 - 1]) { j1 = n1 - 2; t1 = 1.0; }
             else {
               j1 = jf > n1 - 2 ? n1 - 2 : jf;
-              t1 = s.log1 ? (lx - s.lr[j1]) / (s.lr[j1 + 1] - s.lr[j1]) : (x - r[j1]) / (r[j1 + 1] - r[j1]);
+              if (j1 == k || j1 == k - 1) {
+                const double inv = j1 == k ? iT1 : iT0;
+                t1 = s.log1 ? (lx - s.lr[j1]) * inv : (x - r[j1]) * inv;
+              } else {
+                t1 = 0.0;  // reaches no T entry of this row
+              }
             }
             if (j1 == k) {
               t_di += w * (1.0 - t1) * (1.0 - t1);
@@ -153,14 +171,20 @@ __global__ void nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets, con
           else if (x >= r[N - 1]) { j2 = N - 2; t2 = 1.0; }
           else {
             j2 = jf > N - 2 ? N - 2 : jf;
-            t2 = s.log2 ? (lx - s.lr[j2]) / (s.lr[j2 + 1] - s.lr[j2]) : (x - r[j2]) / (r[j2 + 1] - r[j2]);
+            const int dj = j2 - k;  // -1, 0 or 1 inside the window
+            const double inv = dj < 0 ? iB0 : (dj == 0 ? iB1 : iB2);
+            t2 = s.log2 ? (lx - s.lr[j2]) * inv : (x - r[j2]) * inv;
           }
-          const double wr = (x - r[il]) / (r[ir] - r[il] + 1e-30);
+          const double wr = (x - r[il]) * (il == k ? iW1 : iW0);
           const double q = il == k ? 1.0 - wr : wr;
           const int d0 = j2 - k;
           if (d0 < -2 || d0 + 1 > 2) { bad = true; continue; }
-          band[d0 + 2] += q * w * (1.0 - t2);
-          band[d0 + 3] += q * w * t2;
+          const double v0 = q * w * (1.0 - t2), v1 = q * w * t2;
+          // taps d0, d0+1 of the row's band (registers: no dynamic indexing)
+          if (d0 == -2) { band0 += v0; band1 += v1; }
+          else if (d0 == -1) { band1 += v0; band2 += v1; }
+          else if (d0 == 0) { band2 += v0; band3 += v1; }
+          else { band3 += v0; band4 += v1; }
         }
       }
     }
@@ -169,8 +193,12 @@ __global__ void nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets, con
       d.ta_dev[3 * k + 1] = t_di;
       d.ta_dev[3 * k + 2] = t_up;
     }
-#pragma unroll
-    for (int q = 0; q < 5; ++q) d.bx_dev[5 * k + q] = band[q];
+    double* bx = d.bx_dev + 5 * (int64_t)k;
+    bx[0] = band0;
+    bx[1] = band1;
+    bx[2] = band2;
+    bx[3] = band3;
+    bx[4] = band4;
     if (bad) atomicExch(status, 1);
   }
 }
@@ -183,8 +211,8 @@ extern "C" int dwba_build_nodesets(const dwba_nodeset_t* sets_dev, int n_sets, i
   if (!sets_dev || !cc_x_dev || !cc_w_dev || !status_dev || n_cc < 2 || n_cc > MAX_CC || max_grid < 2 ||
       n_sets > 65535)
     return DWBA_ERR_INVALID_ARG;
-  dim3 grid(dwba_grid_1d(max_grid, 128, 4096), n_sets);
-  nodeset_rows_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc, status_dev);
+  dim3 grid(dwba_grid_1d(max_grid, ROWS_CTA), n_sets);
+  nodeset_rows_kernel<<<grid, ROWS_CTA, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc, status_dev);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;
 }

@@ -60,10 +60,16 @@ def check_cupy_runtime() -> bool:
         return False
 
 
+ENGINE_NAMES = ("dense", "semisep", "tc_bf16x3", "tc_bf16x6", "auto", "auto_split")
+
+
 def _engine_name(engine: Optional[str]) -> str:
+    """Engine of a call: the argument, else DWBA_B200_ENGINE, else the plain FP64 kernel. ``auto``
+    times the FP64 engines per shape class and keeps the fastest; ``auto_split`` also admits the
+    split-BF16 tensor-core form."""
     e = engine or os.environ.get("DWBA_B200_ENGINE", "dense")
-    if e not in ("dense", "semisep", "tc_bf16x3", "tc_bf16x6"):
-        raise ValueError(f"unknown engine {e!r} (dense | semisep | tc_bf16x3 | tc_bf16x6)")
+    if e not in ENGINE_NAMES:
+        raise ValueError(f"unknown engine {e!r} ({' | '.join(ENGINE_NAMES)})")
     return e
 
 
@@ -188,11 +194,22 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
     import torch
     if not torch.cuda.is_available():
         raise RuntimeError("radial_ME_all_L: no CUDA device available (the B200 engine has no CPU fallback)")
-    from .engine import run_job
+    from .engine import PreparedJob, plan_job, run_job
+    from . import tune
     cache = _cache_for(grid, gpu_cache)
     job = _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, cache)
+    eng = _engine_name(engine)
     with torch.cuda.device(cache.device):
-        I_dir, I_exc = run_job(job, cache.dg, engine=_engine_name(engine))
+        if tune.is_auto(eng):
+            plans = plan_job(job)
+            cands = tune.candidates(eng)
+            key = tune.TUNER.key(cache.info.N, 2 * len(job.transitions) * len(job.pairs), L_max, cands)
+            _, pj = tune.TUNER.select(key, cands, lambda e: PreparedJob(job, cache.dg, e, plans=plans),
+                                      lambda p: p.launch())
+            pj.launch()
+            I_dir, I_exc = pj.collect()
+        else:
+            I_dir, I_exc = run_job(job, cache.dg, engine=eng)
     return [[RadialDWBAIntegrals(I_L_direct={L: float(I_dir[t, p, L]) for L in range(L_max + 1)},
                                  I_L_exchange={L: float(I_exc[t, p, L]) for L in range(L_max + 1)})
              for p in range(len(pairs))] for t in range(I_dir.shape[0])]
@@ -266,20 +283,30 @@ def radial_ME_all_L_sweep(points: Sequence[dict], L_max: int, engine: Optional[s
     import torch
     if not torch.cuda.is_available():
         raise RuntimeError("radial_ME_all_L_sweep: no CUDA device available (the B200 engine has no CPU fallback)")
-    from .engine import MultiPrepared, PreparedJob
+    from .engine import MultiPrepared, PreparedJob, plan_job
+    from . import tune
     kw = dict(use_oscillatory_quadrature=options.get("use_oscillatory_quadrature", True),
               oscillatory_method=options.get("oscillatory_method", "advanced"),
               CC_nodes=options.get("CC_nodes", 5), phase_increment=options.get("phase_increment", 1.5708),
               min_grid_fraction=options.get("min_grid_fraction", 0.10), k_threshold=options.get("k_threshold", 0.5))
     eng = _engine_name(engine)
-    parts, shapes = [], []
+    jobs, shapes = [], []
     for pt in points:
         cache = pt.get("gpu_cache") or GPUCache(pt["grid"])
         job = _make_job(pt["grid"], pt["V_core_array"], pt["U_i_array"], pt["bound_i"], pt["bound_f"],
                         list(pt["pairs"]), L_max, pt.get("U_f_array"), kw, cache)
-        parts.append(PreparedJob(job, cache.dg, eng, rebuild_nodesets=True))
+        jobs.append((job, cache, plan_job(job)))
         shapes.append(isinstance(pt["bound_i"], (list, tuple)))
-    mp = MultiPrepared(parts)
+
+    def build(e):
+        return MultiPrepared([PreparedJob(j, c.dg, e, plans=pl, rebuild_nodesets=True) for j, c, pl in jobs])
+    if tune.is_auto(eng):
+        cands = tune.candidates(eng)
+        n_forms = sum(2 * len(j.transitions) * len(j.pairs) for j, _, _ in jobs)
+        key = tune.TUNER.key(max(c.info.N for _, c, _ in jobs), n_forms, L_max, cands)
+        _, mp = tune.TUNER.select(key, cands, build, lambda m: m.launch())
+    else:
+        mp = build(eng)
     if graph:
         mp.capture()
         for _ in range(max(0, int(replays)) + 1):

@@ -107,6 +107,14 @@ class NodeSetBatch:
         self.recs_d = _dev(recs.view(np.uint8), dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
 
+    def algorithmic_bytes(self) -> float:
+        """Bytes a build must move: the operators written (3 n1 + 5 N doubles per set) and the grid
+        read (r and log r, 2 N doubles per set)."""
+        if self.n == 0:
+            return 0.0
+        N = float(self.dg.info.N)
+        return float(np.sum(8.0 * (3.0 * self.recs["n1"].astype(np.float64) + 7.0 * N)))
+
     def launch(self) -> None:
         if self.n == 0:
             return
@@ -672,6 +680,13 @@ class PreparedJob:
         """Dense-equivalent work: 2 n_rows n_cols flops per (form, L)."""
         f = self.forms_host
         return float(np.sum(2.0 * f["n_rows"].astype(np.float64) * f["n_cols"])) * self.nl
+
+    def fold_bytes(self) -> float:
+        """Bytes the folds must move: (2h+1) operator taps per output row, f and g over n_src,
+        the outputs over n_clear."""
+        f = self.folds_host
+        taps = (2.0 * f["half_band"].astype(np.float64) + 1.0) * f["n_out"]
+        return float(np.sum(8.0 * (taps + 2.0 * f["n_src"] + f["n_clear"])))
 
     def algorithmic_bytes(self) -> float:
         """Operand bytes of the semiseparable evaluation: a, b and r read once per form."""

@@ -420,7 +420,8 @@ def main():
             pass
     if rank == 0:
         per_forms = {"dense": 2, "semisep": 1, "tc_bf16x3": 5, "tc_bf16x6": 5}[args.engine]
-        n_launch = sum((1 if p.nodesets.n else 0) + (p.n_folds + 65534) // 65535 + per_forms for p in preps)
+        n_launch = sum((1 if p.nodesets.n else 0) + (p.n_folds + 65534) // 65535 + (p.n_multi + 65534) // 65535 +
+                       per_forms for p in preps)
         line = {"metric": METRIC, "value": value, "unit": "integrals/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "bf16 split (x3/x6) + f64" if tc else "f64", "data": "synthetic",

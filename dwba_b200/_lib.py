@@ -32,6 +32,10 @@ FORM_GRAD_DTYPE = np.dtype([("r", "<u8"), ("a", "<u8"), ("b", "<u8"), ("ga", "<u
                             ("n_rows", "<i4"), ("n_cols", "<i4")])
 FOLD_ADJ_DTYPE = np.dtype([("op", "<u8"), ("y", "<u8"), ("z", "<u8"), ("half_band", "<i4"), ("n_out", "<i4"),
                            ("n_src", "<i4"), ("pad", "<i4")])
+FOLD_MULTI = 8
+FOLD_MULTI_DTYPE = np.dtype([("op", "<u8"), ("g", "<u8"), ("f", "<u8", (FOLD_MULTI,)), ("out", "<u8", (FOLD_MULTI,)),
+                             ("n_f", "<i4"), ("half_band", "<i4"), ("n_out", "<i4"), ("n_src", "<i4"),
+                             ("n_clear", "<i4"), ("pad", "<i4")])
 TAIL_DTYPE = np.dtype([("wave", "<f8", (10,)), ("r_m", "<f8"), ("r_max", "<f8"), ("moments", "<u8"), ("out", "<u8"),
                        ("mode", "<i4"), ("pad", "<i4")])
 
@@ -69,6 +73,7 @@ def _declare(lib):
         "dwba_outer_tails_batch": (c_int, [c_vp, c_int, c_int, c_int, c_dbl, c_vp]),
         "dwba_bilinear_semisep_backward_fp64": (c_int, [c_vp, c_int, c_int, c_vp, c_vp, c_dbl, c_dbl, c_vp]),
         "dwba_fold_adjoint": (c_int, [c_vp, c_int, c_int, c_vp]),
+        "dwba_fold_multi": (c_int, [c_vp, c_int, c_int, c_vp]),
         "dwba_outer_tail_on_device": (c_int, [c_vp, c_dbl, c_dbl]),
     }
     for name, (res, args) in sig.items():
@@ -89,10 +94,10 @@ def load():
     lib = _declare(ctypes.CDLL(LIB_PATH))
     if lib.dwba_abi_version() != 1:
         raise ImportError("libdwba_b200.so ABI version mismatch")
-    sizes = (ctypes.c_int64 * 6)()
-    lib.dwba_struct_sizes(sizes, 6)
+    sizes = (ctypes.c_int64 * 7)()
+    lib.dwba_struct_sizes(sizes, 7)
     want = (NODESET_DTYPE.itemsize, FOLD_DTYPE.itemsize, FORM_DTYPE.itemsize, TAIL_DTYPE.itemsize,
-            FORM_GRAD_DTYPE.itemsize, FOLD_ADJ_DTYPE.itemsize)
+            FORM_GRAD_DTYPE.itemsize, FOLD_ADJ_DTYPE.itemsize, FOLD_MULTI_DTYPE.itemsize)
     if tuple(sizes) != want:
         raise ImportError(f"struct layout mismatch: library {tuple(sizes)} vs binding {want}")
     _lib = lib

@@ -94,7 +94,7 @@ class _BilinearFn(torch.autograd.Function):
         gops.index_add_(0, as_idx((fh["a"] - Op) // row), GA)
         gops.index_add_(0, as_idx((fh["b"] - Op) // row), GB)
         # adjoint of every fold: z = Op^T y, then d(f*g) -> f, g
-        fo = pj.folds_host
+        fo = pj.fold_singles
         nfo = len(fo)
         Z = torch.zeros((nfo, N), dtype=torch.float64, device=dev)
         adj = np.zeros(nfo, dtype=_lib.FOLD_ADJ_DTYPE)

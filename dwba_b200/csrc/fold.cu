@@ -33,7 +33,52 @@ __global__ void fold_kernel(const dwba_fold_t* __restrict__ folds) {
   }
 }
 
+template <int H>
+__device__ __forceinline__ void fold_multi_row(const dwba_fold_multi_t& m, int i) {
+  double tap[2 * H + 1], gv[2 * H + 1];
+  const double* __restrict__ op = m.op_dev + (int64_t)(2 * H + 1) * i;
+#pragma unroll
+  for (int d = -H; d <= H; ++d) {
+    const int k = i + d;
+    const bool in = k >= 0 && k < m.n_src;
+    tap[d + H] = in ? op[d + H] : 0.0;
+    gv[d + H] = in ? m.g_dev[k] : 0.0;
+  }
+  for (int t = 0; t < m.n_f; ++t) {
+    const double* __restrict__ f = m.f_dev[t];
+    double acc = 0.0;
+#pragma unroll
+    for (int d = -H; d <= H; ++d) {
+      const int k = i + d;
+      if (k >= 0 && k < m.n_src) acc += tap[d + H] * (f[k] * gv[d + H]);
+    }
+    m.out_dev[t][i] = acc;
+  }
+}
+
+__global__ void fold_multi_kernel(const dwba_fold_multi_t* __restrict__ folds) {
+  const dwba_fold_multi_t m = folds[blockIdx.y];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n_clear; i += gridDim.x * blockDim.x) {
+    if (i < m.n_out) {
+      if (m.half_band == 0) fold_multi_row<0>(m, i);
+      else if (m.half_band == 1) fold_multi_row<1>(m, i);
+      else fold_multi_row<2>(m, i);
+    } else {
+      for (int t = 0; t < m.n_f; ++t) m.out_dev[t][i] = 0.0;
+    }
+  }
+}
+
 }  // namespace
+
+extern "C" int dwba_fold_multi(const dwba_fold_multi_t* folds_dev, int n_folds, int max_rows, dwba_stream_t stream) {
+  if (n_folds <= 0) return DWBA_OK;
+  if (!folds_dev || max_rows < 0 || n_folds > 65535) return DWBA_ERR_INVALID_ARG;
+  dim3 grid(dwba_grid_1d(max_rows, 256, 1024), n_folds);
+  fold_multi_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(folds_dev);
+  DWBA_CHECK_LAUNCH();
+  return DWBA_OK;
+}
 
 extern "C" int dwba_fold(const dwba_fold_t* folds_dev, int n_folds, int max_rows, dwba_stream_t stream) {
   if (n_folds <= 0) return DWBA_OK;

@@ -459,6 +459,7 @@ extern "C" int dwba_struct_sizes(int64_t* sizes, int n) {
   if (n >= 4) sizes[3] = (int64_t)sizeof(dwba_tail_t);
   if (n >= 5) sizes[4] = (int64_t)sizeof(dwba_form_grad_t);
   if (n >= 6) sizes[5] = (int64_t)sizeof(dwba_fold_adj_t);
+  if (n >= 7) sizes[6] = (int64_t)sizeof(dwba_fold_multi_t);
   return DWBA_OK;
 }
 

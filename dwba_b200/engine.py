@@ -439,6 +439,21 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
                    tail_limits=(max_seg, max_dphi))
 
 
+def expand_multi(multi: np.ndarray) -> np.ndarray:
+    """The single folds a set of multi-folds stands for (same operator, factors and output)."""
+    n = int(np.sum(multi["n_f"])) if len(multi) else 0
+    out = np.zeros(n, dtype=_lib.FOLD_DTYPE)
+    if n == 0:
+        return out
+    g = np.repeat(np.arange(len(multi)), multi["n_f"])
+    pos = np.arange(n) - np.repeat(np.cumsum(multi["n_f"]) - multi["n_f"], multi["n_f"])
+    out["op"], out["g"] = multi["op"][g], multi["g"][g]
+    out["f"], out["out"] = multi["f"][g, pos], multi["out"][g, pos]
+    for k in ("half_band", "n_out", "n_src", "n_clear"):
+        out[k] = multi[k][g]
+    return out
+
+
 class PreparedJob:
     """A job planned on the host with its inputs and descriptors resident on the device.
 
@@ -508,6 +523,7 @@ class PreparedJob:
             a["half_band"], a["n_out"], a["n_src"], a["n_clear"] = h, n_out, n_src, n_clear
             return a
 
+        A_parts = []  # node-set branch entries, grouped into multi-folds after the loop
         for ti, (iu_i, iu_f) in enumerate(tidx):
             ui_p, uf_p = fptr(iu_i), fptr(iu_f)
             b_full = Op + row * np.uint64(SL * T * P + ti)  # filon inner integral runs over all N
@@ -522,9 +538,9 @@ class PreparedJob:
             B = plans.osc & (k < 0)
             C = ~plans.osc
             if A.any():
-                fold_parts.append(mk(ta_ptr[k[A]], cf_p[A], ci_p[A], a_dir[A], 1, n1[A], n1[A], n1[A]))
-                fold_parts.append(mk(ta_ptr[k[A]], uf_p, ci_p[A], a_ex[A], 1, n1[A], n1[A], n1[A]))
-                fold_parts.append(mk(bx_ptr[k[A]], cf_p[A], ui_p, b_ex[A], 2, nb[A], N, nb[A]))
+                nA = int(A.sum())
+                A_parts.append((np.full(nA, ti), pidx[A], k[A], a_dir[A], a_ex[A], b_ex[A], n1[A], nb[A],
+                                np.full(nA, uf_p, dtype=np.uint64), np.full(nA, ui_p, dtype=np.uint64), fo[A]))
                 forms["r"][fo[A]], forms["a"][fo[A]], forms["b"][fo[A]] = r_ptr, a_dir[A], b_full
                 forms["n_rows"][fo[A]], forms["n_cols"][fo[A]] = n1[A], N
                 forms["r"][fo[A] + 1], forms["a"][fo[A] + 1], forms["b"][fo[A] + 1] = r_ptr, a_ex[A], b_ex[A]
@@ -550,10 +566,49 @@ class PreparedJob:
                 forms["n_rows"][fo[C]], forms["n_cols"][fo[C]] = n1[C], n1[C]
                 forms["r"][fo[C] + 1], forms["a"][fo[C] + 1], forms["b"][fo[C] + 1] = r_ptr, a_ex[C], b_ex[C]
                 forms["n_rows"][fo[C] + 1], forms["n_cols"][fo[C] + 1] = n1[C], n1[C]
+        # node-set branch: one multi-fold per (pair, node set) and operator -- T with g = chi_i for
+        # a_dir (f = chi_f) and a_ex of every transition (f = u_f), B with g = chi_f for b_ex of every
+        # transition (f = u_i); a_dir no longer depends on the transition, so its direct forms share it
+        multi = np.zeros(0, dtype=_lib.FOLD_MULTI_DTYPE)
+        if A_parts:
+            cols = [np.concatenate(c) for c in zip(*A_parts)]
+            t_a, p_a, k_a, adir_a, aex_a, bex_a, n1_a, nb_a, uf_a, ui_a, fo_a = cols
+            order = np.lexsort((t_a, k_a, p_a))
+            t_a, p_a, k_a, adir_a, aex_a, bex_a, n1_a, nb_a, uf_a, ui_a, fo_a = (c[order] for c in cols)
+            n = len(p_a)
+            new_run = np.ones(n, dtype=bool)
+            new_run[1:] = (p_a[1:] != p_a[:-1]) | (k_a[1:] != k_a[:-1])
+            run_start = np.maximum.accumulate(np.where(new_run, np.arange(n), 0))
+            pos_run = np.arange(n) - run_start
+            per = _lib.FOLD_MULTI - 1  # transitions per group (one f slot of T holds a_dir)
+            new_grp = new_run | (pos_run % per == 0)
+            gid = np.cumsum(new_grp) - 1
+            G = int(gid[-1]) + 1
+            first = np.nonzero(new_grp)[0]
+            pos = np.arange(n) - first[gid]
+            cnt = np.bincount(gid, minlength=G)
+            mT = np.zeros(G, dtype=_lib.FOLD_MULTI_DTYPE)
+            mB = np.zeros(G, dtype=_lib.FOLD_MULTI_DTYPE)
+            pf, kf = p_a[first], k_a[first]
+            mT["op"], mT["g"] = ta_ptr[kf], ci_p[pf]
+            mT["f"][:, 0], mT["out"][:, 0] = cf_p[pf], adir_a[first]
+            mT["f"][gid, 1 + pos], mT["out"][gid, 1 + pos] = uf_a, aex_a
+            mT["n_f"], mT["half_band"] = 1 + cnt, 1
+            mT["n_out"] = mT["n_src"] = mT["n_clear"] = n1_a[first]
+            mB["op"], mB["g"] = bx_ptr[kf], cf_p[pf]
+            mB["f"][gid, pos], mB["out"][gid, pos] = ui_a, bex_a
+            mB["n_f"], mB["half_band"] = cnt, 2
+            mB["n_out"], mB["n_src"], mB["n_clear"] = nb_a[first], N, nb_a[first]
+            forms["a"][fo_a] = adir_a[first][gid]
+            multi = np.concatenate([mT, mB])
+        self.multi_host = multi
+        self.n_multi = len(multi)
+        self.multi_d = _dev(multi.view(np.uint8), dev) if len(multi) else None
         folds = np.concatenate(fold_parts)
         nf = len(folds)
         self.n_folds = nf
         self.folds_host = folds
+        self.fold_singles = np.concatenate([folds, expand_multi(multi)])
         self.folds_d = _dev(folds.view(np.uint8), dev)
         self.ops, self.wl_cache = ops, wl_cache
         # 4. bilinear form descriptors
@@ -624,6 +679,10 @@ class PreparedJob:
             n = min(65535, nf - s0)
             _lib.check(lib.dwba_fold(_ptr(self.folds_d) + s0 * _lib.FOLD_DTYPE.itemsize, n, self.job.grid.N,
                                      _stream()), "dwba_fold")
+        for s0 in range(0, self.n_multi, 65535):
+            n = min(65535, self.n_multi - s0)
+            _lib.check(lib.dwba_fold_multi(_ptr(self.multi_d) + s0 * _lib.FOLD_MULTI_DTYPE.itemsize, n,
+                                           self.job.grid.N, _stream()), "dwba_fold_multi")
 
     def launch_forms_direct(self) -> None:
         """Tensor-core engines: the direct forms share b per transition and use the exact FP64 O(N L) form."""
@@ -682,11 +741,17 @@ class PreparedJob:
         return float(np.sum(2.0 * f["n_rows"].astype(np.float64) * f["n_cols"])) * self.nl
 
     def fold_bytes(self) -> float:
-        """Bytes the folds must move: (2h+1) operator taps per output row, f and g over n_src,
-        the outputs over n_clear."""
+        """Bytes the folds must move: (2h+1) operator taps per output row, the factors over n_src,
+        the outputs over n_clear (a multi-fold reads its operator and shared factor once)."""
         f = self.folds_host
         taps = (2.0 * f["half_band"].astype(np.float64) + 1.0) * f["n_out"]
-        return float(np.sum(8.0 * (taps + 2.0 * f["n_src"] + f["n_clear"])))
+        b = float(np.sum(8.0 * (taps + 2.0 * f["n_src"] + f["n_clear"])))
+        m = self.multi_host
+        if len(m):
+            taps = (2.0 * m["half_band"].astype(np.float64) + 1.0) * m["n_out"]
+            nf = m["n_f"].astype(np.float64)
+            b += float(np.sum(8.0 * (taps + (1.0 + nf) * m["n_src"] + nf * m["n_clear"])))
+        return b
 
     def algorithmic_bytes(self) -> float:
         """Operand bytes of the semiseparable evaluation: a, b and r read once per form."""
@@ -754,6 +819,9 @@ class MultiPrepared:
         folds = np.concatenate([p.folds_host for p in parts])
         self.n_folds = len(folds)
         self.folds_d = _dev(folds.view(np.uint8), dev)
+        multi = np.concatenate([p.multi_host for p in parts])
+        self.n_multi = len(multi)
+        self.multi_d = _dev(multi.view(np.uint8), dev) if len(multi) else None
         forms = np.concatenate([p.forms_host for p in parts])
         self.n_forms = len(forms)
         self.forms_host = forms
@@ -793,6 +861,10 @@ class MultiPrepared:
             n = min(65535, self.n_folds - s0)
             _lib.check(lib.dwba_fold(_ptr(self.folds_d) + s0 * _lib.FOLD_DTYPE.itemsize, n, self.max_grid, st),
                        "dwba_fold")
+        for s0 in range(0, self.n_multi, 65535):
+            n = min(65535, self.n_multi - s0)
+            _lib.check(lib.dwba_fold_multi(_ptr(self.multi_d) + s0 * _lib.FOLD_MULTI_DTYPE.itemsize, n,
+                                           self.max_grid, st), "dwba_fold_multi")
         if self.engine == "dense":
             _lib.check(lib.dwba_bilinear_dense_fp64(_ptr(self.forms_d), self.n_forms, self.L_max, self.ds.ctypes.data,
                                                     _ptr(self.prefix_d), self.n_cta, _ptr(self.partial),

@@ -97,6 +97,28 @@ typedef struct {
 
 int dwba_fold(const dwba_fold_t* folds_dev, int n_folds, int max_rows, dwba_stream_t stream);
 
+/* Several folds that share the operator and the second factor, in one pass:
+ *   out_t[i] = sum_{d=-h..h} op[(2h+1)*i + d+h] * f_t[i+d] * g[i+d],  t < n_f <= DWBA_FOLD_MULTI,
+ * with the same n_out / n_src / n_clear rules as dwba_fold. The node-set operator and the
+ * continuum wave are read once for every transition of a pair (a_dir with a_ex of each
+ * transition; b_ex of each transition). Same products as dwba_fold (the reference's densities,
+ * dwba_matrix_elements.py:1028-1046). */
+#define DWBA_FOLD_MULTI 8
+typedef struct {
+  const double* op_dev;
+  const double* g_dev;
+  const double* f_dev[DWBA_FOLD_MULTI];
+  double* out_dev[DWBA_FOLD_MULTI];
+  int32_t n_f;
+  int32_t half_band;
+  int32_t n_out;
+  int32_t n_src;
+  int32_t n_clear;
+  int32_t pad;
+} dwba_fold_multi_t;
+
+int dwba_fold_multi(const dwba_fold_multi_t* folds_dev, int n_folds, int max_rows, dwba_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Bilinear forms in FP64: for each form f and L = 0..L_max,
  *   out[f*(L_max+1) + L] = sum_{i<n_rows} sum_{j<n_cols} a_i K_L(r_i, r_j) b_j.
@@ -241,7 +263,8 @@ int dwba_abi_version(void);
 const char* dwba_status_string(int status);
 int dwba_device_probe(int* n_devices, int* cc_major, int* cc_minor);
 /* sizeof(dwba_nodeset_t), sizeof(dwba_fold_t), sizeof(dwba_form_t), sizeof(dwba_tail_t),
- * sizeof(dwba_form_grad_t), sizeof(dwba_fold_adj_t) into sizes[0..5] (the first n of them). */
+ * sizeof(dwba_form_grad_t), sizeof(dwba_fold_adj_t), sizeof(dwba_fold_multi_t) into
+ * sizes[0..6] (the first n of them). */
 int dwba_struct_sizes(int64_t* sizes, int n);
 
 #ifdef __cplusplus

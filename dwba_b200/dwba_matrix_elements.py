@@ -187,6 +187,20 @@ def _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f
                tails_on_device=os.environ.get("DWBA_B200_TAILS", "device").strip().lower() != "host")
 
 
+def _results(I_dir: np.ndarray, I_exc: np.ndarray):
+    """(T, P, L_max+1) arrays -> results[t][p] as RadialDWBAIntegrals of Python floats."""
+    import gc
+    d, e = I_dir.tolist(), I_exc.tolist()
+    enabled = gc.isenabled()
+    gc.disable()  # many small containers: skip collector passes while they are made
+    try:
+        return [[RadialDWBAIntegrals(I_L_direct=dict(enumerate(dp)), I_L_exchange=dict(enumerate(ep)))
+                 for dp, ep in zip(dt, et)] for dt, et in zip(d, e)]
+    finally:
+        if enabled:
+            gc.enable()
+
+
 def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, gpu_cache, engine):
     """Evaluate a job; returns results[t][p] (a list of RadialDWBAIntegrals per transition)."""
     if not HAS_CUPY:
@@ -210,9 +224,7 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
             I_dir, I_exc = pj.collect()
         else:
             I_dir, I_exc = run_job(job, cache.dg, engine=eng)
-    return [[RadialDWBAIntegrals(I_L_direct={L: float(I_dir[t, p, L]) for L in range(L_max + 1)},
-                                 I_L_exchange={L: float(I_exc[t, p, L]) for L in range(L_max + 1)})
-             for p in range(len(pairs))] for t in range(I_dir.shape[0])]
+    return _results(I_dir, I_exc)
 
 
 def radial_ME_all_L(grid, V_core_array, U_i_array, bound_i, bound_f, cont_i, cont_f, L_max: int,
@@ -316,8 +328,6 @@ def radial_ME_all_L_sweep(points: Sequence[dict], L_max: int, engine: Optional[s
     outs = mp.collect()
     results = []
     for (I_dir, I_exc), multi, pt in zip(outs, shapes, points):
-        per_t = [[RadialDWBAIntegrals(I_L_direct={L: float(I_dir[t, p, L]) for L in range(L_max + 1)},
-                                      I_L_exchange={L: float(I_exc[t, p, L]) for L in range(L_max + 1)})
-                  for p in range(I_dir.shape[1])] for t in range(I_dir.shape[0])]
+        per_t = _results(I_dir, I_exc)
         results.append(per_t if multi else per_t[0])
     return results

@@ -94,13 +94,30 @@ class NodeSetBatch:
         self.ccx, self.ccw = CCTables.get(n_cc, dev)
         recs = np.zeros(len(todo), dtype=_lib.NODESET_DTYPE)
         self.keep = []
+        # operators of the sets not cached yet: views of one allocation (one allocator call per batch)
+        fresh = [p for p in todo if p.key not in dg.nodesets]
+        sizes = [3 * p.key.n1 + 5 * N for p in fresh]
+        block = torch.empty(int(sum(sizes)), dtype=torch.float64, device=dev) if fresh else None
+        offs = dict(zip([p.key for p in fresh], np.cumsum([0] + sizes[:-1]).tolist())) if fresh else {}
+        # Coulomb breakpoint lists (eta != 0) of every set: one upload, views per set
+        with_br = [p for p in todo if p.breaks is not None]
+        br_all = _dev(np.concatenate([np.asarray(p.breaks, dtype=np.float64) for p in with_br]), dev) \
+            if with_br else None
+        br_off, o_br = {}, 0
+        for p in with_br:
+            br_off[id(p)] = o_br
+            o_br += len(p.breaks)
+        self.keep.append(br_all)
         for i, p in enumerate(todo):
             old = dg.nodesets.get(p.key)
-            ta = old.ta if old is not None else torch.empty(3 * p.key.n1, dtype=torch.float64, device=dev)
-            bx = old.bx if old is not None else torch.empty(5 * N, dtype=torch.float64, device=dev)
-            br = _dev(p.breaks, dev) if p.breaks is not None else None
-            self.keep.append(br)
-            recs[i] = (_ptr(dg.r), _ptr(dg.logr), _ptr(br), _ptr(ta), _ptr(bx), N, p.key.n1, p.n_breaks,
+            if old is not None:
+                ta, bx = old.ta, old.bx
+            else:
+                o = int(offs[p.key])
+                ta = block.narrow(0, o, 3 * p.key.n1)
+                bx = block.narrow(0, o + 3 * p.key.n1, 5 * N)
+            br_ptr = (_ptr(br_all) + 8 * br_off[id(p)]) if p.breaks is not None else 0
+            recs[i] = (_ptr(dg.r), _ptr(dg.logr), br_ptr, _ptr(ta), _ptr(bx), N, p.key.n1, p.n_breaks,
                        int(p.log1), int(p.log2), 0)
             dg.nodesets[p.key] = DeviceNodeSet(p, ta, bx, 8 * (3 * p.key.n1 + 5 * N))
         self.recs = recs
@@ -274,19 +291,54 @@ class WaveMatrix:
                 else np.zeros((1, self.N))
         return self._m
 
+    @staticmethod
+    def _row_of(a: np.ndarray, N: int):
+        """(base, row) when ``a`` is a full row of a C-contiguous float64 2-D host matrix, else None."""
+        b = a.base
+        if (b is None or not isinstance(b, np.ndarray) or b.ndim != 2 or b.dtype != np.float64 or
+                not b.flags.c_contiguous or b.shape[1] < N or a.dtype != np.float64 or a.ndim != 1 or
+                a.strides != (8,)):
+            return None
+        off = a.__array_interface__["data"][0] - b.__array_interface__["data"][0]
+        rb = 8 * b.shape[1]
+        if off % rb != 0:
+            return None
+        return b, off // rb
+
     def upload(self, device) -> torch.Tensor:
-        """Copy every row to the device. Rows that are consecutive rows of one C-contiguous
-        host block are copied as one block (pinned when the caller's memory is pinned)."""
+        """Copy every row to the device. Rows taken from one C-contiguous host matrix (in any
+        order) are copied with that matrix in one transfer (asynchronous when it is pinned) and
+        gathered on the device; other rows that are consecutive in memory go as one block."""
         N = self.N
         out = torch.empty((max(1, len(self.arrays)), N), dtype=torch.float64, device=device)
-        i = 0
         n = len(self.arrays)
+        done = np.zeros(n, dtype=bool)
+        groups: Dict[int, list] = {}
+        for i, a in enumerate(self.arrays):
+            rb = self._row_of(a, N)
+            if rb is not None:
+                groups.setdefault(id(rb[0]), [rb[0], [], []])
+                groups[id(rb[0])][1].append(i)
+                groups[id(rb[0])][2].append(rb[1])
+        for base, idx, rows in groups.values():
+            if len(idx) < 2 or 2 * len(set(rows)) < base.shape[0]:
+                continue  # a small share of a large matrix: per-row copies below
+            src = torch.from_numpy(base)
+            dev_base = src.to(device, non_blocking=src.is_pinned())
+            sel = torch.as_tensor(np.asarray(rows, dtype=np.int64), device=device)
+            out[torch.as_tensor(np.asarray(idx, dtype=np.int64), device=device)] = \
+                dev_base.index_select(0, sel)[:, :N]
+            done[idx] = True
+        i = 0
         while i < n:
+            if done[i]:
+                i += 1
+                continue
             a = self.arrays[i]
             p0 = a.__array_interface__["data"][0]
             j = i + 1
             ok = a.flags.c_contiguous and a.dtype == np.float64 and len(a) == N
-            while ok and j < n:
+            while ok and j < n and not done[j]:
                 b = self.arrays[j]
                 if not (b.flags.c_contiguous and b.dtype == np.float64 and len(b) == N and
                         b.__array_interface__["data"][0] == p0 + 8 * N * (j - i)):
@@ -372,11 +424,11 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
         # distinct node sets of this transition (pairs of one energy share k_total and eta)
         cand = np.nonzero(osc & (n1 >= 2))[0]
         if len(cand):
-            keys = np.rec.fromarrays([n1[cand], k_total[cand], d[cand], eta_total[cand]])
-            uk, inv = np.unique(keys, return_inverse=True)
+            keys = np.stack([n1[cand].astype(np.float64), k_total[cand], d[cand], eta_total[cand]], axis=1)
+            uk, inv = np.unique(keys, axis=0, return_inverse=True)
             pos = np.empty(len(uk), dtype=np.int64)
-            for u, rec in enumerate(uk):
-                key = NodeSetKey(id(g), int(rec[0]), float(rec[1]), float(rec[2]), float(rec[3]), int(job.CC_nodes))
+            for u, rec in enumerate(uk.tolist()):
+                key = NodeSetKey(id(g), int(rec[0]), rec[1], rec[2], rec[3], int(job.CC_nodes))
                 q = ns_pos.get(key)
                 if q is None:
                     nsp = plan_nodeset(g, key)

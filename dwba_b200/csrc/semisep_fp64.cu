@@ -6,15 +6,14 @@
 // B_L(p) = sum_{q<p} Y_q r_q^L:
 //   I_L = sum_p r_p^-(L+1) (X_p B_L(p) + Y_p A_L(p)) + sum_p X_p Y_p (1-1e-12)^L / r_p,
 // the same identity the reference uses for Hartree potentials
-// (distorting_potential.py:235-251). One CTA per form: each thread owns a
-// contiguous segment, segment totals are scanned in shared memory, then every
-// thread sweeps its segment again with its running prefix.
+// (distorting_potential.py:235-251). One CTA per form and one pass over the operands:
+// each thread owns a contiguous segment (see semisep_kernel).
 #include "common.cuh"
 
 namespace {
 
-constexpr int THREADS = 128;  // 2*16*(128+1) doubles of scan storage stay under 48 KB
-constexpr int NL_MAX = 16;
+constexpr int THREADS = 128;
+constexpr int NL_MAX = 9;  // multipoles per launch (5 accumulators each per thread)
 
 struct DiagScale {
   double v[DWBA_MAX_L + 1];
@@ -30,103 +29,79 @@ __device__ __forceinline__ double ipow(double x, int e) {
   return r;
 }
 
+// Single pass over the operands. Thread s owns a contiguous segment and accumulates, per L,
+//   TA = sum X r^L, TB = sum Y r^L          (segment totals)
+//   SX = sum X r^-(L+1), SY = sum Y r^-(L+1)
+//   LOC = sum r_p^-(L+1) (X_p B_loc(p) + Y_p A_loc(p))   (prefixes local to the segment)
+// and with the exclusive prefixes A0, B0 of TA, TB over the segments before it,
+//   I_L = sum_s [LOC_s + A0_s SY_s + B0_s SX_s] + sum_p X_p Y_p d_L / r_p.
+// The prefixes over segments come from warp shuffles and a per-warp table in shared memory.
 template <int NL>
 __global__ void __launch_bounds__(THREADS)
 semisep_kernel(const dwba_form_t* __restrict__ forms, int L0, int n_ltot, DiagScale ds, double* __restrict__ out) {
-  __shared__ double scan[2 * NL][THREADS + 1];
-  __shared__ double red[THREADS / 32][NL];
+  constexpr int NW = THREADS / 32;
+  __shared__ double wtot[2 * NL][NW];
+  __shared__ double red[NW][NL];
   const dwba_form_t F = forms[blockIdx.x];
   const int M = F.n_rows > F.n_cols ? F.n_rows : F.n_cols;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int seg = (M + THREADS - 1) / THREADS;
   const int p0 = tid * seg;
   const int p1 = min(M, p0 + seg);
 
-  // pass 1: segment totals of X r^L and Y r^L
-  double sa[NL], sb[NL];
+  double A[NL], B[NL], SX[NL], SY[NL], LOC[NL];
 #pragma unroll
-  for (int l = 0; l < NL; ++l) sa[l] = sb[l] = 0.0;
-  for (int p = p0; p < p1; ++p) {
-    const double X = p < F.n_rows ? F.a_dev[p] : 0.0;
-    const double Y = p < F.n_cols ? F.b_dev[p] : 0.0;
-    const double r = F.r_dev[p];
-    double pw = L0 > 0 ? ipow(r, L0) : 1.0;
-#pragma unroll
-    for (int l = 0; l < NL; ++l) {
-      sa[l] += X * pw;
-      sb[l] += Y * pw;
-      pw *= r;
-    }
-  }
-#pragma unroll
-  for (int l = 0; l < NL; ++l) {
-    scan[l][tid + 1] = sa[l];
-    scan[NL + l][tid + 1] = sb[l];
-  }
-  __syncthreads();
-  if (tid < 2 * NL) {  // exclusive scan over the segments, one thread per series
-    double s = 0.0;
-    scan[tid][0] = 0.0;
-    for (int k = 1; k <= THREADS; ++k) {
-      s += scan[tid][k];
-      scan[tid][k] = s;
-    }
-  }
-  __syncthreads();
-  double A[NL], B[NL], acc[NL];
-#pragma unroll
-  for (int l = 0; l < NL; ++l) {
-    A[l] = scan[l][tid];
-    B[l] = scan[NL + l][tid];
-    acc[l] = 0.0;
-  }
-  // pass 2: sweep with running prefixes; two elements per iteration so their power chains
-  // overlap. The diagonal term sum_p X_p Y_p / r_p is collected once and scaled per L at the end.
+  for (int l = 0; l < NL; ++l) A[l] = B[l] = SX[l] = SY[l] = LOC[l] = 0.0;
   double dsum = 0.0;
-  int p = p0;
-  for (; p + 1 < p1; p += 2) {
-    const double X0 = p < F.n_rows ? F.a_dev[p] : 0.0, X1 = p + 1 < F.n_rows ? F.a_dev[p + 1] : 0.0;
-    const double Y0 = p < F.n_cols ? F.b_dev[p] : 0.0, Y1 = p + 1 < F.n_cols ? F.b_dev[p + 1] : 0.0;
-    const double r0 = F.r_dev[p], r1 = F.r_dev[p + 1];
-    const double i0 = 1.0 / r0, i1 = 1.0 / r1;
-    double pw0 = L0 > 0 ? ipow(r0, L0) : 1.0, pw1 = L0 > 0 ? ipow(r1, L0) : 1.0;
-    double ip0 = L0 > 0 ? ipow(i0, L0 + 1) : i0, ip1 = L0 > 0 ? ipow(i1, L0 + 1) : i1;
-    dsum += X0 * Y0 * i0;
-    dsum += X1 * Y1 * i1;
-#pragma unroll
-    for (int l = 0; l < NL; ++l) {
-      acc[l] += ip0 * fma(X0, B[l], Y0 * A[l]);
-      A[l] += X0 * pw0;
-      B[l] += Y0 * pw0;
-      acc[l] += ip1 * fma(X1, B[l], Y1 * A[l]);
-      A[l] += X1 * pw1;
-      B[l] += Y1 * pw1;
-      pw0 *= r0;
-      pw1 *= r1;
-      ip0 *= i0;
-      ip1 *= i1;
-    }
-  }
-  for (; p < p1; ++p) {
+  for (int p = p0; p < p1; ++p) {
     const double X = p < F.n_rows ? F.a_dev[p] : 0.0;
     const double Y = p < F.n_cols ? F.b_dev[p] : 0.0;
     const double r = F.r_dev[p];
     const double inv = 1.0 / r;
     double pw = L0 > 0 ? ipow(r, L0) : 1.0;
-    double ipw = L0 > 0 ? ipow(inv, L0 + 1) : inv;
+    double ip = L0 > 0 ? ipow(inv, L0 + 1) : inv;
     dsum += X * Y * inv;
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
-      acc[l] += ipw * fma(X, B[l], Y * A[l]);
+      LOC[l] += ip * fma(X, B[l], Y * A[l]);
+      SX[l] += ip * X;
+      SY[l] += ip * Y;
       A[l] += X * pw;
       B[l] += Y * pw;
       pw *= r;
-      ipw *= inv;
+      ip *= inv;
     }
   }
+  // exclusive prefix over segments of A and B (warp scan, then warp totals)
 #pragma unroll
-  for (int l = 0; l < NL; ++l) acc[l] += dsum * ds.v[L0 + l];
-  const int lane = tid & 31, warp = tid >> 5;
+  for (int l = 0; l < NL; ++l) {
+    double va = A[l], vb = B[l];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double ta = __shfl_up_sync(0xffffffffu, va, off), tb = __shfl_up_sync(0xffffffffu, vb, off);
+      if (lane >= off) {
+        va += ta;
+        vb += tb;
+      }
+    }
+    if (lane == 31) {
+      wtot[l][warp] = va;
+      wtot[NL + l][warp] = vb;
+    }
+    A[l] = va - A[l];  // exclusive within the warp
+    B[l] = vb - B[l];
+  }
+  __syncthreads();
+  double acc[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    double oa = 0.0, ob = 0.0;
+    for (int w = 0; w < warp; ++w) {
+      oa += wtot[l][w];
+      ob += wtot[NL + l][w];
+    }
+    acc[l] = LOC[l] + (A[l] + oa) * SY[l] + (B[l] + ob) * SX[l] + dsum * ds.v[L0 + l];
+  }
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
     double v = acc[l];
@@ -138,7 +113,7 @@ semisep_kernel(const dwba_form_t* __restrict__ forms, int L0, int n_ltot, DiagSc
   if (tid < NL) {
     double s = 0.0;
 #pragma unroll
-    for (int w = 0; w < THREADS / 32; ++w) s += red[w][tid];
+    for (int w = 0; w < NW; ++w) s += red[w][tid];
     out[(int64_t)blockIdx.x * n_ltot + L0 + tid] = s;
   }
 }
@@ -157,8 +132,7 @@ int launch_nl(int nl, const dwba_form_t* forms, int n_forms, int L0, int n_ltot,
 #define DWBA_CASE(N) \
   case N: return launch<N>(forms, n_forms, L0, n_ltot, ds, out, st);
     DWBA_CASE(1) DWBA_CASE(2) DWBA_CASE(3) DWBA_CASE(4) DWBA_CASE(5) DWBA_CASE(6) DWBA_CASE(7) DWBA_CASE(8)
-    DWBA_CASE(9) DWBA_CASE(10) DWBA_CASE(11) DWBA_CASE(12) DWBA_CASE(13) DWBA_CASE(14) DWBA_CASE(15)
-    DWBA_CASE(16)
+    DWBA_CASE(9)
 #undef DWBA_CASE
     default: return DWBA_ERR_INVALID_ARG;
   }

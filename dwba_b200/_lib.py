@@ -74,6 +74,8 @@ def _declare(lib):
         "dwba_bilinear_semisep_backward_fp64": (c_int, [c_vp, c_int, c_int, c_vp, c_vp, c_dbl, c_dbl, c_vp]),
         "dwba_fold_adjoint": (c_int, [c_vp, c_int, c_int, c_vp]),
         "dwba_fold_multi": (c_int, [c_vp, c_int, c_int, c_vp]),
+        "dwba_cross_sections": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_dbl,
+                                        c_vp, c_vp, c_vp]),
         "dwba_outer_tail_on_device": (c_int, [c_vp, c_dbl, c_dbl]),
     }
     for name, (res, args) in sig.items():

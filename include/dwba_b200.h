@@ -240,6 +240,15 @@ typedef struct {
 
 int dwba_fold_adjoint(const dwba_fold_adj_t* adj_dev, int n, int max_len, dwba_stream_t stream);
 
+/* Amplitudes -> DCS -> TCS for many partial-wave channels of one transition (replaces the
+ * per-channel loop of driver.py:1036-1052 over calculate_amplitude_contribution,
+ * dwba_coupling.py:285-505, and dcs_dwba / integrate_dcs_over_angles, sigma_total.py:147-217).
+ * cf, cg: complex (re, im) coefficient tables [n_M][P][nl]; yd, ye: angular factors
+ * [n_M][P][n_theta]; I_dir, I_exc: [P][nl]; dcs: [n_theta]; tcs: one value (may be NULL). */
+int dwba_cross_sections(const double* cf_dev, const double* cg_dev, const double* yd_dev, const double* ye_dev,
+                        const double* I_dir_dev, const double* I_exc_dev, const double* theta_dev, int n_M, int P,
+                        int nl, int n_theta, double pref, double* dcs_dev, double* tcs_dev, dwba_stream_t stream);
+
 /* Outer tails on the GPU, one warp per (record, L): the same quantity and formulas as
  * dwba_outer_tails (Filon / Levin segments split across the lanes, compensated lane sums).
  * Records whose mid-interval frequency is below 1e-10 take the reference's adaptive-quadrature

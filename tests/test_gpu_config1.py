@@ -68,3 +68,20 @@ def test_config1_fp64_integrals_match_reference(engine_results, engine):
     scale = np.max(np.abs(I_ref), axis=2, keepdims=True)
     ok = np.abs(engine_results[engine] - I_ref) <= 1e-12 * np.abs(I_ref) + 1e-13 * scale
     assert ok.all(), np.argwhere(~ok)[:5]
+
+
+def test_gpu_cross_sections_match_reference(engine_results):
+    """DCS/TCS on the device (dwba_cross_sections with the host coupling tables) from the reference's
+    integrals reproduce the reference's DCS and TCS; from each engine's integrals they stay within
+    that engine's tolerance (exact evaluation, no linearisation)."""
+    from dwba_b200.coupling import CouplingTables
+    tab = CouplingTables(Z["theta"], [tuple(p) for p in META["pairs"]], META["L_max"], META["k_i"], META["k_f"], 0, 1)
+    dcs, tcs = tab.cross_sections_gpu(Z["I_dir"], Z["I_exc"])
+    dcs = dcs.cpu().numpy()
+    assert np.all(np.abs(dcs - Z["dcs"]) <= 1e-11 * np.abs(Z["dcs"]) + 1e-14 * np.max(Z["dcs"]))
+    assert abs(float(tcs[0]) - float(Z["tcs"][0])) <= 1e-12 * float(Z["tcs"][0])
+    for eng, I in engine_results.items():
+        _, t = tab.cross_sections_gpu(I[0], I[1])
+        rel = abs(float(t[0]) - float(Z["tcs"][0])) / float(Z["tcs"][0])
+        print(f"{eng}: TCS through the device coupling, rel {rel:.2e}")
+        assert rel <= TCS_TOL[eng]

@@ -166,3 +166,35 @@ def test_fit_to_cross_section_recovers_parameters():
                                       max_iter=100, tol=1e-24)
     assert hist[-1] < 1e-14 * hist[0], hist[-5:]
     assert torch.allclose(beta, beta_true, rtol=1e-6, atol=1e-8), beta
+
+
+def test_gradients_config4_sizes():
+    """Config-4 sizes (N = 6000, L = 0..4) with the synthetic batch's waves and a live
+    L=0 correction (V_core != U_i): gradients of a random functional against central differences."""
+    import bench
+    from dwba_b200.autograd import RadialIntegrals
+    g, z, bounds, pairs = bench.make_workload(N=6000, n_cont=4, n_bound=1, seed_shift=44)
+    bi, bf = bounds[0]
+    r = np.asarray(g.r)
+    V = -1.0 / r
+    U = V + 0.3 * np.exp(-r)  # V_core - U_i != 0: the L=0 correction takes part
+    model = RadialIntegrals(g, bi, bf, pairs, 4, U_f_array=U, engine="semisep")
+    x = dict(V_core=_t(V), U_i=_t(U), u_i=_t(bi.u_of_r), u_f=_t(bf.u_of_r),
+             chi_i=_t(np.stack([p[0].chi_of_r for p in pairs])), chi_f=_t(np.stack([p[1].chi_of_r for p in pairs])))
+    rng = np.random.default_rng(45)
+    c = _t(rng.normal(size=(len(pairs), 2, 5)))
+    xs = {k: v.clone().requires_grad_(True) for k, v in x.items()}
+    loss = (model(**xs) * c).sum()
+    loss.backward()
+    for name in x:
+        v = _t(rng.normal(size=tuple(x[name].shape))) * x[name].abs()
+
+        def f(s):
+            y = dict(x)
+            y[name] = x[name] + s * v
+            with torch.no_grad():
+                return float((model(**y) * c).sum())
+        fd = (f(1e-6) - f(-1e-6)) / 2e-6
+        an = float((xs[name].grad * v).sum())
+        scale = float((xs[name].grad.abs() * v.abs()).sum()) + 1e-300
+        assert abs(fd - an) <= 1e-6 * scale + 1e-9 * abs(float(loss)), (name, fd, an, scale)

@@ -147,3 +147,30 @@ def test_semiseparable_overflow_guard():
     args[7] = 60  # (1e-5)^-(61) overflows FP64
     with pytest.raises(_lib.DWBAError):
         radial_ME_all_L(*args, **call["kwargs"], engine="semisep")
+
+
+def test_ionization_transitions_in_one_batch_equal_single_calls():
+    """Several ejected waves (one transition each, as one ejected energy of the reference's ionization
+    loop, ionization.py:526-608) with all (l_i, l_f) pairs in one batch: every (transition, pair)
+    equals the single call, and the golden ejected wave equals the reference."""
+    import dataclasses
+    from dwba_b200.dwba_matrix_elements import radial_ME_all_L, radial_ME_all_L_batch
+    common, calls = gc.load_case("h_ionization_100eV")
+    grid, V, Ui, bi, bf = common["grid"], common["V_core"], common["U_i"], common["bound_i"], common["bound_f"]
+    r = np.asarray(grid.r)
+    ejected = [bf] + [dataclasses.replace(bf, chi_of_r=bf.chi_of_r * (1.0 + s * np.exp(-r / 7.0)),
+                                          phase_shift=bf.phase_shift + 0.1 * s) for s in (0.3, -0.2)]
+    L_max = min(c["L_max"] for c in calls)
+    pairs = [(c["args"][5], c["args"][6]) for c in calls]
+    kw = dict(calls[0]["kwargs"])
+    batch = radial_ME_all_L_batch(grid, V, Ui, [bi] * len(ejected), ejected, pairs, L_max, **kw)
+    assert len(batch) == len(ejected) and all(len(b) == len(pairs) for b in batch)
+    for t, ej in enumerate(ejected):
+        for p, (ci, cf) in enumerate(pairs):
+            single = radial_ME_all_L(grid, V, Ui, bi, ej, ci, cf, L_max, **kw)
+            assert batch[t][p].I_L_direct == single.I_L_direct
+            assert batch[t][p].I_L_exchange == single.I_L_exchange
+    for p, c in enumerate(calls):
+        d = np.array([batch[0][p].I_L_direct[L] for L in range(L_max + 1)])
+        assert np.all(np.abs(d - c["ref_dir"][:L_max + 1]) <= 1e-11 * np.abs(c["ref_dir"][:L_max + 1]) +
+                      1e-13 * np.max(np.abs(c["ref_dir"])))

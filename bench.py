@@ -245,6 +245,8 @@ def main():
     ap.add_argument("--n-cont", type=int, default=N_CONT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip timing the split-BF16 and plain FP64 engines on the same batch")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -407,6 +409,33 @@ def main():
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "path": "radial_ME_all_L_batch (4 transitions x 2048 pairs) from pinned host NumPy inputs"}
 
+    # the same batch through the split-BF16 tensor-core form and the plain FP64 kernel (whole step,
+    # node sets rebuilt), so the line carries the split-BF16 vs FP64 comparison of the metric
+    compare = None
+    if rank == 0 and world == 1 and not args.no_compare:
+        def time_engine(eng, warm, reps):
+            pj = PreparedJob(job, cache.dg, eng, plans=preps[0].plans, rebuild_nodesets=True)
+            for _ in range(warm):
+                pj.launch()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(reps):
+                pj.launch()
+            e1.record(st)
+            e1.synchronize()
+            out = e0.elapsed_time(e1) / reps
+            del pj
+            torch.cuda.empty_cache()
+            return out
+        t_x3 = time_engine("tc_bf16x3", 2, 5)
+        t_dense = time_engine("dense", 1, 1)
+        compare = {"tc_bf16x3_ms_per_step": t_x3, "dense_fp64_ms_per_step": t_dense,
+                   "split_bf16_vs_plain_fp64_speedup": t_dense / t_x3,
+                   "semisep_fp64_ms_per_step": ms if args.engine == "semisep" else None,
+                   "note": "whole step (node sets, folds, forms) on the same batch; the accuracy of each engine "
+                           "against the reference's TCS is checked in tests/test_gpu_config1.py"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ips, dt, rows = cpu_sample(seconds_hint=15.0)
@@ -430,6 +459,7 @@ def main():
                            "engine": args.engine, "integrals_per_step_per_gpu": n_int,
                            "l2": "inputs larger than L2 (operands ~1 GB/step)", "parallelism": f"dp{world}"},
                 "split_ms": split, "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu,
+                "engines": compare,
                 "gpu_launches": n_launch * args.steps, "results_finite": bool(finite and nonzero), "clocks": clk.summary()}
         print(json.dumps(line))
     if world > 1:

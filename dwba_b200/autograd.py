@@ -141,7 +141,9 @@ class RadialIntegrals:
         self.pairs = list(pairs)
         self.L_max = int(L_max)
         self.U_f = U_f_array
-        self.engine = _engine_name(engine)
+        eng = _engine_name(engine)
+        # the autotuned names choose per call; the differentiable path uses one fixed forward engine
+        self.engine = {"auto": "semisep", "auto_split": "tc_bf16x3"}.get(eng, eng)
         self.cache = gpu_cache or GPUCache(grid)
         self.options = dict(use_oscillatory_quadrature=options.get("use_oscillatory_quadrature", True),
                             oscillatory_method=options.get("oscillatory_method", "advanced"),

@@ -187,20 +187,32 @@ def _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f
                tails_on_device=os.environ.get("DWBA_B200_TAILS", "device").strip().lower() != "host")
 
 
+def _no_gc(fn):
+    """Run ``fn`` with the cyclic garbage collector paused (a call allocates many small host
+    objects -- descriptors, keys, result dicts -- none of which form cycles), restoring its state."""
+    import functools
+    import gc
+
+    @functools.wraps(fn)
+    def wrapper(*args, **kwargs):
+        enabled = gc.isenabled()
+        gc.disable()
+        try:
+            return fn(*args, **kwargs)
+        finally:
+            if enabled:
+                gc.enable()
+    return wrapper
+
+
 def _results(I_dir: np.ndarray, I_exc: np.ndarray):
     """(T, P, L_max+1) arrays -> results[t][p] as RadialDWBAIntegrals of Python floats."""
-    import gc
     d, e = I_dir.tolist(), I_exc.tolist()
-    enabled = gc.isenabled()
-    gc.disable()  # many small containers: skip collector passes while they are made
-    try:
-        return [[RadialDWBAIntegrals(I_L_direct=dict(enumerate(dp)), I_L_exchange=dict(enumerate(ep)))
-                 for dp, ep in zip(dt, et)] for dt, et in zip(d, e)]
-    finally:
-        if enabled:
-            gc.enable()
+    return [[RadialDWBAIntegrals(I_L_direct=dict(enumerate(dp)), I_L_exchange=dict(enumerate(ep)))
+             for dp, ep in zip(dt, et)] for dt, et in zip(d, e)]
 
 
+@_no_gc
 def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, gpu_cache, engine):
     """Evaluate a job; returns results[t][p] (a list of RadialDWBAIntegrals per transition)."""
     if not HAS_CUPY:
@@ -278,6 +290,7 @@ def radial_ME_all_L_batch(grid, V_core_array, U_i_array, bound_i, bound_f,
     return res if multi else res[0]
 
 
+@_no_gc
 def radial_ME_all_L_sweep(points: Sequence[dict], L_max: int, engine: Optional[str] = None, graph: bool = False,
                           replays: int = 0, **options):
     """Many energy points in shared launches (new entry point; the reference loops over energies).

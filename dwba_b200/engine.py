@@ -60,10 +60,24 @@ class DeviceGrid:
 
 @dataclass
 class DeviceNodeSet:
+    """Operators of one node set: device addresses inside ``block`` (which keeps them alive)."""
     plan: NodeSetPlan
-    ta: torch.Tensor
-    bx: torch.Tensor
+    block: torch.Tensor
+    ta_ptr: int
+    bx_ptr: int
     nbytes: int
+
+    @property
+    def ta(self) -> torch.Tensor:
+        return self._view(self.ta_ptr, 3 * self.plan.key.n1)
+
+    @property
+    def bx(self) -> torch.Tensor:
+        return self._view(self.bx_ptr, (self.nbytes // 8) - 3 * self.plan.key.n1)
+
+    def _view(self, ptr: int, n: int) -> torch.Tensor:
+        off = (ptr - self.block.data_ptr()) // 8
+        return self.block.narrow(0, off, n)
 
 
 class CCTables:
@@ -92,34 +106,44 @@ class NodeSetBatch:
         if not todo:
             return
         self.ccx, self.ccw = CCTables.get(n_cc, dev)
-        recs = np.zeros(len(todo), dtype=_lib.NODESET_DTYPE)
+        n = len(todo)
         self.keep = []
-        # operators of the sets not cached yet: views of one allocation (one allocator call per batch)
-        fresh = [p for p in todo if p.key not in dg.nodesets]
-        sizes = [3 * p.key.n1 + 5 * N for p in fresh]
-        block = torch.empty(int(sum(sizes)), dtype=torch.float64, device=dev) if fresh else None
-        offs = dict(zip([p.key for p in fresh], np.cumsum([0] + sizes[:-1]).tolist())) if fresh else {}
-        # Coulomb breakpoint lists (eta != 0) of every set: one upload, views per set
-        with_br = [p for p in todo if p.breaks is not None]
-        br_all = _dev(np.concatenate([np.asarray(p.breaks, dtype=np.float64) for p in with_br]), dev) \
-            if with_br else None
-        br_off, o_br = {}, 0
-        for p in with_br:
-            br_off[id(p)] = o_br
-            o_br += len(p.breaks)
-        self.keep.append(br_all)
+        # operators of the sets not cached yet: one allocation for the batch, addresses by offset
+        fresh_mask = np.array([p.key not in dg.nodesets for p in todo], dtype=bool)
+        n1s = np.array([p.key.n1 for p in todo], dtype=np.int64)
+        sizes = np.where(fresh_mask, 3 * n1s + 5 * N, 0)
+        offs = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+        block = torch.empty(int(sizes.sum()), dtype=torch.float64, device=dev) if fresh_mask.any() else None
+        ta_p = np.zeros(n, dtype=np.uint64)
+        bx_p = np.zeros(n, dtype=np.uint64)
+        if block is not None:
+            base = np.uint64(_ptr(block))
+            ta_p[fresh_mask] = base + np.uint64(8) * offs[fresh_mask].astype(np.uint64)
+            bx_p[fresh_mask] = ta_p[fresh_mask] + np.uint64(8) * (3 * n1s[fresh_mask]).astype(np.uint64)
+        # Coulomb breakpoint lists (eta != 0) of every set: one upload, addresses by offset
+        br_len = np.array([0 if p.breaks is None else len(p.breaks) for p in todo], dtype=np.int64)
+        br_p = np.zeros(n, dtype=np.uint64)
+        if br_len.any():
+            br_all = _dev(np.concatenate([np.asarray(p.breaks, dtype=np.float64) for p in todo
+                                          if p.breaks is not None]), dev)
+            self.keep.append(br_all)
+            br_off = np.concatenate([[0], np.cumsum(br_len)[:-1]])
+            has = br_len > 0
+            br_p[has] = np.uint64(_ptr(br_all)) + np.uint64(8) * br_off[has].astype(np.uint64)
         for i, p in enumerate(todo):
-            old = dg.nodesets.get(p.key)
-            if old is not None:
-                ta, bx = old.ta, old.bx
+            if fresh_mask[i]:
+                dg.nodesets[p.key] = DeviceNodeSet(p, block, int(ta_p[i]), int(bx_p[i]),
+                                                   8 * (3 * p.key.n1 + 5 * N))
             else:
-                o = int(offs[p.key])
-                ta = block.narrow(0, o, 3 * p.key.n1)
-                bx = block.narrow(0, o + 3 * p.key.n1, 5 * N)
-            br_ptr = (_ptr(br_all) + 8 * br_off[id(p)]) if p.breaks is not None else 0
-            recs[i] = (_ptr(dg.r), _ptr(dg.logr), br_ptr, _ptr(ta), _ptr(bx), N, p.key.n1, p.n_breaks,
-                       int(p.log1), int(p.log2), 0)
-            dg.nodesets[p.key] = DeviceNodeSet(p, ta, bx, 8 * (3 * p.key.n1 + 5 * N))
+                old = dg.nodesets[p.key]
+                ta_p[i], bx_p[i] = old.ta_ptr, old.bx_ptr
+        recs = np.zeros(n, dtype=_lib.NODESET_DTYPE)
+        recs["r"], recs["logr"] = _ptr(dg.r), _ptr(dg.logr)
+        recs["breaks"], recs["ta"], recs["bx"] = br_p, ta_p, bx_p
+        recs["n_grid"], recs["n1"] = N, n1s
+        recs["n_breaks"] = np.array([p.n_breaks for p in todo], dtype=np.int32)
+        recs["log1"] = np.array([int(p.log1) for p in todo], dtype=np.int32)
+        recs["log2"] = np.array([int(p.log2) for p in todo], dtype=np.int32)
         self.recs = recs
         self.recs_d = _dev(recs.view(np.uint8), dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -421,9 +445,12 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
         n1 = _idx_limits(job, pa, t)
         n1_all[ti] = n1
         d = _dphis(job, n1, k_total, eta_total)
-        # distinct node sets of this transition (pairs of one energy share k_total and eta)
+        # distinct node sets of this transition (pairs of one energy share k_total and eta); a
+        # transition with the same integration limits as the previous one has the same node sets
         cand = np.nonzero(osc & (n1 >= 2))[0]
-        if len(cand):
+        if ti > 0 and np.array_equal(n1, n1_all[ti - 1]):
+            ns_index[ti] = ns_index[ti - 1]
+        elif len(cand):
             keys = np.stack([n1[cand].astype(np.float64), k_total[cand], d[cand], eta_total[cand]], axis=1)
             uk, inv = np.unique(keys, axis=0, return_inverse=True)
             pos = np.empty(len(uk), dtype=np.int64)
@@ -562,8 +589,9 @@ class PreparedJob:
                 wl_cache[n1] = t_
             return t_.data_ptr()
 
-        ta_ptr = np.array([dg.nodesets[ns.key].ta.data_ptr() for ns in plans.nodesets] + [0], dtype=np.uint64)
-        bx_ptr = np.array([dg.nodesets[ns.key].bx.data_ptr() for ns in plans.nodesets] + [0], dtype=np.uint64)
+        dns = [dg.nodesets[ns.key] for ns in plans.nodesets]
+        ta_ptr = np.array([d_.ta_ptr for d_ in dns] + [0], dtype=np.uint64)
+        bx_ptr = np.array([d_.bx_ptr for d_ in dns] + [0], dtype=np.uint64)
         w_ptr, r_ptr = np.uint64(_ptr(dg.w)), np.uint64(_ptr(dg.r))
         fold_parts, forms = [], np.zeros(2 * T * P, dtype=_lib.FORM_DTYPE)
         pidx = np.arange(P, dtype=np.int64)

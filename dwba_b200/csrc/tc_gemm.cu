@@ -35,8 +35,11 @@ constexpr int GEN_WARPS = 16;  // K_L tile generators: 4 x 32 rows x 4 column qu
 constexpr int GEN_THREADS = 32 * GEN_WARPS;
 constexpr int THREADS = 32 + GEN_THREADS;  // + warp 0: TMA and MMA issue
 constexpr int TC_BN2 = 256;  // forms per CTA with two terms
-constexpr int TC_STAGES = 3;  // pipeline stages (B tiles in shared memory, K_L tiles in tensor memory)
-constexpr int TMEM_COLS = 512;  // accumulator (BN columns) + TC_STAGES x NT K_L terms of BK/2 columns
+constexpr int TC_BN3 = 256;   // forms per CTA with three terms
+// pipeline stages (B tiles in shared memory, K_L tiles in tensor memory): 3 with two terms,
+// 2 with three (tensor memory: BN accumulator columns + S x NT x BK/2 K_L columns <= 512)
+__host__ __device__ constexpr int tc_stages(int nt) { return nt == 2 ? 3 : 2; }
+constexpr int TMEM_COLS = 512;
 constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz
 
 struct GemmParams {
@@ -203,7 +206,7 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
   constexpr int B_BYTES = BN * BK * 2;            // one term
   constexpr int STAGE = NT * B_BYTES;             // shared memory per stage
   constexpr int NPROD = NT == 2 ? 3 : 6;
-  constexpr int S = TC_STAGES;
+  constexpr int S = tc_stages(NT);
   constexpr int A_COLS = BK / 2;                  // tensor-memory columns of one K_L term
   static_assert(BN + S * NT * A_COLS <= TMEM_COLS, "tensor memory");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -581,7 +584,7 @@ int launch_tc(const GemmParams& P, const __nv_bfloat16* bterms, int n_L, cudaStr
                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) return DWBA_ERR_CUDA;
-  const int smem = TC_STAGES * NT * (BN * BK * 2) + 1024;
+  const int smem = tc_stages(NT) * NT * (BN * BK * 2) + 1024;
   if (cudaFuncSetAttribute(tc_exchange_kernel<NT, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
       cudaSuccess)
     return DWBA_ERR_CUDA;
@@ -595,7 +598,7 @@ int launch_tc(const GemmParams& P, const __nv_bfloat16* bterms, int n_L, cudaStr
 
 extern "C" int64_t dwba_tc_workspace_bytes(int n_forms, int n_grid, int L_max, int n_terms) {
   if (n_forms < 0 || n_grid < 2 || L_max < 0 || L_max > DWBA_MAX_L || (n_terms != 2 && n_terms != 3)) return -1;
-  const int bn = n_terms == 2 ? TC_BN2 : 128;
+  const int bn = n_terms == 2 ? TC_BN2 : TC_BN3;
   const int64_t n_pad = ((int64_t)n_grid + BK - 1) / BK * BK;
   const int64_t f_pad = ((int64_t)n_forms + bn - 1) / bn * bn;
   const int64_t n_iblk = ((int64_t)n_grid + BM - 1) / BM;
@@ -620,7 +623,7 @@ extern "C" int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, 
   const int64_t need = dwba_tc_workspace_bytes(n_forms, n_grid, L_max, n_terms);
   if (need < 0 || workspace_bytes < need) return DWBA_ERR_WORKSPACE;
   if (((uintptr_t)workspace & 255) != 0) return DWBA_ERR_INVALID_ARG;
-  const int bn = n_terms == 2 ? TC_BN2 : 128;
+  const int bn = n_terms == 2 ? TC_BN2 : TC_BN3;
   GemmParams P;
   P.n_grid = n_grid;
   P.n_pad = (n_grid + BK - 1) / BK * BK;
@@ -667,7 +670,7 @@ extern "C" int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, 
                                                                           bexp, bterms);
   DWBA_CHECK_LAUNCH();
   const int n_L = L_max + 1;
-  int rc = n_terms == 2 ? launch_tc<2, TC_BN2>(P, bterms, n_L, st) : launch_tc<3, 128>(P, bterms, n_L, st);
+  int rc = n_terms == 2 ? launch_tc<2, TC_BN2>(P, bterms, n_L, st) : launch_tc<3, TC_BN3>(P, bterms, n_L, st);
   if (rc != DWBA_OK) return rc;
   tc_reduce_kernel<<<dwba_grid_1d((int64_t)n_forms * n_L, 256), 256, 0, st>>>(P.partial, n_forms, P.f_pad,
                                                                             P.n_iblk, n_L, out_dev);

@@ -783,7 +783,7 @@ class PreparedJob:
         """(dense-equivalent, executed) tensor flops of the exchange forms per launch."""
         N = self.job.grid.N
         n_pad = (N + 63) // 64 * 64
-        bn = 256 if TC_TERMS[self.engine] == 2 else 128
+        bn = 256
         f_pad = (self.T * self.P + bn - 1) // bn * bn
         n_iblk = (N + 127) // 128
         prods = 3 if TC_TERMS[self.engine] == 2 else 6

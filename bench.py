@@ -31,6 +31,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
+WORKLOAD = ("synthetic kernel batch: N=15000 exp grid r in [1e-5,400], 2048 continuum pairs x 4 bound pairs "
+            "per GPU, L=0..8, direct+exchange")
 METRIC = "radial integrals/s (split-BF16 vs FP64, 1 B200) at <=1e-6 rel TCS error; ms per energy"
 N_GRID, R_MAX, N_CONT, N_BOUND, L_MAX = 15000, 400.0, 2048, 4, 8
 
@@ -223,8 +225,8 @@ def run_reference(args):
     line = {"metric": METRIC, "value": v, "unit": "integrals/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * 147456 / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "synthetic kernel batch N=15000 r<=400, 2048 continuum x 4 bound pairs, L<=8",
-                       "integrals_per_step": 147456},
+            "config": {"workload": WORKLOAD, "engine": "reference CPU algorithm (oracle port)",
+                       "integrals_per_step_per_gpu": 147456, "parallelism": "host"},
             "cpu_baseline": {"value": v, "unit": "integrals/s", "cores": cores, "kind": "port",
                              "sample": "oracle port of the reference CPU algorithm: row blocks of one pair at "
                                        "N=15000, L=0..8, direct+exchange, scaled by rows/n1"},
@@ -454,9 +456,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "integrals/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "bf16 split (x3/x6) + f64" if tc else "f64", "data": "synthetic",
-                "config": {"workload": "synthetic kernel batch: N=15000 exp grid r in [1e-5,400], "
-                                       "2048 continuum pairs x 4 bound pairs per GPU, L=0..8, direct+exchange",
-                           "engine": args.engine, "integrals_per_step_per_gpu": n_int,
+                "config": {"workload": WORKLOAD, "engine": args.engine, "integrals_per_step_per_gpu": n_int,
                            "l2": "inputs larger than L2 (operands ~1 GB/step)", "parallelism": f"dp{world}"},
                 "split_ms": split, "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu,
                 "engines": compare,

@@ -34,37 +34,39 @@ __global__ void fold_kernel(const dwba_fold_t* __restrict__ folds) {
 }
 
 template <int H>
-__device__ __forceinline__ void fold_multi_row(const dwba_fold_multi_t& m, int i) {
+__device__ __forceinline__ void fold_multi_row(const dwba_fold_multi_t* __restrict__ m, int n_f, int n_src, int i) {
   double tap[2 * H + 1], gv[2 * H + 1];
-  const double* __restrict__ op = m.op_dev + (int64_t)(2 * H + 1) * i;
+  const double* __restrict__ op = m->op_dev + (int64_t)(2 * H + 1) * i;
+  const double* __restrict__ g = m->g_dev;
 #pragma unroll
   for (int d = -H; d <= H; ++d) {
     const int k = i + d;
-    const bool in = k >= 0 && k < m.n_src;
+    const bool in = k >= 0 && k < n_src;
     tap[d + H] = in ? op[d + H] : 0.0;
-    gv[d + H] = in ? m.g_dev[k] : 0.0;
+    gv[d + H] = in ? g[k] : 0.0;
   }
-  for (int t = 0; t < m.n_f; ++t) {
-    const double* __restrict__ f = m.f_dev[t];
+  for (int t = 0; t < n_f; ++t) {
+    const double* __restrict__ f = m->f_dev[t];  // descriptor fields read from global memory
     double acc = 0.0;
 #pragma unroll
     for (int d = -H; d <= H; ++d) {
       const int k = i + d;
-      if (k >= 0 && k < m.n_src) acc += tap[d + H] * (f[k] * gv[d + H]);
+      if (k >= 0 && k < n_src) acc += tap[d + H] * (f[k] * gv[d + H]);
     }
-    m.out_dev[t][i] = acc;
+    m->out_dev[t][i] = acc;
   }
 }
 
 __global__ void fold_multi_kernel(const dwba_fold_multi_t* __restrict__ folds) {
-  const dwba_fold_multi_t m = folds[blockIdx.y];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n_clear; i += gridDim.x * blockDim.x) {
-    if (i < m.n_out) {
-      if (m.half_band == 0) fold_multi_row<0>(m, i);
-      else if (m.half_band == 1) fold_multi_row<1>(m, i);
-      else fold_multi_row<2>(m, i);
+  const dwba_fold_multi_t* __restrict__ m = folds + blockIdx.y;
+  const int n_f = m->n_f, H = m->half_band, n_out = m->n_out, n_src = m->n_src, n_clear = m->n_clear;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_clear; i += gridDim.x * blockDim.x) {
+    if (i < n_out) {
+      if (H == 0) fold_multi_row<0>(m, n_f, n_src, i);
+      else if (H == 1) fold_multi_row<1>(m, n_f, n_src, i);
+      else fold_multi_row<2>(m, n_f, n_src, i);
     } else {
-      for (int t = 0; t < m.n_f; ++t) m.out_dev[t][i] = 0.0;
+      for (int t = 0; t < n_f; ++t) m->out_dev[t][i] = 0.0;
     }
   }
 }

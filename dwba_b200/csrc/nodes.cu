@@ -74,10 +74,11 @@ __device__ __forceinline__ int interval_floor(const SetView& s, double x) {
 constexpr int ROWS_CTA = 32;
 __global__ void __launch_bounds__(ROWS_CTA, 24) nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets, const double* __restrict__ ccx_g,
                                     const double* __restrict__ ccw_g, int n_cc, int* status) {
-  __shared__ double ccx[MAX_CC], ccw[MAX_CC];
+  __shared__ double ccx[MAX_CC], ccw[MAX_CC], ccx1[MAX_CC];
   if (threadIdx.x < n_cc) {
     ccx[threadIdx.x] = ccx_g[threadIdx.x];
     ccw[threadIdx.x] = ccw_g[threadIdx.x];
+    ccx1[threadIdx.x] = rn_add(ccx_g[threadIdx.x], 1.0);
   }
   __syncthreads();
   const dwba_nodeset_t d = sets[blockIdx.y];
@@ -112,6 +113,10 @@ __global__ void __launch_bounds__(ROWS_CTA, 24) nodeset_rows_kernel(const dwba_n
     const double iB0 = recip(k - 1, s.log2), iB1 = recip(k, s.log2), iB2 = recip(k + 1, s.log2);
     const double iW0 = k >= 1 ? 1.0 / (r[k] - r[k - 1] + 1e-30) : 0.0;          // il = k-1
     const double iW1 = k + 1 <= N - 1 ? 1.0 / (r[k + 1] - r[k] + 1e-30) : 0.0;  // il = k
+    // grid values the nodes of this row can touch, held in registers
+    const double rk = r[k], rkm = k >= 1 ? r[k - 1] : 0.0, rkp = k + 1 <= N - 1 ? r[k + 1] : 0.0;
+    const double lk = s.lr[k], lkm = k >= 1 ? s.lr[k - 1] : 0.0, lkp = k + 1 <= N - 1 ? s.lr[k + 1] : 0.0;
+    const double r_first = r[0], r_lim = r[n1 - 1], r_last = r[N - 1];
     // nodes never leave [r0, r[n1-1]]; rows past n1+1 have none
     if (k <= n1 + 1) {
       // one interval earlier too: its top node can coincide with the window's lower end
@@ -124,27 +129,36 @@ __global__ void __launch_bounds__(ROWS_CTA, 24) nodeset_rows_kernel(const dwba_n
         if (!(width > 1e-12)) continue;
         const double hw = rn_mul(0.5, width);
         for (int sl = n_cc - 1; sl >= 0; --sl) {  // ascending positions within the interval
-          double x = rn_add(rn_mul(hw, rn_add(ccx[sl], 1.0)), a);
+          double x = rn_add(rn_mul(hw, ccx1[sl]), a);
           x = fmin(fmax(x, a), b);  // the top node can round one ulp past b
           if (x < wlo || x > whi) continue;
+          // kernel columns: searchsorted(r, x, 'left') within the window, clipped to [1, N-1]
+          int ir;
+          if (k >= 1 && x <= rkm) ir = k - 1;
+          else if (x <= rk) ir = k;
+          else ir = k + 1;
+          ir = ir < 1 ? 1 : (ir > N - 1 ? N - 1 : ir);
+          const int il = ir - 1;
+          const bool b_row = il == k || il == k - 1;
+          if (k >= n1 && !b_row) continue;  // reaches neither a T nor a B entry of this row
           const double w = rn_mul(ccw[sl], hw);
           // interpolation interval on r[:n] (np.interp after clipping; x is inside [r_{k-1}, r_{k+1}])
           const double lx = (s.log1 || s.log2) ? log(x) : 0.0;
           int jf;  // floor index in the full grid
-          if (k + 1 <= N - 1 && x >= r[k + 1]) jf = k + 1;
-          else if (x >= r[k]) jf = k;
+          if (k + 1 <= N - 1 && x >= rkp) jf = k + 1;
+          else if (x >= rk) jf = k;
           else jf = k - 1;
           // --- T rows: nodes with j1 in {k-1, k}
           if (k < n1) {
             int j1;
             double t1;
-            if (x <= r[0]) { j1 = 0; t1 = 0.0; }
-            else if (x >= r[n1 - 1]) { j1 = n1 - 2; t1 = 1.0; }
+            if (x <= r_first) { j1 = 0; t1 = 0.0; }
+            else if (x >= r_lim) { j1 = n1 - 2; t1 = 1.0; }
             else {
               j1 = jf > n1 - 2 ? n1 - 2 : jf;
               if (j1 == k || j1 == k - 1) {
                 const double inv = j1 == k ? iT1 : iT0;
-                t1 = s.log1 ? (lx - s.lr[j1]) * inv : (x - r[j1]) * inv;
+                t1 = s.log1 ? (lx - (j1 == k ? lk : lkm)) * inv : (x - (j1 == k ? rk : rkm)) * inv;
               } else {
                 t1 = 0.0;  // reaches no T entry of this row
               }
@@ -158,24 +172,19 @@ __global__ void __launch_bounds__(ROWS_CTA, 24) nodeset_rows_kernel(const dwba_n
             }
           }
           // --- B rows: nodes with il in {k-1, k}
-          int ir;  // searchsorted(r, x, 'left') within the window, then clipped to [1, N-1]
-          if (k >= 1 && x <= r[k - 1]) ir = k - 1;
-          else if (x <= r[k]) ir = k;
-          else ir = k + 1;
-          ir = ir < 1 ? 1 : (ir > N - 1 ? N - 1 : ir);
-          const int il = ir - 1;
-          if (il != k && il != k - 1) continue;
+          if (!b_row) continue;
           int j2;
           double t2;
-          if (x <= r[0]) { j2 = 0; t2 = 0.0; }
-          else if (x >= r[N - 1]) { j2 = N - 2; t2 = 1.0; }
+          if (x <= r_first) { j2 = 0; t2 = 0.0; }
+          else if (x >= r_last) { j2 = N - 2; t2 = 1.0; }
           else {
             j2 = jf > N - 2 ? N - 2 : jf;
             const int dj = j2 - k;  // -1, 0 or 1 inside the window
             const double inv = dj < 0 ? iB0 : (dj == 0 ? iB1 : iB2);
-            t2 = s.log2 ? (lx - s.lr[j2]) * inv : (x - r[j2]) * inv;
+            t2 = s.log2 ? (lx - (dj < 0 ? lkm : (dj == 0 ? lk : lkp))) * inv
+                        : (x - (dj < 0 ? rkm : (dj == 0 ? rk : rkp))) * inv;
           }
-          const double wr = (x - r[il]) * (il == k ? iW1 : iW0);
+          const double wr = (x - (il == k ? rk : rkm)) * (il == k ? iW1 : iW0);
           const double q = il == k ? 1.0 - wr : wr;
           const int d0 = j2 - k;
           if (d0 < -2 || d0 + 1 > 2) { bad = true; continue; }

@@ -205,6 +205,23 @@ def _no_gc(fn):
     return wrapper
 
 
+def _early_upload(job, device):
+    """The job's functions (continuum waves, bound pairs) as rows of one device matrix, copied before
+    the host planning so that a copy from pinned memory overlaps it; planning and preparation then
+    find them uploaded."""
+    from .engine import WaveMatrix
+    waves = WaveMatrix(job.grid.N)
+    for ci, _ in job.pairs:
+        waves.add(ci.chi_of_r)
+    for _, cf in job.pairs:
+        waves.add(cf.chi_of_r)
+    for t in job.transitions:
+        waves.add(t.u_i)
+        waves.add(t.u_f)
+    waves.upload(device)
+    return waves
+
+
 def _results(I_dir: np.ndarray, I_exc: np.ndarray):
     """(T, P, L_max+1) arrays -> results[t][p] as RadialDWBAIntegrals of Python floats."""
     d, e = I_dir.tolist(), I_exc.tolist()
@@ -220,14 +237,14 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
     import torch
     if not torch.cuda.is_available():
         raise RuntimeError("radial_ME_all_L: no CUDA device available (the B200 engine has no CPU fallback)")
-    from .engine import PreparedJob, plan_job, run_job
+    from .engine import PreparedJob, plan_job
     from . import tune
     cache = _cache_for(grid, gpu_cache)
     job = _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, cache)
     eng = _engine_name(engine)
     with torch.cuda.device(cache.device):
+        plans = plan_job(job, _early_upload(job, cache.device))
         if tune.is_auto(eng):
-            plans = plan_job(job)
             cands = tune.candidates(eng)
             key = tune.TUNER.key(cache.info.N, 2 * len(job.transitions) * len(job.pairs), L_max, cands)
             _, pj = tune.TUNER.select(key, cands, lambda e: PreparedJob(job, cache.dg, e, plans=plans),
@@ -235,7 +252,9 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
             pj.launch()
             I_dir, I_exc = pj.collect()
         else:
-            I_dir, I_exc = run_job(job, cache.dg, engine=eng)
+            pj = PreparedJob(job, cache.dg, eng, plans=plans)
+            pj.launch()
+            I_dir, I_exc = pj.collect()
     return _results(I_dir, I_exc)
 
 

@@ -298,15 +298,19 @@ class WaveMatrix:
         self.N = N
         self.idx: Dict[Tuple[int, int], int] = {}
         self.arrays: List[np.ndarray] = []
+        self.ptrs: List[int] = []
+        self._uploaded: Dict[str, Tuple[int, torch.Tensor]] = {}
 
     def add(self, arr: np.ndarray) -> int:
         a = np.asarray(arr)
-        key = (a.__array_interface__["data"][0], a.strides[0] if a.ndim else 0)
+        ptr = a.__array_interface__["data"][0]
+        key = (ptr, a.strides[0] if a.ndim else 0)
         i = self.idx.get(key)
         if i is None:
             i = len(self.arrays)
             self.idx[key] = i
             self.arrays.append(a[: self.N])
+            self.ptrs.append(ptr)
         return i
 
     def matrix(self) -> np.ndarray:
@@ -316,14 +320,18 @@ class WaveMatrix:
         return self._m
 
     @staticmethod
-    def _row_of(a: np.ndarray, N: int):
-        """(base, row) when ``a`` is a full row of a C-contiguous float64 2-D host matrix, else None."""
+    def _row_of(a: np.ndarray, N: int, ptr: int, base_ptrs: dict):
+        """(base, row) when ``a`` (data at ``ptr``) is a full row of a C-contiguous float64 2-D host
+        matrix, else None."""
         b = a.base
         if (b is None or not isinstance(b, np.ndarray) or b.ndim != 2 or b.dtype != np.float64 or
                 not b.flags.c_contiguous or b.shape[1] < N or a.dtype != np.float64 or a.ndim != 1 or
                 a.strides != (8,)):
             return None
-        off = a.__array_interface__["data"][0] - b.__array_interface__["data"][0]
+        bp = base_ptrs.get(id(b))
+        if bp is None:
+            bp = base_ptrs[id(b)] = b.__array_interface__["data"][0]
+        off = ptr - bp
         rb = 8 * b.shape[1]
         if off % rb != 0:
             return None
@@ -334,12 +342,16 @@ class WaveMatrix:
         order) are copied with that matrix in one transfer (asynchronous when it is pinned) and
         gathered on the device; other rows that are consecutive in memory go as one block."""
         N = self.N
-        out = torch.empty((max(1, len(self.arrays)), N), dtype=torch.float64, device=device)
         n = len(self.arrays)
+        cached = self._uploaded.get(str(device))
+        if cached is not None and cached[0] == n:
+            return cached[1]  # already on the device (no rows added since)
+        out = torch.empty((max(1, n), N), dtype=torch.float64, device=device)
         done = np.zeros(n, dtype=bool)
         groups: Dict[int, list] = {}
+        base_ptrs: Dict[int, int] = {}
         for i, a in enumerate(self.arrays):
-            rb = self._row_of(a, N)
+            rb = self._row_of(a, N, self.ptrs[i], base_ptrs)
             if rb is not None:
                 groups.setdefault(id(rb[0]), [rb[0], [], []])
                 groups[id(rb[0])][1].append(i)
@@ -376,6 +388,7 @@ class WaveMatrix:
                 src = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).reshape(1, N)
             out[i:j].copy_(src, non_blocking=src.is_pinned())
             i = j
+        self._uploaded[str(device)] = (n, out)
         return out
 
 

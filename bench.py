@@ -111,6 +111,90 @@ def make_workload(N=N_GRID, n_cont=N_CONT, n_bound=N_BOUND, seed_shift=0, pinned
     return g, zeros, bounds, pairs
 
 
+def make_ragged_points(n_energy=64, l_max_wave=40, r_max=200.0, seed=3):
+    """Ragged multi-energy sweep with the shapes of the He+ 1s->2s / 1s->2p study: energies
+    geomspace(45, 1000, n_energy) eV, one grid per energy with N_e = round(2000 * 7.5^(e/(n-1))) points,
+    l_i, l_f <= l_max_wave (parity-filtered per transition), Coulomb-like waves (z = 1: eta = -1/k,
+    matching index inside the grid, so n1 < N and the outer tails take part), hydrogenic Z = 2 bound
+    states. Synthetic (seeded) stand-ins for the reference's solver outputs. One point per
+    (energy, transition)."""
+    rng = np.random.default_rng(seed)
+    Z, hartree = 2.0, 27.211386245988
+    dE = {"2s": 0.75 * Z * Z / 2 * hartree, "2p": 0.75 * Z * Z / 2 * hartree}
+    points = []
+    energies = np.geomspace(45.0, 1000.0, n_energy)
+    for e, E in enumerate(energies):
+        N = int(round(2000 * 7.5 ** (e / max(1, n_energy - 1))))
+        g = make_grid(N, 1e-5, r_max)
+        r = g.r
+        u1s = 2.0 * Z ** 1.5 * r * np.exp(-Z * r)
+        bound = {"2s": (Z / 2) ** 1.5 / np.sqrt(2.0) * r * (2.0 - Z * r) * np.exp(-Z * r / 2),
+                 "2p": (Z / 2) ** 2.5 / np.sqrt(6.0) * r * r * np.exp(-Z * r / 2)}
+        k_i = np.sqrt(2.0 * E / hartree)
+        im = int(np.searchsorted(r, 0.6 * r_max))
+        for name, lf_par in (("2s", 0), ("2p", 1)):
+            k_f = np.sqrt(2.0 * (E - dE[name]) / hartree)
+
+            def wave(l, k):
+                eta = -1.0 / k
+                d, sig = float(rng.uniform(0, np.pi)), float(rng.uniform(-1, 1))
+                r0 = (l + 1) / k
+                chi = np.sin(k * r - 0.5 * l * np.pi + eta * np.log(2 * k * r) + sig + d) * \
+                    (1.0 - np.exp(-(r / r0) ** (l + 1)))
+                w = _Wave(l, k, d, chi)
+                w.eta, w.sigma_l, w.idx_match = eta, sig, im
+                return w
+            wi = [wave(l, k_i) for l in range(l_max_wave + 1)]
+            wf = [wave(l, k_f) for l in range(l_max_wave + 1)]
+            pairs = [(wi[a], wf[b]) for a in range(l_max_wave + 1) for b in range(l_max_wave + 1)
+                     if (a + b) % 2 == lf_par]
+            V = -Z / r
+            points.append(dict(grid=g, V_core_array=V, U_i_array=V, bound_i=_Bound(0, u1s),
+                               bound_f=_Bound(1 if name == "2p" else 0, bound[name]), pairs=pairs, U_f_array=V))
+    return points
+
+
+def ragged_sweep(engine, L_max=6, replays=5):
+    """Device time of the ragged sweep (node sets, folds, forms and tails of all points in shared
+    launches, replayed from a CUDA graph)."""
+    import torch
+    from dwba_b200.dwba_matrix_elements import GPUCache, _make_job
+    from dwba_b200.engine import MultiPrepared, PreparedJob
+    points = make_ragged_points()
+    kw = dict(use_oscillatory_quadrature=True, oscillatory_method="advanced", CC_nodes=5, phase_increment=1.5708,
+              min_grid_fraction=0.10, k_threshold=0.5)
+    parts = []
+    for pt in points:
+        cache = GPUCache(pt["grid"])
+        job = _make_job(pt["grid"], pt["V_core_array"], pt["U_i_array"], pt["bound_i"], pt["bound_f"], pt["pairs"],
+                        L_max, pt["U_f_array"], kw, cache)
+        parts.append(PreparedJob(job, cache.dg, engine, rebuild_nodesets=True))
+    mp = MultiPrepared(parts)
+    mp.capture()
+    mp.replay()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(replays):
+        mp.replay()
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / replays
+    outs = mp.collect()
+    finite = all(np.isfinite(d).all() and np.isfinite(e).all() for d, e in outs)
+    n_int = sum(2 * p.T * p.P * p.nl for p in parts)
+    n_energy = len(points) // 2
+    Ns = [len(pt["grid"].r) for pt in points]
+    return {"workload": f"ragged sweep: {n_energy} energies geomspace(45, 1000) eV, N_e = 2000..15000 "
+                        f"(own grid per energy), He+-like 1s->2s and 1s->2p, l <= 40 parity-filtered, L=0..{L_max}, "
+                        "Coulomb-like waves (eta = -1/k, n1 < N, outer tails on the device), synthetic",
+            "engine": engine, "energies": n_energy, "points": len(points), "N_min": min(Ns), "N_max": max(Ns),
+            "integrals": n_int, "ms_per_sweep": ms, "ms_per_energy": ms / n_energy,
+            "integrals_per_s": n_int / (ms * 1e-3), "graph": True, "replays": replays,
+            "tail_records": int(sum(p.n_tail for p in parts)), "results_finite": bool(finite)}
+
+
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
@@ -247,6 +331,7 @@ def main():
     ap.add_argument("--n-cont", type=int, default=N_CONT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ragged", action="store_true", help="skip the ragged multi-energy sweep")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip timing the split-BF16 and plain FP64 engines on the same batch")
     args = ap.parse_args()
@@ -438,6 +523,10 @@ def main():
                    "note": "whole step (node sets, folds, forms) on the same batch; the accuracy of each engine "
                            "against the reference's TCS is checked in tests/test_gpu_config1.py"}
 
+    ragged = None
+    if rank == 0 and world == 1 and not args.no_ragged and args.engine in ("semisep", "dense"):
+        ragged = ragged_sweep("semisep")
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ips, dt, rows = cpu_sample(seconds_hint=15.0)
@@ -459,7 +548,7 @@ def main():
                 "config": {"workload": WORKLOAD, "engine": args.engine, "integrals_per_step_per_gpu": n_int,
                            "l2": "inputs larger than L2 (operands ~1 GB/step)", "parallelism": f"dp{world}"},
                 "split_ms": split, "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu,
-                "engines": compare,
+                "engines": compare, "ragged_sweep": ragged,
                 "gpu_launches": n_launch * args.steps, "results_finite": bool(finite and nonzero), "clocks": clk.summary()}
         print(json.dumps(line))
     if world > 1:

@@ -1,4 +1,6 @@
-// Outer tails of the direct integral on the GPU: one warp per (pair, L), lanes over segments.
+// Outer tails of the direct integral on the GPU: one warp per (pair, chunk of up to 8 multipoles),
+// lanes over segments; each node's phase factor, each Filon panel's weights and each Levin
+// segment's factorised collocation system serve every multipole of the chunk.
 //
 // Same quantity and formulas as the host path (host.cpp, dwba_outer_tails), which follows
 // oscillatory_integrals.py: dwba_outer_integral_1d (:459-535) with
@@ -82,8 +84,6 @@ struct PhaseD {
   }
 };
 
-__device__ __forceinline__ double envelope(double m, int L, double r) { return r > 1e-6 ? m / pow(r, (double)(L + 1)) : 0.0; }
-
 // numpy.linspace(a, b, n)[i]
 __device__ __forceinline__ double lin(double a, double b, int n, int i) {
   if (i == n - 1) return b;
@@ -100,120 +100,191 @@ struct KSum {
   }
 };
 
-// Filon on one segment with nn equally spaced nodes (nn odd), _filon_segment_complex
-__device__ cplx filon_segment(double m, int L, double a, double b, int nn, double omega, double off) {
-  cplx res = {0.0, 0.0};
-  if (!(b - a >= 1e-15)) return res;
-  double xs[15], fs[15];
-  for (int i = 0; i < nn; ++i) {
-    xs[i] = lin(a, b, nn, i);
-    fs[i] = envelope(m, L, xs[i]);
-  }
-  if (fabs(omega * (b - a)) < 1e-3) {  // scipy simpson with possibly unequal spacing
-    double acc = 0.0;
-    for (int i = 0; i + 2 < nn; i += 2) {
-      const double h0 = xs[i + 1] - xs[i], h1 = xs[i + 2] - xs[i + 1];
-      const double hs = h0 + h1, hp = h0 * h1, q = h0 / h1;
-      acc += hs / 6.0 * (fs[i] * (2.0 - 1.0 / q) + fs[i + 1] * (hs * (hs / hp)) + fs[i + 2] * (2.0 - q));
-    }
-    return cscale(acc, cexpi(omega * (a + b) / 2 + off));
-  }
-  for (int i = 0; i + 2 < nn; i += 2) {
-    const double x0 = xs[i], x1 = xs[i + 1], x2 = xs[i + 2];
-    const double h = x2 - x0;
-    if (h < 1e-15) continue;
-    if (fabs(omega * h) < 1e-3) {  // the 3-node panel itself is non-oscillatory: Simpson times the mid phase
-      const double h0 = x1 - x0, h1 = x2 - x1;
-      const double hs = h0 + h1, hp = h0 * h1, q = h0 / h1;
-      const double v = hs / 6.0 * (fs[i] * (2.0 - 1.0 / q) + fs[i + 1] * (hs * (hs / hp)) + fs[i + 2] * (2.0 - q));
-      res = cadd(res, cscale(v, cexpi(omega * (x0 + x2) / 2 + off)));
-      continue;
-    }
-    const double th = omega * h / 2;
-    double st, ct;
-    sincos(th, &st, &ct);
-    double al, be, ga;
-    if (fabs(th) < 0.3) {
-      const double t2 = th * th, t3 = pow(th, 3.0);
-      al = 2 * t3 / 45 * (1 - t2 / 7 + (t2 * t2) / 189);
-      be = 2.0 / 3 + 2 * t2 / 15 - 4 * (t2 * t2) / 105 + 2 * pow(t2, 3.0) / 567;
-      ga = 4.0 / 3 - 2 * t2 / 15 + 1 * (t2 * t2) / 210 - pow(t2, 3.0) / 11340;
-    } else {
-      const double t2 = th * th, t3 = pow(th, 3.0);
-      double s2, c2;
-      sincos(2 * th, &s2, &c2);
-      al = (t2 + th * s2 / 2 - 2 * (st * st)) / t3;
-      be = 2 * (th * (1 + c2) - s2) / t3;
-      ga = 4 * (st - th * ct) / t3;
-    }
-    const cplx e0 = cexpi(omega * x0 + off), e1 = cexpi(omega * x1 + off), e2 = cexpi(omega * x2 + off);
-    const cplx mi = {0.0, -1.0 / omega};
-    const cplx d02 = csub(cscale(fs[i + 2], e2), cscale(fs[i], e0));
-    const cplx s02 = cadd(cscale(fs[i], e0), cscale(fs[i + 2], e2));
-    cplx t = cadd(cmul(cscale(al, mi), d02), cadd(cscale(be, s02), cscale(ga * fs[i + 1], e1)));
-    res = cadd(res, cscale(h / 2, t));
-  }
-  return res;
-}
-
 struct LevinD {
   double D[8][8];  // Chebyshev differentiation matrix of descending Lobatto points (reference convention)
   double xr[8];    // ascending reference nodes in [-1, 1]
 };
 
-// Levin collocation on one segment, _levin_segment_complex (8 nodes)
-__device__ cplx levin_segment(double m, int L, const PhaseD& ph, double a, double b, const LevinD& lv) {
-  cplx A[8][8], u[8];
-  double x[8];
-  for (int k = 0; k < 8; ++k) x[k] = 0.5 * (b - a) * (lv.xr[k] + 1) + a;
-  const double h = x[7] - x[0];
-  if (h < 1e-15) return {0.0, 0.0};
-  const double sc = 2.0 / h;
-  for (int i = 0; i < 8; ++i) {
-    for (int j = 0; j < 8; ++j) A[i][j] = {lv.D[i][j] * sc, 0.0};
-    A[i][i].im += ph.d1(x[i]);
-    u[i] = {envelope(m, L, x[i]), 0.0};
-  }
-  for (int k = 0; k < 8; ++k) {  // partial pivoting by |re| + |im|
-    int piv = k;
-    double best = -1.0;
-    for (int i = k; i < 8; ++i) {
-      const double mm = fabs(A[i][k].re) + fabs(A[i][k].im);
-      if (mm > best) { best = mm; piv = i; }
-    }
-    if (best == 0.0) return {0.0, 0.0};
-    if (piv != k) {
-      for (int j = 0; j < 8; ++j) { cplx t = A[k][j]; A[k][j] = A[piv][j]; A[piv][j] = t; }
-      cplx t = u[k]; u[k] = u[piv]; u[piv] = t;
-    }
-    const cplx inv = cdiv({1.0, 0.0}, A[k][k]);
-    for (int i = k + 1; i < 8; ++i) {
-      const cplx l = cmul(A[i][k], inv);
-      for (int j = k + 1; j < 8; ++j) A[i][j] = csub(A[i][j], cmul(l, A[k][j]));
-      u[i] = csub(u[i], cmul(l, u[k]));
-    }
-  }
-  for (int i = 7; i >= 0; --i) {
-    cplx s = u[i];
-    for (int j = i + 1; j < 8; ++j) s = csub(s, cmul(A[i][j], u[j]));
-    u[i] = cdiv(s, A[i][i]);
-  }
-  return csub(cmul(u[7], cexpi(ph.phi(x[7]))), cmul(u[0], cexpi(ph.phi(x[0]))));
-}
+__shared__ LevinD s_lv;  // the launch's Levin tables, staged once per block
 
 __device__ double warp_sum(double v) {
   for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
   return __shfl_sync(0xffffffffu, v, 0);
 }
 
-// one branch (cos(Phi_a -/+ Phi_b)) of the outer integral; Re part, summed over the warp
-__device__ double outer_branch(double m, int L, const PhaseD& ph, double rm, double rmax, int max_seg,
-                               double max_dphi, const LevinD& lv, int lane) {
+constexpr int LC = 8;  // multipoles evaluated together (one accumulator each per lane)
+
+// envelopes f_L(x) = m_L / x^(L+1) for L = L0 .. L0+nl-1 (zero where |m_L| <= 1e-12 or x <= 1e-6)
+__device__ __forceinline__ void envelopes(const double* m, int L0, int nl, double x, double* f) {
+  if (!(x > 1e-6)) {
+#pragma unroll
+    for (int q = 0; q < LC; ++q) f[q] = 0.0;
+    return;
+  }
+  const double inv = 1.0 / x;
+  double p = pow(inv, (double)(L0 + 1));
+#pragma unroll
+  for (int q = 0; q < LC; ++q) {
+    f[q] = q < nl ? m[q] * p : 0.0;
+    p *= inv;
+  }
+}
+
+// Re of the Filon integral over one segment (nn equally spaced nodes, nn odd) for every multipole
+// of the chunk: _filon_segment_complex with the node phases and the panel weights shared by all L
+__device__ void filon_segment_all(const double* m, int L0, int nl, double a, double b, int nn, double omega,
+                                  double off, KSum* acc) {
+  if (!(b - a >= 1e-15)) return;
+  double f0[LC], f1[LC], f2[LC];
+  if (fabs(omega * (b - a)) < 1e-3) {  // scipy simpson with possibly unequal spacing, times the mid phase
+    const double ce = cexpi(omega * (a + b) / 2 + off).re;
+    double part[LC];
+#pragma unroll
+    for (int q = 0; q < LC; ++q) part[q] = 0.0;
+    for (int i = 0; i + 2 < nn; i += 2) {
+      const double x0 = lin(a, b, nn, i), x1 = lin(a, b, nn, i + 1), x2 = lin(a, b, nn, i + 2);
+      const double h0 = x1 - x0, h1 = x2 - x1;
+      const double hs = h0 + h1, hp = h0 * h1, qq = h0 / h1;
+      envelopes(m, L0, nl, x0, f0);
+      envelopes(m, L0, nl, x1, f1);
+      envelopes(m, L0, nl, x2, f2);
+#pragma unroll
+      for (int q = 0; q < LC; ++q)
+        part[q] += hs / 6.0 * (f0[q] * (2.0 - 1.0 / qq) + f1[q] * (hs * (hs / hp)) + f2[q] * (2.0 - qq));
+    }
+#pragma unroll
+    for (int q = 0; q < LC; ++q) acc[q].add(part[q] * ce);
+    return;
+  }
+  double seg[LC];
+#pragma unroll
+  for (int q = 0; q < LC; ++q) seg[q] = 0.0;
+  double x0 = a;
+  cplx e0 = cexpi(omega * x0 + off);
+  envelopes(m, L0, nl, x0, f0);
+  for (int i = 0; i + 2 < nn; i += 2) {
+    const double x1 = lin(a, b, nn, i + 1), x2 = lin(a, b, nn, i + 2);
+    const double h = x2 - x0;
+    const cplx e1 = cexpi(omega * x1 + off), e2 = cexpi(omega * x2 + off);
+    envelopes(m, L0, nl, x1, f1);
+    envelopes(m, L0, nl, x2, f2);
+    if (h >= 1e-15) {
+      if (fabs(omega * h) < 1e-3) {  // the 3-node panel itself is non-oscillatory: Simpson times the mid phase
+        const double h0 = x1 - x0, h1 = x2 - x1;
+        const double hs = h0 + h1, hp = h0 * h1, qq = h0 / h1;
+        const double ce = cexpi(omega * (x0 + x2) / 2 + off).re;
+#pragma unroll
+        for (int q = 0; q < LC; ++q)
+          seg[q] += ce * (hs / 6.0 * (f0[q] * (2.0 - 1.0 / qq) + f1[q] * (hs * (hs / hp)) + f2[q] * (2.0 - qq)));
+      } else {
+        const double th = omega * h / 2;
+        double st, ct;
+        sincos(th, &st, &ct);
+        double al, be, ga;
+        if (fabs(th) < 0.3) {
+          const double t2 = th * th, t3 = pow(th, 3.0);
+          al = 2 * t3 / 45 * (1 - t2 / 7 + (t2 * t2) / 189);
+          be = 2.0 / 3 + 2 * t2 / 15 - 4 * (t2 * t2) / 105 + 2 * pow(t2, 3.0) / 567;
+          ga = 4.0 / 3 - 2 * t2 / 15 + 1 * (t2 * t2) / 210 - pow(t2, 3.0) / 11340;
+        } else {
+          const double t2 = th * th, t3 = pow(th, 3.0);
+          double s2, c2;
+          sincos(2 * th, &s2, &c2);
+          al = (t2 + th * s2 / 2 - 2 * (st * st)) / t3;
+          be = 2 * (th * (1 + c2) - s2) / t3;
+          ga = 4 * (st - th * ct) / t3;
+        }
+        // (h/2) [alpha (-i/omega) (f2 e2 - f0 e0) + beta (f0 e0 + f2 e2) + gamma f1 e1], real part,
+        // as weights of f0, f1, f2 that every multipole shares
+        const cplx mi = {0.0, -1.0 / omega};
+        const cplx am = cscale(al, mi);
+        const double w0 = (h / 2) * cmul(csub(cplx{be, 0.0}, am), e0).re;
+        const double w1 = (h / 2) * (ga * e1.re);
+        const double w2 = (h / 2) * cmul(cadd(cplx{be, 0.0}, am), e2).re;
+#pragma unroll
+        for (int q = 0; q < LC; ++q) seg[q] += w0 * f0[q] + w1 * f1[q] + w2 * f2[q];
+      }
+    }
+    x0 = x2;
+    e0 = e2;
+#pragma unroll
+    for (int q = 0; q < LC; ++q) f0[q] = f2[q];
+  }
+#pragma unroll
+  for (int q = 0; q < LC; ++q) acc[q].add(seg[q]);
+}
+
+// Levin collocation on one segment (8 nodes) for every multipole of the chunk: the system matrix
+// does not depend on L, so it is factorised once and solved for each envelope
+__device__ void levin_segment_all(const double* m, int L0, int nl, const PhaseD& ph, double a, double b,
+                                  KSum* acc) {
+  const LevinD& lv = s_lv;
+  cplx A[8][8];
+  double x[8];
+  int perm[8];
+  for (int k = 0; k < 8; ++k) x[k] = 0.5 * (b - a) * (lv.xr[k] + 1) + a;
+  const double h = x[7] - x[0];
+  if (h < 1e-15) return;
+  const double sc = 2.0 / h;
+  for (int i = 0; i < 8; ++i) {
+    for (int j = 0; j < 8; ++j) A[i][j] = {lv.D[i][j] * sc, 0.0};
+    A[i][i].im += ph.d1(x[i]);
+    perm[i] = i;
+  }
+#pragma unroll 1
+  for (int k = 0; k < 8; ++k) {  // partial pivoting by |re| + |im|, multipliers kept in A
+    int piv = k;
+    double best = -1.0;
+    for (int i = k; i < 8; ++i) {
+      const double mm = fabs(A[i][k].re) + fabs(A[i][k].im);
+      if (mm > best) { best = mm; piv = i; }
+    }
+    if (best == 0.0) return;
+    if (piv != k) {
+      for (int j = 0; j < 8; ++j) { cplx t = A[k][j]; A[k][j] = A[piv][j]; A[piv][j] = t; }
+      const int t = perm[k]; perm[k] = perm[piv]; perm[piv] = t;
+    }
+    const cplx inv = cdiv({1.0, 0.0}, A[k][k]);
+    for (int i = k + 1; i < 8; ++i) {
+      const cplx l = cmul(A[i][k], inv);
+      A[i][k] = l;
+      for (int j = k + 1; j < 8; ++j) A[i][j] = csub(A[i][j], cmul(l, A[k][j]));
+    }
+  }
+  const cplx e7 = cexpi(ph.phi(x[7])), e0 = cexpi(ph.phi(x[0]));
+  double inv[8], pw[8];  // 1 / x and x^-(L+1) at the permuted nodes, advanced by one power per multipole
+  for (int i = 0; i < 8; ++i) {
+    const double xi = x[perm[i]];
+    inv[i] = xi > 1e-6 ? 1.0 / xi : 0.0;
+    pw[i] = xi > 1e-6 ? pow(inv[i], (double)(L0 + 1)) : 0.0;
+  }
+#pragma unroll 1
+  for (int q = 0; q < nl; ++q) {
+    cplx u[8];
+    for (int i = 0; i < 8; ++i) {
+      u[i] = {m[q] * pw[i], 0.0};
+      pw[i] *= inv[i];
+    }
+    for (int k = 0; k < 8; ++k)
+      for (int i = k + 1; i < 8; ++i) u[i] = csub(u[i], cmul(A[i][k], u[k]));
+    for (int i = 7; i >= 0; --i) {
+      cplx sum = u[i];
+      for (int j = i + 1; j < 8; ++j) sum = csub(sum, cmul(A[i][j], u[j]));
+      u[i] = cdiv(sum, A[i][i]);
+    }
+    acc[q].add(csub(cmul(u[7], e7), cmul(u[0], e0)).re);
+  }
+}
+
+// one phase branch (cos(Phi_a -/+ Phi_b)) of the outer integral for a chunk of multipoles: Re part
+// per multipole, summed over the warp into res[q]
+__device__ __noinline__ void outer_branch_all(const double* m, int L0, int nl, const PhaseD& ph, double rm, double rmax,
+                                 int max_seg, double max_dphi, int lane, double* res) {
   const double delta_phi = M_PI / 4;
   const double om = fabs(ph.d1((rm + rmax) / 2));
   const double h = delta_phi / om;
   const double lin_t = fabs(ph.d2((rm + rmax) / 2)) * h * h;
-  KSum re;
+  KSum acc[LC];
   if (lin_t < 0.1) {
     const double off = ph.phi(rm) - om * rm;
     const double dr = delta_phi / om;
@@ -227,16 +298,17 @@ __device__ double outer_branch(double m, int L, const PhaseD& ph, double rm, dou
     }
     for (int s = lane; s < nseg; s += 32) {
       const double a = lin(rm, rmax, nseg + 1, s), b = lin(rm, rmax, nseg + 1, s + 1);
-      re.add(filon_segment(m, L, a, b, nn, om, off).re);
+      filon_segment_all(m, L0, nl, a, b, nn, om, off, acc);
     }
   } else {
     const int nseg = (int)max(1.0, ceil((rmax - rm) / h));
     for (int s = lane; s < nseg; s += 32) {
       const double a = lin(rm, rmax, nseg + 1, s), b = lin(rm, rmax, nseg + 1, s + 1);
-      re.add(levin_segment(m, L, ph, a, b, lv).re);
+      levin_segment_all(m, L0, nl, ph, a, b, acc);
     }
   }
-  return warp_sum(re.s + re.c);
+#pragma unroll
+  for (int q = 0; q < LC; ++q) res[q] = warp_sum(acc[q].s + acc[q].c);
 }
 
 __device__ double analytical_tail(double r_m, const WaveD& wi, const WaveD& wf, int L, double overlap) {
@@ -260,35 +332,54 @@ __device__ double analytical_tail(double r_m, const WaveD& wi, const WaveD& wf, 
   return t * overlap;
 }
 
-__global__ void tails_kernel(const dwba_tail_t* __restrict__ recs, int n, int L_max, int max_seg, double max_dphi,
+// one warp per (record, chunk of up to LC multipoles): the Filon / Levin segments of both phase
+// branches over the lanes, every node's phase factor and every panel's weights shared by the chunk
+__global__ void __launch_bounds__(128, 4) tails_kernel(const dwba_tail_t* __restrict__ recs, int n, int L_max, int max_seg, double max_dphi,
                              LevinD lv) {
+  for (int i = threadIdx.x; i < 72; i += blockDim.x)
+    (&s_lv.D[0][0])[i] = i < 64 ? lv.D[i / 8][i % 8] : lv.xr[i - 64];
+  __syncthreads();
   const int lane = threadIdx.x & 31;
+  const int n_chunk = (L_max + LC - 1) / LC;
   const int64_t warp_g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t n_items = (int64_t)n * L_max;
+  const int64_t n_items = (int64_t)n * n_chunk;
   const int64_t stride = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t it = warp_g; it < n_items; it += stride) {
-    const int rec = (int)(it / L_max);
-    const int L = (int)(it - (int64_t)rec * L_max) + 1;
-    const dwba_tail_t R = recs[rec];
-    const WaveD wi = {R.wave[0], R.wave[2], R.wave[3], R.wave[4], (int)R.wave[1]};
-    const WaveD wf = {R.wave[5], R.wave[7], R.wave[8], R.wave[9], (int)R.wave[6]};
-    const double m = R.moments_dev[L];
-    double t = 0.0;
-    if (fabs(m) > 1e-12) {
-      if (R.mode == 1) {
-        t = analytical_tail(R.r_m, wi, wf, L, m);
-      } else {
-        if (!(R.r_max <= R.r_m + 1e-10)) {
-          const double im = outer_branch(m, L, PhaseD(wi, wf, -1), R.r_m, R.r_max, max_seg, max_dphi, lv, lane);
-          const double ip = outer_branch(m, L, PhaseD(wi, wf, +1), R.r_m, R.r_max, max_seg, max_dphi, lv, lane);
-          t = 0.5 * (im - ip);
-        }
-        t += analytical_tail(R.r_max, wi, wf, L, m);
-      }
+    const int rec = (int)(it / n_chunk);
+    const int L0 = 1 + (int)(it - (int64_t)rec * n_chunk) * LC;  // multipoles L0 .. L0+nl-1
+    const int nl = min(LC, L_max + 1 - L0);
+    const dwba_tail_t* R = recs + rec;
+    const WaveD wi = {R->wave[0], R->wave[2], R->wave[3], R->wave[4], (int)R->wave[1]};
+    const WaveD wf = {R->wave[5], R->wave[7], R->wave[8], R->wave[9], (int)R->wave[6]};
+    const double r_m = R->r_m, r_max = R->r_max;
+    double m[LC];
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < LC; ++q) {
+      const double v = q < nl ? R->moments_dev[L0 + q] : 0.0;
+      m[q] = fabs(v) > 1e-12 ? v : 0.0;  // moments at or below the cut-off give a zero tail
+      any = any || m[q] != 0.0;
+    }
+    double t[LC];
+#pragma unroll
+    for (int q = 0; q < LC; ++q) t[q] = 0.0;
+    if (any && R->mode != 1 && !(r_max <= r_m + 1e-10)) {
+      double im[LC], ip[LC];
+      outer_branch_all(m, L0, nl, PhaseD(wi, wf, -1), r_m, r_max, max_seg, max_dphi, lane, im);
+      outer_branch_all(m, L0, nl, PhaseD(wi, wf, +1), r_m, r_max, max_seg, max_dphi, lane, ip);
+#pragma unroll
+      for (int q = 0; q < LC; ++q) t[q] = 0.5 * (im[q] - ip[q]);
     }
     if (lane == 0) {
-      R.out_dev[L] = t;
-      if (L == 1) R.out_dev[0] = 0.0;
+      for (int q = 0; q < nl; ++q) {
+        double v = 0.0;
+        if (m[q] != 0.0) {
+          v = R->mode == 1 ? analytical_tail(r_m, wi, wf, L0 + q, m[q])
+                           : t[q] + analytical_tail(r_max, wi, wf, L0 + q, m[q]);
+        }
+        R->out_dev[L0 + q] = v;
+      }
+      if (L0 == 1) R->out_dev[0] = 0.0;
     }
   }
 }
@@ -318,7 +409,7 @@ extern "C" int dwba_outer_tails_batch(const dwba_tail_t* tails_dev, int n, int L
     lv.D[i][i] = -rs;
   }
   for (int k = 0; k < 8; ++k) lv.xr[k] = cos(M_PI * (7 - k) / 7);
-  const int64_t warps = (int64_t)n * L_max;
+  const int64_t warps = (int64_t)n * ((L_max + LC - 1) / LC);
   const int blocks = dwba_grid_1d(warps * 32, 128, 65535);
   tails_kernel<<<blocks, 128, 0, (cudaStream_t)stream>>>(tails_dev, n, L_max, max_filon_segments, max_effective_dphi,
                                                          lv);

@@ -154,13 +154,13 @@ def make_ragged_points(n_energy=64, l_max_wave=40, r_max=200.0, seed=3):
     return points
 
 
-def ragged_sweep(engine, L_max=6, replays=5):
+def ragged_sweep(engine, L_max=6, replays=5, n_energy=64):
     """Device time of the ragged sweep (node sets, folds, forms and tails of all points in shared
     launches, replayed from a CUDA graph)."""
     import torch
     from dwba_b200.dwba_matrix_elements import GPUCache, _make_job
     from dwba_b200.engine import MultiPrepared, PreparedJob
-    points = make_ragged_points()
+    points = make_ragged_points(n_energy)
     kw = dict(use_oscillatory_quadrature=True, oscillatory_method="advanced", CC_nodes=5, phase_increment=1.5708,
               min_grid_fraction=0.10, k_threshold=0.5)
     parts = []

@@ -114,6 +114,17 @@ __device__ double warp_sum(double v) {
 
 constexpr int LC = 8;  // multipoles evaluated together (one accumulator each per lane)
 
+// b^e for e >= 0 by repeated squaring
+__device__ __forceinline__ double ipow(double b, int e) {
+  double r = 1.0;
+  while (e) {
+    if (e & 1) r *= b;
+    b *= b;
+    e >>= 1;
+  }
+  return r;
+}
+
 // envelopes f_L(x) = m_L / x^(L+1) for L = L0 .. L0+nl-1 (zero where |m_L| <= 1e-12 or x <= 1e-6)
 __device__ __forceinline__ void envelopes(const double* m, int L0, int nl, double x, double* f) {
   if (!(x > 1e-6)) {
@@ -122,7 +133,7 @@ __device__ __forceinline__ void envelopes(const double* m, int L0, int nl, doubl
     return;
   }
   const double inv = 1.0 / x;
-  double p = pow(inv, (double)(L0 + 1));
+  double p = ipow(inv, L0 + 1);
 #pragma unroll
   for (int q = 0; q < LC; ++q) {
     f[q] = q < nl ? m[q] * p : 0.0;
@@ -132,7 +143,7 @@ __device__ __forceinline__ void envelopes(const double* m, int L0, int nl, doubl
 
 // Re of the Filon integral over one segment (nn equally spaced nodes, nn odd) for every multipole
 // of the chunk: _filon_segment_complex with the node phases and the panel weights shared by all L
-__device__ void filon_segment_all(const double* m, int L0, int nl, double a, double b, int nn, double omega,
+__device__ __noinline__ void filon_segment_all(const double* m, int L0, int nl, double a, double b, int nn, double omega,
                                   double off, KSum* acc) {
   if (!(b - a >= 1e-15)) return;
   double f0[LC], f1[LC], f2[LC];
@@ -182,12 +193,12 @@ __device__ void filon_segment_all(const double* m, int L0, int nl, double a, dou
         sincos(th, &st, &ct);
         double al, be, ga;
         if (fabs(th) < 0.3) {
-          const double t2 = th * th, t3 = pow(th, 3.0);
+          const double t2 = th * th, t3 = t2 * th, t6 = t2 * t2 * t2;
           al = 2 * t3 / 45 * (1 - t2 / 7 + (t2 * t2) / 189);
-          be = 2.0 / 3 + 2 * t2 / 15 - 4 * (t2 * t2) / 105 + 2 * pow(t2, 3.0) / 567;
-          ga = 4.0 / 3 - 2 * t2 / 15 + 1 * (t2 * t2) / 210 - pow(t2, 3.0) / 11340;
+          be = 2.0 / 3 + 2 * t2 / 15 - 4 * (t2 * t2) / 105 + 2 * t6 / 567;
+          ga = 4.0 / 3 - 2 * t2 / 15 + 1 * (t2 * t2) / 210 - t6 / 11340;
         } else {
-          const double t2 = th * th, t3 = pow(th, 3.0);
+          const double t2 = th * th, t3 = t2 * th;
           double s2, c2;
           sincos(2 * th, &s2, &c2);
           al = (t2 + th * s2 / 2 - 2 * (st * st)) / t3;
@@ -216,7 +227,7 @@ __device__ void filon_segment_all(const double* m, int L0, int nl, double a, dou
 
 // Levin collocation on one segment (8 nodes) for every multipole of the chunk: the system matrix
 // does not depend on L, so it is factorised once and solved for each envelope
-__device__ void levin_segment_all(const double* m, int L0, int nl, const PhaseD& ph, double a, double b,
+__device__ __noinline__ void levin_segment_all(const double* m, int L0, int nl, const PhaseD& ph, double a, double b,
                                   KSum* acc) {
   const LevinD& lv = s_lv;
   cplx A[8][8];
@@ -256,7 +267,7 @@ __device__ void levin_segment_all(const double* m, int L0, int nl, const PhaseD&
   for (int i = 0; i < 8; ++i) {
     const double xi = x[perm[i]];
     inv[i] = xi > 1e-6 ? 1.0 / xi : 0.0;
-    pw[i] = xi > 1e-6 ? pow(inv[i], (double)(L0 + 1)) : 0.0;
+    pw[i] = xi > 1e-6 ? ipow(inv[i], L0 + 1) : 0.0;
   }
 #pragma unroll 1
   for (int q = 0; q < nl; ++q) {

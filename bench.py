@@ -181,6 +181,15 @@ def ragged_sweep(engine, L_max=6, replays=5, n_energy=64):
     e1.record(st)
     e1.synchronize()
     ms = e0.elapsed_time(e1) / replays
+    # per-stage device time of one more (un-captured) launch sequence, with each stage's bytes
+    marks = []
+    mp.launch(marks)
+    torch.cuda.synchronize()
+    split = {f"{b[0]}_ms": a[1].elapsed_time(b[1]) for a, b in zip(marks[:-1], marks[1:])}
+    stage_bytes = {"nodesets_ms": sum(p.nodesets.algorithmic_bytes() for p in parts if p.nodesets.n),
+                   "folds_ms": sum(p.fold_bytes() for p in parts),
+                   "forms_ms": sum(p.algorithmic_bytes() for p in parts)}
+    gbs = {k.replace("_ms", "_gbs"): stage_bytes[k] / (split[k] * 1e-3) / 1e9 for k in stage_bytes if split.get(k)}
     outs = mp.collect()
     finite = all(np.isfinite(d).all() and np.isfinite(e).all() for d, e in outs)
     n_int = sum(2 * p.T * p.P * p.nl for p in parts)
@@ -192,6 +201,7 @@ def ragged_sweep(engine, L_max=6, replays=5, n_energy=64):
             "engine": engine, "energies": n_energy, "points": len(points), "N_min": min(Ns), "N_max": max(Ns),
             "integrals": n_int, "ms_per_sweep": ms, "ms_per_energy": ms / n_energy,
             "integrals_per_s": n_int / (ms * 1e-3), "graph": True, "replays": replays,
+            "split_ms": split, "split_algorithmic_gbs": gbs,
             "tail_records": int(sum(p.n_tail for p in parts)), "results_finite": bool(finite)}
 
 

@@ -14,12 +14,12 @@
 // sum_c K(r_i, x_c) W_c (P2 rho2)_c equals sum_k K_ik (B rho2)_k with
 // B = Q^T diag(W) P2 (band of half-width 2).
 //
-// One thread per grid row k gathers the nodes that touch row k: a node with
-// interpolation interval j feeds rows j and j+1, so row k needs exactly the
-// nodes in [r_{k-1}, r_{k+1}]. The thread enumerates the phase intervals that
-// overlap that window, recomputes their nodes with the reference's arithmetic,
-// and sums the contributions in ascending node order (deterministic, no scratch
-// memory, no atomics).
+// Every CC node lies in one grid interval (r_g, r_{g+1}] and feeds only rows g,
+// g+1 and g+2, so one thread per grid interval evaluates the nodes it owns once
+// (enumerating the phase intervals that overlap its grid interval and recomputing
+// their nodes with the reference's arithmetic), sums their contributions per
+// target row in ascending node order, and each row adds the sums of its three
+// owners through warp shuffles (deterministic, no scratch memory, no atomics).
 #include "common.cuh"
 
 namespace {
@@ -69,14 +69,26 @@ __device__ __forceinline__ int interval_floor(const SetView& s, double x) {
   return m;
 }
 
-// One warp per CTA: 32 consecutive rows do similar work (their windows hold similar node counts),
-// and the small CTAs keep the SMs evenly loaded although the work per row grows with r.
-constexpr int ROWS_CTA = 32;
-__global__ void __launch_bounds__(ROWS_CTA, 24) nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets, const double* __restrict__ ccx_g,
-                                    const double* __restrict__ ccw_g, int n_cc, int* status) {
-  __shared__ double ccx[MAX_CC], ccw[MAX_CC], ccx1[MAX_CC];
+// reciprocal width of interpolation interval j (log r or r), zero past the grid
+__device__ __forceinline__ double recip_width(const SetView& s, int j, bool lg) {
+  if (j < 0 || j + 1 > s.n_grid - 1) return 0.0;
+  return lg ? 1.0 / (s.lr[j + 1] - s.lr[j]) : 1.0 / (s.r[j + 1] - s.r[j]);
+}
+
+// One warp per CTA covers OWN_ROWS consecutive grid rows. Lane j owns grid interval
+// g = k0 - 2 + j: the CC nodes whose kernel-column interval (searchsorted left, clipped) is
+// il = g, i.e. x in (r_g, r_{g+1}] (g = 0: [r_0, r_1]). Each node is evaluated once, by its
+// owner, and reaches rows g, g+1 (T and B) and g+2 (T, a node exactly at r_{g+1}); the owner
+// sums them per target row in ascending node order, and row k adds the sums of lanes k-2,
+// k-1 and k in that order through warp shuffles. Lanes 0 and 1 are the halo of the first two
+// rows (their own rows are written by the previous CTA).
+constexpr int OWN_ROWS = 30;
+__global__ void __launch_bounds__(32, 24) nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets,
+                                                              const double* __restrict__ ccx_g,
+                                                              const double* __restrict__ ccw_g, int n_cc,
+                                                              int* status) {
+  __shared__ double ccw[MAX_CC], ccx1[MAX_CC];
   if (threadIdx.x < n_cc) {
-    ccx[threadIdx.x] = ccx_g[threadIdx.x];
     ccw[threadIdx.x] = ccw_g[threadIdx.x];
     ccx1[threadIdx.x] = rn_add(ccx_g[threadIdx.x], 1.0);
   }
@@ -96,118 +108,117 @@ __global__ void __launch_bounds__(ROWS_CTA, 24) nodeset_rows_kernel(const dwba_n
   s.step = rn_sub(s.stop, s.start) / (double)s.n_int;
   const int N = s.n_grid, n1 = s.n1;
   const double* __restrict__ r = s.r;
+  const int lane = threadIdx.x;
+  const double r_first = r[0], r_lim = r[n1 - 1], r_last = r[N - 1];
 
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
-    const double wlo = k >= 1 ? r[k - 1] : -1.0e308;
-    const double whi = k + 1 <= N - 1 ? r[k + 1] : 1.0e308;
-    double t_lo = 0.0, t_di = 0.0, t_up = 0.0;
-    double band0 = 0.0, band1 = 0.0, band2 = 0.0, band3 = 0.0, band4 = 0.0;
+  for (int k0 = blockIdx.x * OWN_ROWS; k0 < N; k0 += gridDim.x * OWN_ROWS) {
+    const int g = k0 - 2 + lane;
+    // sums for row g (o_*), row g+1 (x_*) and row g+2 (n_*)
+    double o_di = 0.0, o_up = 0.0, o_b2 = 0.0, o_b3 = 0.0, o_b4 = 0.0;
+    double x_lo = 0.0, x_di = 0.0, x_up = 0.0, x_b1 = 0.0, x_b2 = 0.0, x_b3 = 0.0;
+    double n_lo = 0.0, n_di = 0.0;
     bool bad = false;
-    // the interpolation intervals a node of this row can use are j in {k-1, k, k+1}: their
-    // reciprocal widths (log r or r) and the reciprocal kernel-column spacings, once per row
-    auto recip = [&](int j, bool lg) -> double {
-      if (j < 0 || j + 1 > N - 1) return 0.0;
-      return lg ? 1.0 / (s.lr[j + 1] - s.lr[j]) : 1.0 / (r[j + 1] - r[j]);
-    };
-    const double iT0 = recip(k - 1, s.log1), iT1 = recip(k, s.log1);
-    const double iB0 = recip(k - 1, s.log2), iB1 = recip(k, s.log2), iB2 = recip(k + 1, s.log2);
-    const double iW0 = k >= 1 ? 1.0 / (r[k] - r[k - 1] + 1e-30) : 0.0;          // il = k-1
-    const double iW1 = k + 1 <= N - 1 ? 1.0 / (r[k + 1] - r[k] + 1e-30) : 0.0;  // il = k
-    // grid values the nodes of this row can touch, held in registers
-    const double rk = r[k], rkm = k >= 1 ? r[k - 1] : 0.0, rkp = k + 1 <= N - 1 ? r[k + 1] : 0.0;
-    const double lk = s.lr[k], lkm = k >= 1 ? s.lr[k - 1] : 0.0, lkp = k + 1 <= N - 1 ? s.lr[k + 1] : 0.0;
-    const double r_first = r[0], r_lim = r[n1 - 1], r_last = r[N - 1];
-    // nodes never leave [r0, r[n1-1]]; rows past n1+1 have none
-    if (k <= n1 + 1) {
-      // one interval earlier too: its top node can coincide with the window's lower end
-      const int m0 = max(0, interval_floor(s, wlo) - 1);
-      for (int m = m0; m < s.n_int; ++m) {
+    // nodes lie in [r_0, r_{n1-1}], so owners stop at g = n1 - 2
+    if (g >= 0 && g <= n1 - 2) {
+      const double rg = r[g], rg1 = r[g + 1];
+      const double lo = g == 0 ? -1.0e308 : rg;  // exclusive lower end of the owned interval
+      bool first = true;
+      double iT0 = 0.0, iT1 = 0.0, iB0 = 0.0, iB1 = 0.0, iW = 0.0, lg = 0.0, lg1 = 0.0;
+      for (int m = interval_floor(s, rg); m < s.n_int; ++m) {
         double a, b;
         interval(s, m, a, b);
-        if (a > whi) break;
+        if (a > rg1) break;
         const double width = rn_sub(b, a);
         if (!(width > 1e-12)) continue;
         const double hw = rn_mul(0.5, width);
         for (int sl = n_cc - 1; sl >= 0; --sl) {  // ascending positions within the interval
           double x = rn_add(rn_mul(hw, ccx1[sl]), a);
           x = fmin(fmax(x, a), b);  // the top node can round one ulp past b
-          if (x < wlo || x > whi) continue;
-          // kernel columns: searchsorted(r, x, 'left') within the window, clipped to [1, N-1]
-          int ir;
-          if (k >= 1 && x <= rkm) ir = k - 1;
-          else if (x <= rk) ir = k;
-          else ir = k + 1;
-          ir = ir < 1 ? 1 : (ir > N - 1 ? N - 1 : ir);
-          const int il = ir - 1;
-          const bool b_row = il == k || il == k - 1;
-          if (k >= n1 && !b_row) continue;  // reaches neither a T nor a B entry of this row
+          if (!(x > lo)) continue;
+          if (x > rg1) break;
+          if (first) {  // reciprocal widths of the intervals j in {g, g+1} a node of this owner uses
+            iT0 = recip_width(s, g, s.log1);
+            iT1 = recip_width(s, g + 1, s.log1);
+            iB0 = recip_width(s, g, s.log2);
+            iB1 = recip_width(s, g + 1, s.log2);
+            iW = 1.0 / (rg1 - rg + 1e-30);
+            lg = s.lr[g];
+            lg1 = s.lr[g + 1];
+            first = false;
+          }
           const double w = rn_mul(ccw[sl], hw);
-          // interpolation interval on r[:n] (np.interp after clipping; x is inside [r_{k-1}, r_{k+1}])
           const double lx = (s.log1 || s.log2) ? log(x) : 0.0;
-          int jf;  // floor index in the full grid
-          if (k + 1 <= N - 1 && x >= rkp) jf = k + 1;
-          else if (x >= rk) jf = k;
-          else jf = k - 1;
-          // --- T rows: nodes with j1 in {k-1, k}
-          if (k < n1) {
+          const bool at_top = x >= rg1;  // floor index in the full grid: g + 1 at r_{g+1}, else g
+          // --- T: rows j1 and j1 + 1, j1 in {g, g+1}
+          {
             int j1;
             double t1;
             if (x <= r_first) { j1 = 0; t1 = 0.0; }
             else if (x >= r_lim) { j1 = n1 - 2; t1 = 1.0; }
             else {
-              j1 = jf > n1 - 2 ? n1 - 2 : jf;
-              if (j1 == k || j1 == k - 1) {
-                const double inv = j1 == k ? iT1 : iT0;
-                t1 = s.log1 ? (lx - (j1 == k ? lk : lkm)) * inv : (x - (j1 == k ? rk : rkm)) * inv;
-              } else {
-                t1 = 0.0;  // reaches no T entry of this row
-              }
+              j1 = (at_top && g + 1 <= n1 - 2) ? g + 1 : g;
+              const bool up = j1 != g;
+              const double inv = up ? iT1 : iT0;
+              t1 = s.log1 ? (lx - (up ? lg1 : lg)) * inv : (x - (up ? rg1 : rg)) * inv;
             }
-            if (j1 == k) {
-              t_di += w * (1.0 - t1) * (1.0 - t1);
-              t_up += w * (1.0 - t1) * t1;
-            } else if (j1 == k - 1) {
-              t_di += w * t1 * t1;
-              t_lo += w * t1 * (1.0 - t1);
+            const double v_di0 = w * (1.0 - t1) * (1.0 - t1), v_up0 = w * (1.0 - t1) * t1;
+            const double v_di1 = w * t1 * t1, v_lo1 = w * t1 * (1.0 - t1);
+            if (j1 == g) {
+              o_di += v_di0; o_up += v_up0;
+              x_di += v_di1; x_lo += v_lo1;
+            } else if (j1 == g + 1) {
+              x_di += v_di0; x_up += v_up0;
+              n_di += v_di1; n_lo += v_lo1;
+            } else {
+              bad = true;
             }
           }
-          // --- B rows: nodes with il in {k-1, k}
-          if (!b_row) continue;
-          int j2;
-          double t2;
-          if (x <= r_first) { j2 = 0; t2 = 0.0; }
-          else if (x >= r_last) { j2 = N - 2; t2 = 1.0; }
-          else {
-            j2 = jf > N - 2 ? N - 2 : jf;
-            const int dj = j2 - k;  // -1, 0 or 1 inside the window
-            const double inv = dj < 0 ? iB0 : (dj == 0 ? iB1 : iB2);
-            t2 = s.log2 ? (lx - (dj < 0 ? lkm : (dj == 0 ? lk : lkp))) * inv
-                        : (x - (dj < 0 ? rkm : (dj == 0 ? rk : rkp))) * inv;
+          // --- B: rows il = g (weight 1 - wr) and g + 1 (weight wr), taps d0, d0 + 1
+          {
+            int j2;
+            double t2;
+            if (x <= r_first) { j2 = 0; t2 = 0.0; }
+            else if (x >= r_last) { j2 = N - 2; t2 = 1.0; }
+            else {
+              j2 = (at_top && g + 1 <= N - 2) ? g + 1 : g;
+              const bool up = j2 != g;
+              const double inv = up ? iB1 : iB0;
+              t2 = s.log2 ? (lx - (up ? lg1 : lg)) * inv : (x - (up ? rg1 : rg)) * inv;
+            }
+            const double wr = (x - rg) * iW;
+            const double q0 = 1.0 - wr, q1 = wr;
+            if (j2 == g) {  // row g: taps 0, 1 (band 2, 3); row g+1: taps -1, 0 (band 1, 2)
+              o_b2 += q0 * w * (1.0 - t2); o_b3 += q0 * w * t2;
+              x_b1 += q1 * w * (1.0 - t2); x_b2 += q1 * w * t2;
+            } else if (j2 == g + 1) {  // row g: taps 1, 2 (band 3, 4); row g+1: taps 0, 1 (band 2, 3)
+              o_b3 += q0 * w * (1.0 - t2); o_b4 += q0 * w * t2;
+              x_b2 += q1 * w * (1.0 - t2); x_b3 += q1 * w * t2;
+            } else {
+              bad = true;
+            }
           }
-          const double wr = (x - (il == k ? rk : rkm)) * (il == k ? iW1 : iW0);
-          const double q = il == k ? 1.0 - wr : wr;
-          const int d0 = j2 - k;
-          if (d0 < -2 || d0 + 1 > 2) { bad = true; continue; }
-          const double v0 = q * w * (1.0 - t2), v1 = q * w * t2;
-          // taps d0, d0+1 of the row's band (registers: no dynamic indexing)
-          if (d0 == -2) { band0 += v0; band1 += v1; }
-          else if (d0 == -1) { band1 += v0; band2 += v1; }
-          else if (d0 == 0) { band2 += v0; band3 += v1; }
-          else { band3 += v0; band4 += v1; }
         }
       }
     }
-    if (k < n1) {
-      d.ta_dev[3 * k + 0] = t_lo;
-      d.ta_dev[3 * k + 1] = t_di;
-      d.ta_dev[3 * k + 2] = t_up;
+    // row g = sums of lane - 2 (its row g+2), lane - 1 (its row g+1) and this lane, in that order
+    const double p_lo = __shfl_up_sync(0xffffffffu, n_lo, 2), p_di = __shfl_up_sync(0xffffffffu, n_di, 2);
+    const double q_lo = __shfl_up_sync(0xffffffffu, x_lo, 1), q_di = __shfl_up_sync(0xffffffffu, x_di, 1);
+    const double q_up = __shfl_up_sync(0xffffffffu, x_up, 1);
+    const double q_b1 = __shfl_up_sync(0xffffffffu, x_b1, 1), q_b2 = __shfl_up_sync(0xffffffffu, x_b2, 1);
+    const double q_b3 = __shfl_up_sync(0xffffffffu, x_b3, 1);
+    if (lane >= 2 && g < N) {
+      if (g < n1) {
+        d.ta_dev[3 * g + 0] = p_lo + q_lo;  // from nodes below r_g only
+        d.ta_dev[3 * g + 1] = (p_di + q_di) + o_di;
+        d.ta_dev[3 * g + 2] = q_up + o_up;
+      }
+      double* bx = d.bx_dev + 5 * (int64_t)g;
+      bx[0] = 0.0;
+      bx[1] = q_b1;
+      bx[2] = q_b2 + o_b2;
+      bx[3] = q_b3 + o_b3;
+      bx[4] = o_b4;
     }
-    double* bx = d.bx_dev + 5 * (int64_t)k;
-    bx[0] = band0;
-    bx[1] = band1;
-    bx[2] = band2;
-    bx[3] = band3;
-    bx[4] = band4;
     if (bad) atomicExch(status, 1);
   }
 }
@@ -220,8 +231,8 @@ extern "C" int dwba_build_nodesets(const dwba_nodeset_t* sets_dev, int n_sets, i
   if (!sets_dev || !cc_x_dev || !cc_w_dev || !status_dev || n_cc < 2 || n_cc > MAX_CC || max_grid < 2 ||
       n_sets > 65535)
     return DWBA_ERR_INVALID_ARG;
-  dim3 grid(dwba_grid_1d(max_grid, ROWS_CTA), n_sets);
-  nodeset_rows_kernel<<<grid, ROWS_CTA, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc, status_dev);
+  dim3 grid((max_grid + OWN_ROWS - 1) / OWN_ROWS, n_sets);
+  nodeset_rows_kernel<<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc, status_dev);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;
 }

@@ -941,15 +941,25 @@ class MultiPrepared:
             self.partial = torch.empty(self.n_cta * self.nl, dtype=torch.float64, device=dev)
         self.graph = None
 
-    def launch(self) -> None:
+    def launch(self, marks: Optional[list] = None) -> None:
+        """The launch sequence. With ``marks`` (a list), a CUDA event is recorded on the stream after
+        each stage and appended as (stage, event): "start", "nodesets", "folds", "forms", "tails"."""
         lib = self.lib
         st = _stream()
+
+        def mark(name):
+            if marks is not None:
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record(torch.cuda.current_stream())
+                marks.append((name, ev))
+        mark("start")
         if self.n_sets:
             for s0 in range(0, self.n_sets, 65535):
                 n = min(65535, self.n_sets - s0)
                 _lib.check(lib.dwba_build_nodesets(_ptr(self.recs_d) + s0 * _lib.NODESET_DTYPE.itemsize, n,
                                                    self.max_grid, _ptr(self.ccx), _ptr(self.ccw), self.n_cc,
                                                    _ptr(self.ns_status), st), "dwba_build_nodesets")
+        mark("nodesets")
         for s0 in range(0, self.n_folds, 65535):
             n = min(65535, self.n_folds - s0)
             _lib.check(lib.dwba_fold(_ptr(self.folds_d) + s0 * _lib.FOLD_DTYPE.itemsize, n, self.max_grid, st),
@@ -958,6 +968,7 @@ class MultiPrepared:
             n = min(65535, self.n_multi - s0)
             _lib.check(lib.dwba_fold_multi(_ptr(self.multi_d) + s0 * _lib.FOLD_MULTI_DTYPE.itemsize, n,
                                            self.max_grid, st), "dwba_fold_multi")
+        mark("folds")
         if self.engine == "dense":
             _lib.check(lib.dwba_bilinear_dense_fp64(_ptr(self.forms_d), self.n_forms, self.L_max, self.ds.ctypes.data,
                                                     _ptr(self.prefix_d), self.n_cta, _ptr(self.partial),
@@ -970,12 +981,17 @@ class MultiPrepared:
         else:
             for p in self.parts:
                 p.launch_forms()
+            mark("forms")
+            for p in self.parts:
                 p.launch_tails()
+            mark("tails")
             return
+        mark("forms")
         if self.n_tail and self.L_max >= 1:
             seg, dphi = self.tail_limits
             _lib.check(lib.dwba_outer_tails_batch(_ptr(self.tails_d), self.n_tail, self.L_max, seg, dphi, st),
                        "dwba_outer_tails_batch")
+        mark("tails")
 
     def capture(self) -> None:
         """Record the launch sequence once in a CUDA graph (warm-up launch first)."""

@@ -69,7 +69,8 @@ typedef struct {
 } dwba_nodeset_t;
 
 /* Builds the banded quadrature operators of n_sets node sets (one thread per grid
- * row gathers the CC nodes in [r_{k-1}, r_{k+1}]; no scratch memory).
+ * interval evaluates the CC nodes in (r_g, r_{g+1}] once; rows add the sums of
+ * their three owners; no scratch memory).
  * cc_x_dev/cc_w_dev: Clenshaw-Curtis reference nodes/weights on [-1, 1]
  * (descending nodes, as oscillatory_integrals.py:120-171 builds them), n_cc <= 15.
  * max_grid >= every set's n_grid. status_dev: one int, set non-zero if a band

@@ -83,7 +83,13 @@ __device__ __forceinline__ double recip_width(const SetView& s, int j, bool lg) 
 // k-1 and k in that order through warp shuffles. Lanes 0 and 1 are the halo of the first two
 // rows (their own rows are written by the previous CTA).
 constexpr int OWN_ROWS = 30;
-__global__ void __launch_bounds__(32, 24) nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets,
+#ifndef DWBA_NODESET_FILL
+#define DWBA_NODESET_FILL 32 // resident-CTA waves the launch aims for
+#endif
+#ifndef DWBA_NODESET_MIN_BLOCKS
+#define DWBA_NODESET_MIN_BLOCKS 24
+#endif
+__global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets,
                                                               const double* __restrict__ ccx_g,
                                                               const double* __restrict__ ccw_g, int n_cc,
                                                               int* status) {
@@ -231,7 +237,11 @@ extern "C" int dwba_build_nodesets(const dwba_nodeset_t* sets_dev, int n_sets, i
   if (!sets_dev || !cc_x_dev || !cc_w_dev || !status_dev || n_cc < 2 || n_cc > MAX_CC || max_grid < 2 ||
       n_sets > 65535)
     return DWBA_ERR_INVALID_ARG;
-  dim3 grid((max_grid + OWN_ROWS - 1) / OWN_ROWS, n_sets);
+  // row groups per set: enough one-warp CTAs in total to fill the GPU several times over, never
+  // more than the largest set needs (the kernel strides over its set's rows)
+  const int need = (max_grid + OWN_ROWS - 1) / OWN_ROWS;
+  const int fill = (int)(((int64_t)148 * 24 * DWBA_NODESET_FILL + n_sets - 1) / n_sets);
+  dim3 grid(need < fill ? need : fill, n_sets);
   nodeset_rows_kernel<<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc, status_dev);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;

@@ -940,6 +940,14 @@ class MultiPrepared:
             self.prefix_d = _dev(prefix, dev)
             self.partial = torch.empty(self.n_cta * self.nl, dtype=torch.float64, device=dev)
         self.graph = None
+        # tensor-core engines: one launch sequence per job, spread over side streams (largest grids
+        # first) so that the small grids of low-energy points run side by side instead of each
+        # leaving most SMs idle in its last wave
+        self.side_streams = []
+        self.tc_order = []
+        if self.engine in TC_TERMS:
+            self.side_streams = [torch.cuda.Stream(device=dev) for _ in range(min(4, len(parts)))]
+            self.tc_order = sorted(range(len(parts)), key=lambda k: -parts[k].job.grid.N)
 
     def launch(self, marks: Optional[list] = None) -> None:
         """The launch sequence. With ``marks`` (a list), a CUDA event is recorded on the stream after
@@ -979,12 +987,19 @@ class MultiPrepared:
                                                       self.r_min, self.r_max, _ptr(self.out), st),
                        "dwba_bilinear_semisep_fp64")
         else:
-            for p in self.parts:
-                p.launch_forms()
-            mark("forms")
-            for p in self.parts:
-                p.launch_tails()
-            mark("tails")
+            main = torch.cuda.current_stream()
+            for stage in ("forms", "tails"):
+                for sd in self.side_streams:
+                    sd.wait_stream(main)
+                for q, k in enumerate(self.tc_order):
+                    with torch.cuda.stream(self.side_streams[q % len(self.side_streams)]):
+                        if stage == "forms":
+                            self.parts[k].launch_forms()
+                        else:
+                            self.parts[k].launch_tails()
+                for sd in self.side_streams:
+                    main.wait_stream(sd)
+                mark(stage)
             return
         mark("forms")
         if self.n_tail and self.L_max >= 1:

@@ -13,7 +13,7 @@ def _point(N, seed, n_pairs=6):
     return dict(grid=g, V_core_array=z, U_i_array=z, bound_i=bi, bound_f=bf, pairs=pairs, U_f_array=z)
 
 
-@pytest.mark.parametrize("engine", ["dense", "semisep"])
+@pytest.mark.parametrize("engine", ["dense", "semisep", "tc_bf16x3"])
 @pytest.mark.parametrize("graph", [False, True])
 def test_sweep_matches_per_energy(engine, graph):
     from dwba_b200.dwba_matrix_elements import radial_ME_all_L_batch, radial_ME_all_L_sweep

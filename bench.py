@@ -154,13 +154,14 @@ def make_ragged_points(n_energy=64, l_max_wave=40, r_max=200.0, seed=3):
     return points
 
 
-def ragged_sweep(engine, L_max=6, replays=5, n_energy=64):
+def ragged_sweep(engine, L_max=6, replays=5, n_energy=64, points=None):
     """Device time of the ragged sweep (node sets, folds, forms and tails of all points in shared
-    launches, replayed from a CUDA graph)."""
+    launches, replayed from a CUDA graph). Returns (summary, [(I_dir, I_exc) per point])."""
     import torch
     from dwba_b200.dwba_matrix_elements import GPUCache, _make_job
     from dwba_b200.engine import MultiPrepared, PreparedJob
-    points = make_ragged_points(n_energy)
+    if points is None:
+        points = make_ragged_points(n_energy)
     kw = dict(use_oscillatory_quadrature=True, oscillatory_method="advanced", CC_nodes=5, phase_increment=1.5708,
               min_grid_fraction=0.10, k_threshold=0.5)
     parts = []
@@ -187,22 +188,48 @@ def ragged_sweep(engine, L_max=6, replays=5, n_energy=64):
     torch.cuda.synchronize()
     split = {f"{b[0]}_ms": a[1].elapsed_time(b[1]) for a, b in zip(marks[:-1], marks[1:])}
     stage_bytes = {"nodesets_ms": sum(p.nodesets.algorithmic_bytes() for p in parts if p.nodesets.n),
-                   "folds_ms": sum(p.fold_bytes() for p in parts),
-                   "forms_ms": sum(p.algorithmic_bytes() for p in parts)}
+                   "folds_ms": sum(p.fold_bytes() for p in parts)}
+    if engine == "semisep":
+        stage_bytes["forms_ms"] = sum(p.algorithmic_bytes() for p in parts)
     gbs = {k.replace("_ms", "_gbs"): stage_bytes[k] / (split[k] * 1e-3) / 1e9 for k in stage_bytes if split.get(k)}
     outs = mp.collect()
     finite = all(np.isfinite(d).all() and np.isfinite(e).all() for d, e in outs)
     n_int = sum(2 * p.T * p.P * p.nl for p in parts)
     n_energy = len(points) // 2
     Ns = [len(pt["grid"].r) for pt in points]
+    n_tail = int(sum(p.n_tail for p in parts))
+    mp.graph = None
+    del mp, parts
+    torch.cuda.empty_cache()
     return {"workload": f"ragged sweep: {n_energy} energies geomspace(45, 1000) eV, N_e = 2000..15000 "
                         f"(own grid per energy), He+-like 1s->2s and 1s->2p, l <= 40 parity-filtered, L=0..{L_max}, "
                         "Coulomb-like waves (eta = -1/k, n1 < N, outer tails on the device), synthetic",
             "engine": engine, "energies": n_energy, "points": len(points), "N_min": min(Ns), "N_max": max(Ns),
             "integrals": n_int, "ms_per_sweep": ms, "ms_per_energy": ms / n_energy,
             "integrals_per_s": n_int / (ms * 1e-3), "graph": True, "replays": replays,
-            "split_ms": split, "split_algorithmic_gbs": gbs,
-            "tail_records": int(sum(p.n_tail for p in parts)), "results_finite": bool(finite)}
+            "split_ms": split, "split_algorithmic_gbs": gbs, "tail_records": n_tail,
+            "results_finite": bool(finite)}, outs
+
+
+def sweep_tcs_errors(points, ref, test, L_max=6):
+    """Max and median relative TCS difference over the sweep's points between two engines' integrals
+    (the DCS is a quadratic form in the integrals; its prefactor and the 2/(pi k_i k_f) scale cancel
+    in the ratio, so one coupling table per transition serves every energy)."""
+    from dwba_b200.coupling import CouplingTables
+    theta = np.linspace(0.0, np.pi, 181)
+    tables = {}
+    rel = []
+    for pt, (rd, re_), (td, te) in zip(points, ref, test):
+        Lf = pt["bound_f"].l
+        chans = [(w_i.l, w_f.l) for w_i, w_f in pt["pairs"]]
+        key = (Lf, len(chans))
+        if key not in tables:
+            tables[key] = CouplingTables(theta, chans, L_max, 1.0, 1.0, 0, Lf)
+        tab = tables[key]
+        t_ref = tab.tcs(rd[0], re_[0])
+        rel.append(abs(tab.tcs(td[0], te[0]) - t_ref) / abs(t_ref))
+    rel = np.array(rel)
+    return float(rel.max()), float(np.median(rel))
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -533,9 +560,28 @@ def main():
                    "note": "whole step (node sets, folds, forms) on the same batch; the accuracy of each engine "
                            "against the reference's TCS is checked in tests/test_gpu_config1.py"}
 
+    # the 64-energy ragged sweep: exact FP64 (semiseparable) engine, and unless --no-compare the
+    # split-BF16 tensor-core engine and the plain FP64 kernel on the same points, with the TCS of
+    # every point from the split-BF16 integrals against the FP64 ones
     ragged = None
     if rank == 0 and world == 1 and not args.no_ragged and args.engine in ("semisep", "dense"):
-        ragged = ragged_sweep("semisep")
+        points = make_ragged_points()
+        ragged, ref_outs = ragged_sweep("semisep", points=points)
+        if not args.no_compare:
+            r_x3, x3_outs = ragged_sweep("tc_bf16x3", replays=3, points=points)
+            worst, med = sweep_tcs_errors(points, ref_outs, x3_outs)
+            del x3_outs
+            r_dense, dense_outs = ragged_sweep("dense", replays=1, points=points)
+            worst_d, _ = sweep_tcs_errors(points, ref_outs, dense_outs)
+            del dense_outs
+            ragged["engines"] = {
+                "tc_bf16x3_ms_per_sweep": r_x3["ms_per_sweep"], "dense_fp64_ms_per_sweep": r_dense["ms_per_sweep"],
+                "split_bf16_vs_plain_fp64_speedup": r_dense["ms_per_sweep"] / r_x3["ms_per_sweep"],
+                "semisep_fp64_vs_plain_fp64_speedup": r_dense["ms_per_sweep"] / ragged["ms_per_sweep"],
+                "tc_bf16x3_tcs_rel_err_max": worst, "tc_bf16x3_tcs_rel_err_median": med,
+                "dense_fp64_tcs_rel_err_max": worst_d,
+                "note": "TCS of every (energy, transition) point from each engine's integrals against the exact "
+                        "FP64 semiseparable engine's (which agrees with the oracle to 1e-12 per integral)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -471,11 +471,16 @@ def main():
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
 
+    # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu capture of
+    # the default workload (profiles/launches_semisep_synthetic_batch_N15000.md); other sizes: null
+    default_size = args.n_cont == N_CONT
+    traffic = {"nodeset_rows_kernel": 1.945e9, "fold_kernel": 4.894e9, "semisep_kernel": 3.223e9}
+
     def hbm_roof(kernel, nbytes, t_ms, note):
         ach = nbytes / (t_ms * 1e-3) / 1e9
         return {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
-                "traffic": None, "kernel": kernel, "ms": t_ms, "algorithmic_bytes": nbytes, "peak_source": peak_src,
-                "note": note}
+                "traffic": traffic.get(kernel) if default_size else None, "kernel": kernel, "ms": t_ms,
+                "algorithmic_bytes": nbytes, "peak_source": peak_src, "note": note}
     kernels = [
         hbm_roof("nodeset_rows_kernel", sum(p.nodesets.algorithmic_bytes() for p in preps), split["nodesets_ms"],
                  "algorithmic bytes = 8*(3*n1 + 5*N) operator doubles written + 8*2*N grid doubles read per "

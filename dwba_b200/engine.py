@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import ctypes
 from dataclasses import dataclass, field
+import hashlib
 from typing import Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
@@ -940,14 +941,51 @@ class MultiPrepared:
             self.prefix_d = _dev(prefix, dev)
             self.partial = torch.empty(self.n_cta * self.nl, dtype=torch.float64, device=dev)
         self.graph = None
-        # tensor-core engines: one launch sequence per job, spread over side streams (largest grids
-        # first) so that the small grids of low-energy points run side by side instead of each
-        # leaving most SMs idle in its last wave
+        # tensor-core engines: the direct forms of every job in one semiseparable launch (each
+        # descriptor names its own grid); the exchange forms of all jobs on equal grids (e.g. the
+        # transitions of one energy) in one tensor-core launch, so that their forms share the
+        # 256-wide form tiles; those launches and the jobs' tails go round-robin (largest grid
+        # first) over side streams, so that the small grids of low-energy points run side by side
+        # instead of each leaving most SMs idle in its last wave. The jobs' result buffers become
+        # views of the shared ones (jobs of a MultiPrepared are launched through it only).
         self.side_streams = []
         self.tc_order = []
+        self.tc_groups = []
         if self.engine in TC_TERMS:
+            nt = TC_TERMS[self.engine]
             self.side_streams = [torch.cuda.Stream(device=dev) for _ in range(min(4, len(parts)))]
             self.tc_order = sorted(range(len(parts)), key=lambda k: -parts[k].job.grid.N)
+            fd = np.concatenate([np.ascontiguousarray(p.forms_host[0::2]) for p in parts])
+            self.tc_n_dir = len(fd)
+            self.tc_dir_d = _dev(fd.view(np.uint8), dev)
+            self.tc_out_dir = torch.empty((len(fd), self.nl), dtype=torch.float64, device=dev)
+            by_grid: Dict[tuple, List[int]] = {}
+            off = 0
+            for k, p in enumerate(parts):
+                n = p.T * p.P
+                p.out_dir = self.tc_out_dir[off:off + n]
+                off += n
+                r = np.ascontiguousarray(p.job.grid.r, dtype=np.float64)
+                by_grid.setdefault((len(r), hashlib.sha1(r.tobytes()).hexdigest()), []).append(k)
+            for ks in sorted(by_grid.values(), key=lambda v: -parts[v[0]].job.grid.N):
+                fe = np.concatenate([np.ascontiguousarray(parts[k].forms_host[1::2]) for k in ks])
+                N = parts[ks[0]].job.grid.N
+                ws = int(self.lib.dwba_tc_workspace_bytes(len(fe), N, self.L_max, nt))
+                if ws < 0:
+                    raise ValueError("invalid tensor-core form sizes")
+                grp = {"forms": _dev(fe.view(np.uint8), dev), "n": len(fe), "N": N, "r": parts[ks[0]].dg.r,
+                       "ws": torch.empty(max(ws, 256), dtype=torch.uint8, device=dev),
+                       "status": torch.zeros(1, dtype=torch.int32, device=dev),
+                       "out": torch.empty((len(fe), self.nl), dtype=torch.float64, device=dev)}
+                off = 0
+                for k in ks:
+                    p = parts[k]
+                    n = p.T * p.P
+                    p.out_ex = grp["out"][off:off + n]
+                    p.tc_status = grp["status"]
+                    p.tc_ws = None  # the group's workspace serves it
+                    off += n
+                self.tc_groups.append(grp)
 
     def launch(self, marks: Optional[list] = None) -> None:
         """The launch sequence. With ``marks`` (a list), a CUDA event is recorded on the stream after
@@ -988,14 +1026,25 @@ class MultiPrepared:
                        "dwba_bilinear_semisep_fp64")
         else:
             main = torch.cuda.current_stream()
+            nt = TC_TERMS[self.engine]
             for stage in ("forms", "tails"):
                 for sd in self.side_streams:
                     sd.wait_stream(main)
-                for q, k in enumerate(self.tc_order):
-                    with torch.cuda.stream(self.side_streams[q % len(self.side_streams)]):
-                        if stage == "forms":
-                            self.parts[k].launch_forms()
-                        else:
+                if stage == "forms":
+                    # direct forms on the main stream, beside the tensor-core groups
+                    _lib.check(lib.dwba_bilinear_semisep_fp64(_ptr(self.tc_dir_d), self.tc_n_dir, self.L_max,
+                                                              self.ds.ctypes.data, self.r_min, self.r_max,
+                                                              _ptr(self.tc_out_dir), st),
+                               "dwba_bilinear_semisep_fp64")
+                    for q, g in enumerate(self.tc_groups):
+                        sd = self.side_streams[q % len(self.side_streams)]
+                        _lib.check(lib.dwba_bilinear_tc_bf16(_ptr(g["forms"]), g["n"], _ptr(g["r"]), g["N"], self.L_max,
+                                                             nt, self.ds.ctypes.data, _ptr(g["ws"]), g["ws"].numel(),
+                                                             _ptr(g["status"]), _ptr(g["out"]), int(sd.cuda_stream)),
+                                   "dwba_bilinear_tc_bf16")
+                else:
+                    for q, k in enumerate(self.tc_order):
+                        with torch.cuda.stream(self.side_streams[q % len(self.side_streams)]):
                             self.parts[k].launch_tails()
                 for sd in self.side_streams:
                     main.wait_stream(sd)

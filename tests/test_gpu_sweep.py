@@ -29,6 +29,26 @@ def test_sweep_matches_per_energy(engine, graph):
                 assert a.I_L_exchange[L] == b.I_L_exchange[L]
 
 
+@pytest.mark.parametrize("engine", ["semisep", "tc_bf16x3"])
+def test_sweep_points_sharing_a_grid_match_per_energy(engine):
+    """Two transitions on one grid object (as at one energy of a sweep) share the tensor-core
+    launch of their exchange forms; every integral equals the per-point evaluation."""
+    from dwba_b200.dwba_matrix_elements import radial_ME_all_L_batch, radial_ME_all_L_sweep
+    first = _point(1203, 2, n_pairs=150)
+    second = _point(1203, 5, n_pairs=130)
+    second["grid"] = first["grid"]
+    points = [first, second, _point(801, 1)]
+    L_max = 4
+    swept = radial_ME_all_L_sweep(points, L_max, engine=engine, graph=True, replays=1)
+    for pt, res in zip(points, swept):
+        ref = radial_ME_all_L_batch(pt["grid"], pt["V_core_array"], pt["U_i_array"], pt["bound_i"], pt["bound_f"],
+                                    pt["pairs"], L_max, U_f_array=pt["U_f_array"], engine=engine)
+        for a, b in zip(res, ref):
+            for L in range(L_max + 1):
+                assert a.I_L_direct[L] == b.I_L_direct[L]
+                assert a.I_L_exchange[L] == b.I_L_exchange[L]
+
+
 def test_sweep_coulomb_points_with_tails_match_reference():
     """Ragged sweep over the golden energy points (Coulomb waves with n1 < N and outer tails on
     the device, H 1s->2p, the low-k standard path): each point equals the reference's I_L."""

@@ -232,6 +232,174 @@ def sweep_tcs_errors(points, ref, test, L_max=6):
     return float(rel.max()), float(np.median(rel))
 
 
+# ----------------------------------------------------------------------------- ionization workload
+IONIZATION_WORKLOAD = ("ionization SDCS: H 1s, E = 200 eV, 40 ejected energies linspace(0.5, 99) eV, N=8000 exp grid "
+                       "r in [1e-5,200], l_i, l_f, l_ej <= 30 parity-filtered, L=0..10, Coulomb-like synthetic waves")
+
+
+class _Continuum(_Wave):
+    """A continuum final state (ejected electron): carries chi_of_r, and u_of_r as the reference's does."""
+
+    @property
+    def u_of_r(self):
+        return self.chi_of_r
+
+
+def make_ionization_points(n_ej=40, l_max=30, N=8000, r_max=200.0, seed=5):
+    """H 1s ionization at 200 eV with the shapes of the reference's SDCS loop (ionization.py:526-608):
+    per ejected energy, one transition per ejected partial wave l_ej, all (l_i, l_f) pairs with
+    l_i + l_f = l_ej (mod 2); the two parity classes are two points on the one grid. Coulomb-like
+    synthetic waves (z = 1, matching index inside the grid) stand in for the solver's."""
+    rng = np.random.default_rng(seed)
+    hartree, E, IP = 27.211386245988, 200.0, 13.605693
+    g = make_grid(N, 1e-5, r_max)
+    r = g.r
+    bound = _Bound(0, 2.0 * r * np.exp(-r))
+    V = -1.0 / r
+    im = int(np.searchsorted(r, 0.6 * r_max))
+
+    def wave(l, k, cls=_Wave):
+        eta = -1.0 / k
+        d, sig = float(rng.uniform(0, np.pi)), float(rng.uniform(-1, 1))
+        chi = np.sin(k * r - 0.5 * l * np.pi + eta * np.log(2 * k * r) + sig + d) * \
+            (1.0 - np.exp(-(r / ((l + 1) / k)) ** (l + 1)))
+        w = cls(l, k, d, chi)
+        w.eta, w.sigma_l, w.idx_match = eta, sig, im
+        return w
+    k_i = np.sqrt(2.0 * E / hartree)
+    incident = [wave(l, k_i) for l in range(l_max + 1)]
+    points = []
+    for E_ej in np.linspace(0.5, 99.0, n_ej):
+        k_ej = np.sqrt(2.0 * E_ej / hartree)
+        k_s = np.sqrt(2.0 * (E - IP - E_ej) / hartree)
+        scat = [wave(l, k_s) for l in range(l_max + 1)]
+        ej = [wave(l, k_ej, _Continuum) for l in range(l_max + 1)]
+        for par in (0, 1):
+            pairs = [(incident[a], scat[b]) for a in range(l_max + 1) for b in range(l_max + 1) if (a + b) % 2 == par]
+            lej = [l for l in range(l_max + 1) if l % 2 == par]
+            points.append(dict(grid=g, V_core_array=V, U_i_array=V, bound_i=[bound] * len(lej),
+                               bound_f=[ej[l] for l in lej], pairs=pairs, U_f_array=V, E_ej=float(E_ej),
+                               k=(k_i, k_s, k_ej), l_ej=lej))
+    return points
+
+
+def ionization_sweep(engine, points, L_max=10, chunk=16, replays=2):
+    """Device time of all points, in chunks of `chunk` points (one MultiPrepared and one CUDA graph
+    each, since every point holds its folded operands). Returns (ms, [(I_dir, I_exc) per point])."""
+    import torch
+    from dwba_b200.dwba_matrix_elements import GPUCache, _make_job
+    from dwba_b200.engine import MultiPrepared, PreparedJob
+    kw = dict(use_oscillatory_quadrature=True, oscillatory_method="advanced", CC_nodes=5, phase_increment=1.5708,
+              min_grid_fraction=0.10, k_threshold=0.5)
+    cache = GPUCache(points[0]["grid"])
+    total, outs = 0.0, []
+    st = torch.cuda.current_stream()
+    for c0 in range(0, len(points), chunk):
+        parts = []
+        for pt in points[c0:c0 + chunk]:
+            job = _make_job(pt["grid"], pt["V_core_array"], pt["U_i_array"], pt["bound_i"], pt["bound_f"],
+                            pt["pairs"], L_max, pt["U_f_array"], kw, cache)
+            parts.append(PreparedJob(job, cache.dg, engine, rebuild_nodesets=True))
+        mp = MultiPrepared(parts)
+        mp.capture()
+        mp.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(replays):
+            mp.replay()
+        e1.record(st)
+        e1.synchronize()
+        total += e0.elapsed_time(e1) / replays
+        outs.extend(mp.collect())
+        mp.graph = None
+        del mp, parts
+        torch.cuda.empty_cache()
+    return total, outs
+
+
+class IonizationSDCS:
+    """Angle-integrated SDCS per ejected energy from the integrals, with the reference's algebra
+    (ionization.py:610-642, dwba_coupling.py:507-620): per (l_ej, l_f, M_f) the direct and exchange
+    amplitudes summed coherently over l_i, then 0.25|f+g|^2 + 0.75|f-g|^2, times
+    (2 pi)^4 (k_s k_ej / k_i) and the amplitude prefactor (2/pi)/(k_i k_s) sqrt(2/pi)/k_ej squared.
+    The channel coefficients depend only on angular momenta and are built once per parity class."""
+
+    def __init__(self, points, L_max=10):
+        from dwba_b200.coupling import channel_coefficients
+        self.L_max = L_max
+        self.tabs = {}
+        for pt in points[:2]:
+            par = pt["l_ej"][0] % 2
+            li = np.array([a.l for a, _ in pt["pairs"]])
+            lf = np.array([b.l for _, b in pt["pairs"]])
+            per_t = []
+            for l_ej in pt["l_ej"]:
+                per_m = []
+                for Mf in range(-l_ej, l_ej + 1):
+                    cf = np.zeros((len(li), L_max + 1), dtype=complex)
+                    cg = np.zeros_like(cf)
+                    for p in range(len(li)):
+                        cf[p], cg[p] = channel_coefficients(int(li[p]), int(lf[p]), L_max, 0, l_ej, 0, Mf)
+                    per_m.append((cf, cg))
+                per_t.append(per_m)
+            self.tabs[par] = (lf, per_t)
+
+    def sdcs(self, pt, I_dir, I_exc):
+        lf, per_t = self.tabs[pt["l_ej"][0] % 2]
+        k_i, k_s, k_ej = pt["k"]
+        amp = (2.0 / np.pi) / (k_i * k_s) * np.sqrt(2.0 / np.pi) / k_ej
+        tot = 0.0
+        for t, per_m in enumerate(per_t):
+            for cf, cg in per_m:
+                f = np.einsum("pl,pl->p", cf, I_dir[t]) * amp
+                g = np.einsum("pl,pl->p", cg, I_exc[t]) * amp
+                F = np.bincount(lf, f.real, minlength=lf.max() + 1) + 1j * np.bincount(lf, f.imag, minlength=lf.max() + 1)
+                G = np.bincount(lf, g.real, minlength=lf.max() + 1) + 1j * np.bincount(lf, g.imag, minlength=lf.max() + 1)
+                tot += float(np.sum(0.25 * np.abs(F + G) ** 2 + 0.75 * np.abs(F - G) ** 2))
+        return (2.0 * np.pi) ** 4 * (k_s * k_ej / k_i) * tot
+
+
+def ionization_run(compare=True):
+    """The ionization workload through the exact FP64 engine and the split-BF16 engine (and the plain
+    FP64 kernel on one ejected energy); SDCS per ejected energy and the trapezoid TICS over them."""
+    import torch
+    points = make_ionization_points()
+    n_int = sum(2 * len(pt["l_ej"]) * len(pt["pairs"]) * 11 for pt in points)
+    ms_ss, ref = ionization_sweep("semisep", points)
+    res = {"workload": IONIZATION_WORKLOAD, "integrals": n_int, "points": len(points),
+           "semisep_ms": ms_ss, "semisep_integrals_per_s": n_int / (ms_ss * 1e-3),
+           "semisep_ms_per_ejected_energy": ms_ss / (len(points) // 2)}
+    if compare:
+        ms_tc, tc = ionization_sweep("tc_bf16x3", points)
+        ms_dense, _ = ionization_sweep("dense", points[:2], replays=1)
+        n_e = len(points) // 2
+        sd = IonizationSDCS(points)
+        E = np.array([pt["E_ej"] for pt in points[0::2]])
+        s_ref = np.array([sd.sdcs(points[2 * e], *ref[2 * e]) + sd.sdcs(points[2 * e + 1], *ref[2 * e + 1])
+                          for e in range(n_e)])
+        s_tc = np.array([sd.sdcs(points[2 * e], *tc[2 * e]) + sd.sdcs(points[2 * e + 1], *tc[2 * e + 1])
+                         for e in range(n_e)])
+        rel = np.abs(s_tc - s_ref) / np.abs(s_ref)
+        tics_ref, tics_tc = np.trapezoid(s_ref, E), np.trapezoid(s_tc, E)
+        # integral-level errors of the split form against the exact FP64 integrals, relative to the
+        # largest integral of the same kind (direct / exchange) and transition
+        dI = np.concatenate([np.abs(np.stack(a) - np.stack(b)).ravel() for a, b in zip(tc, ref)])
+        sc = np.concatenate([np.broadcast_to(np.max(np.abs(np.stack(b)), axis=(2, 3), keepdims=True),
+                                             np.stack(b).shape).ravel() for b in ref])
+        res.update({"tc_bf16x3_ms": ms_tc, "tc_bf16x3_integrals_per_s": n_int / (ms_tc * 1e-3),
+                    "dense_fp64_ms_one_ejected_energy": ms_dense, "dense_fp64_ms_scaled": ms_dense * n_e,
+                    "split_bf16_vs_plain_fp64_speedup": ms_dense * n_e / ms_tc,
+                    "semisep_vs_plain_fp64_speedup": ms_dense * n_e / ms_ss,
+                    "tc_bf16x3_sdcs_rel_err_max": float(rel.max()), "tc_bf16x3_sdcs_rel_err_median": float(np.median(rel)),
+                    "tc_bf16x3_tics_rel_err": float(abs(tics_tc - tics_ref) / abs(tics_ref)),
+                    "tc_bf16x3_max_abs_err_over_transition_max": float(np.max(dI / np.maximum(sc, 1e-300))),
+                    "note": "SDCS per ejected energy from each engine's integrals (reference algebra, angle-integrated), "
+                            "TICS by the trapezoid rule over the 40 ejected energies; the plain FP64 kernel is timed "
+                            "on the first ejected energy and scaled by 40"})
+    return res
+
+
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
@@ -371,9 +539,16 @@ def main():
     ap.add_argument("--no-ragged", action="store_true", help="skip the ragged multi-energy sweep")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip timing the split-BF16 and plain FP64 engines on the same batch")
+    ap.add_argument("--workload", default="batch", choices=["batch", "ionization"],
+                    help="ionization: the H 1s ionization SDCS workload instead of the kernel batch (one GPU)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "ionization":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(ionization_run(compare=not args.no_compare)))
+        return 0
     import torch
     import torch.distributed as dist
     from dwba_b200.dwba_matrix_elements import GPUCache, _make_job, radial_ME_all_L_batch

@@ -116,6 +116,8 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
   const double* __restrict__ r = s.r;
   const int lane = threadIdx.x;
   const double r_first = r[0], r_lim = r[n1 - 1], r_last = r[N - 1];
+  // with n1 == N and one spacing test for both, the B taps of a node are its T taps
+  const bool shared = s.log1 == s.log2 && n1 == N;
 
   for (int k0 = blockIdx.x * OWN_ROWS; k0 < N; k0 += gridDim.x * OWN_ROWS) {
     const int g = k0 - 2 + lane;
@@ -156,9 +158,9 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
           const double lx = (s.log1 || s.log2) ? log(x) : 0.0;
           const bool at_top = x >= rg1;  // floor index in the full grid: g + 1 at r_{g+1}, else g
           // --- T: rows j1 and j1 + 1, j1 in {g, g+1}
+          int j1;
+          double t1;
           {
-            int j1;
-            double t1;
             if (x <= r_first) { j1 = 0; t1 = 0.0; }
             else if (x >= r_lim) { j1 = n1 - 2; t1 = 1.0; }
             else {
@@ -183,7 +185,8 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
           {
             int j2;
             double t2;
-            if (x <= r_first) { j2 = 0; t2 = 0.0; }
+            if (shared) { j2 = j1; t2 = t1; }
+            else if (x <= r_first) { j2 = 0; t2 = 0.0; }
             else if (x >= r_last) { j2 = N - 2; t2 = 1.0; }
             else {
               j2 = (at_top && g + 1 <= N - 2) ? g + 1 : g;

@@ -528,7 +528,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)  # ~0.3 s timed: several clock samples
+    ap.add_argument("--steps", type=int, default=150)  # ~0.9 s timed: several 200 ms clock samples
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--engine", default=os.environ.get("DWBA_BENCH_ENGINE", "semisep"),

@@ -143,7 +143,7 @@ __device__ __forceinline__ void envelopes(const double* m, int L0, int nl, doubl
 
 // Re of the Filon integral over one segment (nn equally spaced nodes, nn odd) for every multipole
 // of the chunk: _filon_segment_complex with the node phases and the panel weights shared by all L
-__device__ __noinline__ void filon_segment_all(const double* m, int L0, int nl, double a, double b, int nn, double omega,
+__device__ __forceinline__ void filon_segment_all(const double* m, int L0, int nl, double a, double b, int nn, double omega,
                                   double off, KSum* acc) {
   if (!(b - a >= 1e-15)) return;
   double f0[LC], f1[LC], f2[LC];

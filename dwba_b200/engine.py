@@ -301,8 +301,19 @@ class WaveMatrix:
         self.arrays: List[np.ndarray] = []
         self.ptrs: List[int] = []
         self._uploaded: Dict[str, Tuple[int, torch.Tensor]] = {}
+        self._by_id: Dict[int, int] = {}
+        self._keep: List[object] = []
 
     def add(self, arr: np.ndarray) -> int:
+        i = self._by_id.get(id(arr))
+        if i is not None:
+            return i
+        i = self._add(arr)
+        self._by_id[id(arr)] = i
+        self._keep.append(arr)  # keeps id(arr) from being reused while the memo holds it
+        return i
+
+    def _add(self, arr: np.ndarray) -> int:
         a = np.asarray(arr)
         ptr = a.__array_interface__["data"][0]
         key = (ptr, a.strides[0] if a.ndim else 0)
@@ -360,11 +371,13 @@ class WaveMatrix:
         for base, idx, rows in groups.values():
             if len(idx) < 2 or 2 * len(set(rows)) < base.shape[0]:
                 continue  # a small share of a large matrix: per-row copies below
+            # the (small, synchronous) index copies first, so that the host does not wait for the
+            # large asynchronous copy of the matrix behind them
+            sel = torch.as_tensor(np.asarray(rows, dtype=np.int64), device=device)
+            dst = torch.as_tensor(np.asarray(idx, dtype=np.int64), device=device)
             src = torch.from_numpy(base)
             dev_base = src.to(device, non_blocking=src.is_pinned())
-            sel = torch.as_tensor(np.asarray(rows, dtype=np.int64), device=device)
-            out[torch.as_tensor(np.asarray(idx, dtype=np.int64), device=device)] = \
-                dev_base.index_select(0, sel)[:, :N]
+            out[dst] = dev_base.index_select(0, sel)[:, :N]
             done[idx] = True
         i = 0
         while i < n:

@@ -400,6 +400,70 @@ def ionization_run(compare=True):
     return res
 
 
+# ----------------------------------------------------------------------------- gradients
+def gradient_run(reps=3):
+    """Forward and forward+backward through the differentiable integrals (RadialIntegrals) at the
+    differentiation config's sizes: N = 6000 on [1e-5, 200], l_i, l_f <= 25 with l_i + l_f odd
+    (338 pairs, one s->p transition), L = 0..4, live L=0 correction (V_core != U_i). Inputs are
+    CUDA tensors; the time includes the host planning that every call repeats."""
+    import torch
+    from dwba_b200.autograd import RadialIntegrals
+    rng = np.random.default_rng(9)
+    g = make_grid(6000, 1e-5, 200.0)
+    r = g.r
+    V = -(1.0 + 10.0 * np.exp(-3.0 * r) + 2.0 * r * np.exp(-1.5 * r) + np.exp(-0.8 * r)) / r
+    U = V + 0.3 * np.exp(-r)
+    u_s = r * np.exp(-r) * (1.0 - 0.4 * r + 0.03 * r * r)
+    u_p = r * r * np.exp(-0.7 * r) * (1.0 - 0.1 * r)
+    bi, bf = _Bound(0, u_s / np.sqrt(np.sum(g.w_trapz * u_s ** 2))), _Bound(1, u_p / np.sqrt(np.sum(g.w_trapz * u_p ** 2)))
+    k_i, k_f = 1.21, 1.02
+
+    def wave(l, k):
+        d = float(rng.uniform(0, np.pi))
+        return _Wave(l, k, d, np.sin(k * r - 0.5 * l * np.pi + d) * (1.0 - np.exp(-(r / ((l + 1) / k)) ** (l + 1))))
+    wi = [wave(l, k_i) for l in range(26)]
+    wf = [wave(l, k_f) for l in range(26)]
+    pairs = [(wi[a], wf[b]) for a in range(26) for b in range(26) if (a + b) % 2 == 1]
+    model = RadialIntegrals(g, bi, bf, pairs, 4, U_f_array=U, engine="semisep")
+    model_tc = RadialIntegrals(g, bi, bf, pairs, 4, U_f_array=U, engine="semisep", backward="tc_bf16x3",
+                               gpu_cache=model.cache)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")  # noqa: E731
+    x = dict(V_core=t(V), U_i=t(U), u_i=t(bi.u_of_r), u_f=t(bf.u_of_r),
+             chi_i=t(np.stack([p[0].chi_of_r for p in pairs])), chi_f=t(np.stack([p[1].chi_of_r for p in pairs])))
+    c = t(rng.normal(size=(len(pairs), 2, 5)))
+
+    def fwd():
+        with torch.no_grad():
+            return float((model(**x) * c).sum())
+
+    def fwd_bwd(m=model):
+        xs = {k: v.clone().requires_grad_(True) for k, v in x.items()}
+        loss = (m(**xs) * c).sum()
+        loss.backward()
+        return {k: v.grad for k, v in xs.items()}
+    g64 = fwd_bwd()
+    gtc = fwd_bwd(model_tc)
+    rel = {k: float(torch.linalg.norm(gtc[k] - g64[k]) / torch.linalg.norm(g64[k])) for k in g64}
+    fwd()
+    torch.cuda.synchronize()
+    out = {}
+    for name, fn in (("forward_ms", fwd), ("forward_backward_ms", fwd_bwd),
+                     ("forward_backward_tc_bf16x3_ms", lambda: fwd_bwd(model_tc))):
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        out[name] = (time.perf_counter() - t0) * 1e3 / reps
+    return {"workload": "differentiation sizes: N=6000 exp grid r in [1e-5,200], 338 (l_i, l_f <= 25) pairs of one "
+                        "s->p transition, L=0..4, parametric SAE-like V_core, synthetic waves",
+            "integrals": len(pairs) * 2 * 5, "gradient_inputs": "V_core, U_i, u_i, u_f, chi_i, chi_f",
+            **out, "tc_bf16x3_vs_fp64_gradient_rel_err": rel,
+            "note": "wall time per call through RadialIntegrals (host planning, FP64 forward, exact FP64 backward "
+                    "kernels, or the split-BF16 tensor-core backward with FP32 accumulation); rel err = |g_tc - "
+                    "g_fp64| / |g_fp64| per input; the FP64 gradients are checked against central differences in "
+                    "tests/test_gpu_autograd.py"}
+
+
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
@@ -763,6 +827,10 @@ def main():
                 "note": "TCS of every (energy, transition) point from each engine's integrals against the exact "
                         "FP64 semiseparable engine's (which agrees with the oracle to 1e-12 per integral)"}
 
+    grad = None
+    if rank == 0 and world == 1 and not args.no_ragged and args.engine in ("semisep", "dense"):
+        grad = gradient_run()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ips, dt, rows = cpu_sample(seconds_hint=15.0)
@@ -784,7 +852,7 @@ def main():
                 "config": {"workload": WORKLOAD, "engine": args.engine, "integrals_per_step_per_gpu": n_int,
                            "l2": "inputs larger than L2 (operands ~1 GB/step)", "parallelism": f"dp{world}"},
                 "split_ms": split, "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu,
-                "engines": compare, "ragged_sweep": ragged,
+                "engines": compare, "ragged_sweep": ragged, "gradient": grad,
                 "gpu_launches": n_launch * args.steps, "results_finite": bool(finite and nonzero), "clocks": clk.summary()}
         print(json.dumps(line))
     if world > 1:

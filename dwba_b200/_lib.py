@@ -73,6 +73,9 @@ def _declare(lib):
         "dwba_outer_tails_batch": (c_int, [c_vp, c_int, c_int, c_int, c_dbl, c_vp]),
         "dwba_bilinear_semisep_backward_fp64": (c_int, [c_vp, c_int, c_int, c_vp, c_vp, c_dbl, c_dbl, c_vp]),
         "dwba_fold_adjoint": (c_int, [c_vp, c_int, c_int, c_vp]),
+        "dwba_tc_backward_workspace_bytes": (c_i64, [c_int, c_int, c_int, c_int]),
+        "dwba_bilinear_tc_bf16_backward": (c_int, [c_vp, c_int, c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_i64,
+                                                   c_vp, c_vp]),
         "dwba_fold_multi": (c_int, [c_vp, c_int, c_int, c_vp]),
         "dwba_cross_sections": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_dbl,
                                         c_vp, c_vp, c_vp]),

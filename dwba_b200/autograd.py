@@ -9,7 +9,8 @@ radial functions and potentials: chi_i, chi_f (P, N), u_i, u_f, V_core, U_i (N).
 
 * the bilinear part a^T K_L b runs on the CUDA engine forward (any engine) and backward
   (dwba_bilinear_semisep_backward_fp64: dLoss/da = K_g b, dLoss/db = K_g a with
-  K_g = sum_L g_L K_L, exact FP64; then dwba_fold_adjoint for the banded folds);
+  K_g = sum_L g_L K_L, exact FP64, or dwba_bilinear_tc_bf16_backward on the tensor cores;
+  then dwba_fold_adjoint for the banded folds);
 * the L=0 correction c_L (dwba_matrix_elements.py:1249-1296) and the outer tail
   t_L = tau_L M_L (dwba_matrix_elements.py:1213-1241; tau_L = tail per unit multipole moment,
   M_L = sum w r^L u_f u_i) are torch expressions, differentiated by autograd.
@@ -83,9 +84,24 @@ class _BilinearFn(torch.autograd.Function):
         desc["n_rows"], desc["n_cols"] = fh["n_rows"], fh["n_cols"]
         desc_d = _dev(desc, dev)
         g = pj.job.grid
-        _lib.check(lib.dwba_bilinear_semisep_backward_fp64(_ptr(desc_d), nf, pj.job.L_max, pj.ds.ctypes.data,
-                                                           _ptr(G), float(g.r[0]), float(g.r[-1]), _stream()),
-                   "dwba_bilinear_semisep_backward_fp64")
+        bwd = getattr(ctx.state, "backward", "fp64")
+        if bwd in TC_TERMS:
+            nt = TC_TERMS[bwd]
+            ws_bytes = int(lib.dwba_tc_backward_workspace_bytes(nf, N, pj.job.L_max, nt))
+            if ws_bytes < 0:
+                raise ValueError("invalid tensor-core form sizes")
+            ws = torch.empty(max(ws_bytes, 256), dtype=torch.uint8, device=dev)
+            status = torch.zeros(1, dtype=torch.int32, device=dev)
+            _lib.check(lib.dwba_bilinear_tc_bf16_backward(_ptr(desc_d), nf, _ptr(pj.dg.r), N, pj.job.L_max, nt,
+                                                          pj.ds.ctypes.data, _ptr(G), _ptr(ws), ws.numel(),
+                                                          _ptr(status), _stream()),
+                       "dwba_bilinear_tc_bf16_backward")
+            if int(status.item()) != 0:
+                raise _lib.DWBAError(_lib.DWBA_ERR_RANGE, "dwba_bilinear_tc_bf16_backward: a bounded wait expired")
+        else:
+            _lib.check(lib.dwba_bilinear_semisep_backward_fp64(_ptr(desc_d), nf, pj.job.L_max, pj.ds.ctypes.data,
+                                                               _ptr(G), float(g.r[0]), float(g.r[-1]), _stream()),
+                       "dwba_bilinear_semisep_backward_fp64")
         # gradients of the folded operands (rows of pj.ops), summed over the forms that read them
         ops = pj.ops
         Op = np.uint64(_ptr(ops))
@@ -133,10 +149,13 @@ class RadialIntegrals:
     call); ``pairs``: (cont_i, cont_f) objects with the ContinuumWave attributes (their chi_of_r is
     replaced by the rows of ``chi_i``/``chi_f``). Options as in ``radial_ME_all_L``.
     Calling the object with torch float64 CUDA tensors returns (P, 2, L_max+1).
+    ``backward``: "fp64" (exact O(N L) FP64 kernels) or "tc_bf16x3" / "tc_bf16x6" (the K_L products
+    of the gradients on the tensor cores with FP32 accumulation, weighted and summed over L in FP64).
     """
 
     def __init__(self, grid, bound_i, bound_f, pairs: Sequence, L_max: int, U_f_array: Optional[np.ndarray] = None,
-                 engine: Optional[str] = None, gpu_cache: Optional[GPUCache] = None, **options):
+                 engine: Optional[str] = None, gpu_cache: Optional[GPUCache] = None, backward: str = "fp64",
+                 **options):
         self.grid, self.bound_i, self.bound_f = grid, bound_i, bound_f
         self.pairs = list(pairs)
         self.L_max = int(L_max)
@@ -144,6 +163,9 @@ class RadialIntegrals:
         eng = _engine_name(engine)
         # the autotuned names choose per call; the differentiable path uses one fixed forward engine
         self.engine = {"auto": "semisep", "auto_split": "tc_bf16x3"}.get(eng, eng)
+        if backward != "fp64" and backward not in TC_TERMS:
+            raise ValueError(f"backward must be 'fp64' or one of {sorted(TC_TERMS)}")
+        self.backward = backward
         self.cache = gpu_cache or GPUCache(grid)
         self.options = dict(use_oscillatory_quadrature=options.get("use_oscillatory_quadrature", True),
                             oscillatory_method=options.get("oscillatory_method", "advanced"),
@@ -171,6 +193,7 @@ class RadialIntegrals:
         plans = plan_job(job)
         state = _State()
         state.prepared = PreparedJob(job, self.cache.dg, self.engine, plans=plans)
+        state.backward = self.backward
         I = _BilinearFn.apply(chi_i, chi_f, u_i, u_f, state)
         dev = chi_i.device
         nl = self.L_max + 1

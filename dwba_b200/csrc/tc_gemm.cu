@@ -51,7 +51,9 @@ struct GemmParams {
   const float* vt;             // [2][n_L][n_pad] column factors within each j block (below, above)
   const float* st;             // [n_L][n_iblk][n_kb] per (row block, j block) scale (0 where K is not rank one)
   int* status;                 // error word
-  int n_grid, n_pad, f_pad, n_iblk, L_max, n_forms, n_kb;
+  const double* gw;            // gradient mode: dLoss/dI per (form, L), [n_forms][n_Ltot]
+  double* gpart;               // gradient mode: g_f,L (K_L b_f)_i per L, [n_L][f_pad][n_pad]
+  int n_grid, n_pad, f_pad, n_iblk, L_max, n_forms, n_kb, n_Ltot;
   double diag[DWBA_MAX_L + 1];
 };
 
@@ -200,7 +202,9 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 // largest radius of the row block, c_b: first radius of the j block):
 //   below the diagonal: K = r_j^L / r_i^(L+1) = [c_lo^L / r_i^(L+1)] [(c_b/c_lo)^L] [(r_j/c_b)^L]
 //   above the diagonal: K = r_i^L / r_j^(L+1) = [(r_i/c_hi)^L] [c_hi^L / c_b^(L+1)] [(r_j/c_b)^-(L+1)]
-template <int NT, int BN>
+// GRAD = false: I_f,L = sum_i a_f[i] Z_L[i, f] (partials per row block). GRAD = true (backward):
+// the epilogue writes g_f,L Z_L[i, f] for every row i instead, summed over L afterwards.
+template <int NT, int BN, bool GRAD>
 __global__ void __launch_bounds__(THREADS, 1)
 tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P) {
   constexpr int B_BYTES = BN * BK * 2;            // one term
@@ -428,7 +432,24 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
   __syncthreads();
   const bool ok = !s_abort;
   tc_fence_after();
-  if (ok && warp >= 1) {
+  if (GRAD && ok && warp >= 1) {
+    // gradient epilogue: every (row, form) value times the form's upstream gradient for this L;
+    // the lanes of a warp write 32 consecutive rows of one form
+    const int g = warp & 3, h = (warp - 1) >> 2;
+    const int i = i0 + 32 * g + lane;
+    for (int c0 = h * (BN / 4); c0 < (h + 1) * (BN / 4); c0 += 32) {
+      float z[32];
+      tmem_ld32(tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)c0, z);
+#pragma unroll
+      for (int c = 0; c < 32; ++c) {
+        const int f = f0 + c0 + c;
+        if (f < P.n_forms && i < P.n_grid)
+          P.gpart[((int64_t)L * P.f_pad + f) * P.n_pad + i] =
+              ldexp((double)z[c], P.bexp[f]) * P.gw[(int64_t)f * P.n_Ltot + L];
+      }
+    }
+  }
+  if (!GRAD && ok && warp >= 1) {
     // epilogue: warp w reads TMEM lanes 32*(w%4).. (its lane quarter); the four warps of a quarter
     // split the columns
     const int g = warp & 3, h = (warp - 1) >> 2;
@@ -455,7 +476,7 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
   }
   tc_fence_before();
   __syncthreads();
-  if (ok) {
+  if (!GRAD && ok) {
     for (int c = tid; c < BN; c += THREADS) {
       const double v = sRed[0][c] + sRed[1][c] + sRed[2][c] + sRed[3][c];
       P.partial[((int64_t)L * P.n_iblk + iblk) * P.f_pad + f0 + c] = v;
@@ -559,6 +580,40 @@ __global__ void tc_reduce_kernel(const double* __restrict__ partial, int n_forms
   out[idx] = s;
 }
 
+// backward: the two form sets whose B operand is b (for dLoss/da) and a (for dLoss/db)
+__global__ void tc_grad_forms_kernel(const dwba_form_grad_t* __restrict__ in, int n, dwba_form_t* __restrict__ for_a,
+                                     dwba_form_t* __restrict__ for_b) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n) return;
+  const dwba_form_grad_t G = in[f];
+  for_a[f].r_dev = G.r_dev;
+  for_a[f].a_dev = G.a_dev;
+  for_a[f].b_dev = G.b_dev;
+  for_a[f].n_rows = G.n_rows;
+  for_a[f].n_cols = G.n_cols;
+  for_b[f].r_dev = G.r_dev;
+  for_b[f].a_dev = G.b_dev;
+  for_b[f].b_dev = G.a_dev;
+  for_b[f].n_rows = G.n_cols;
+  for_b[f].n_cols = G.n_rows;
+}
+
+// ga_f[i] (which = 0, i < n_rows) or gb_f[i] (which = 1, i < n_cols) = sum over L of the partials
+__global__ void tc_grad_reduce_kernel(const double* __restrict__ gpart, const dwba_form_grad_t* __restrict__ forms,
+                                      int n_forms, int f_pad, int n_pad, int n_L, int which) {
+  const int64_t total = (int64_t)n_forms * n_pad;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int f = (int)(idx / n_pad), i = (int)(idx - (int64_t)f * n_pad);
+    const dwba_form_grad_t& G = forms[f];
+    const int len = which == 0 ? G.n_rows : G.n_cols;
+    if (i >= len) continue;
+    double s = 0.0;
+    for (int L = 0; L < n_L; ++L) s += gpart[((int64_t)L * f_pad + f) * n_pad + i];
+    (which == 0 ? G.ga_dev : G.gb_dev)[i] = s;
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -571,7 +626,7 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   return fn;
 }
 
-template <int NT, int BN>
+template <int NT, int BN, bool GRAD = false>
 int launch_tc(const GemmParams& P, const __nv_bfloat16* bterms, int n_L, cudaStream_t st) {
   auto encode = get_encode();
   if (!encode) return DWBA_ERR_CUDA;
@@ -585,11 +640,11 @@ int launch_tc(const GemmParams& P, const __nv_bfloat16* bterms, int n_L, cudaStr
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) return DWBA_ERR_CUDA;
   const int smem = tc_stages(NT) * NT * (BN * BK * 2) + 1024;
-  if (cudaFuncSetAttribute(tc_exchange_kernel<NT, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+  if (cudaFuncSetAttribute(tc_exchange_kernel<NT, BN, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
       cudaSuccess)
     return DWBA_ERR_CUDA;
   dim3 grid(P.n_iblk, P.f_pad / BN, n_L);
-  tc_exchange_kernel<NT, BN><<<grid, THREADS, smem, st>>>(map, P);
+  tc_exchange_kernel<NT, BN, GRAD><<<grid, THREADS, smem, st>>>(map, P);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;
 }
@@ -634,6 +689,9 @@ extern "C" int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, 
   P.forms = forms_dev;
   P.n_forms = n_forms;
   P.status = status_dev;
+  P.gw = nullptr;
+  P.gpart = nullptr;
+  P.n_Ltot = L_max + 1;
   for (int l = 0; l <= DWBA_MAX_L; ++l) P.diag[l] = l <= L_max ? diag_scale_host[l] : 0.0;
   uint8_t* ws = (uint8_t*)workspace;
   const int64_t bbytes = (int64_t)n_terms * P.f_pad * P.n_pad * 2;
@@ -675,5 +733,104 @@ extern "C" int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, 
   tc_reduce_kernel<<<dwba_grid_1d((int64_t)n_forms * n_L, 256), 256, 0, st>>>(P.partial, n_forms, P.f_pad,
                                                                             P.n_iblk, n_L, out_dev);
   DWBA_CHECK_LAUNCH();
+  return DWBA_OK;
+}
+
+// ---- backward ------------------------------------------------------------------------
+namespace {
+int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
+}  // namespace
+
+extern "C" int64_t dwba_tc_backward_workspace_bytes(int n_forms, int n_grid, int L_max, int n_terms) {
+  if (n_forms < 0 || n_grid < 2 || L_max < 0 || L_max > DWBA_MAX_L || (n_terms != 2 && n_terms != 3)) return -1;
+  const int bn = n_terms == 2 ? TC_BN2 : TC_BN3;
+  const int64_t n_pad = ((int64_t)n_grid + BK - 1) / BK * BK;
+  const int64_t f_pad = ((int64_t)n_forms + bn - 1) / bn * bn;
+  const int64_t n_iblk = ((int64_t)n_grid + BM - 1) / BM;
+  const int64_t nL = L_max + 1;
+  return align256((int64_t)n_terms * f_pad * n_pad * 2) + align256(nL * f_pad * n_pad * 8) + align256(f_pad * 4) +
+         align256(n_pad * 8) + align256(2 * nL * n_pad * 4) + align256(nL * n_iblk * (n_pad / BK) * 4) +
+         2 * align256((int64_t)n_forms * (int64_t)sizeof(dwba_form_t));
+}
+
+extern "C" int dwba_bilinear_tc_bf16_backward(const dwba_form_grad_t* forms_dev, int n_forms, const double* r_dev,
+                                              int n_grid, int L_max, int n_terms, const double* diag_scale_host,
+                                              const double* grad_dev, void* workspace, int64_t workspace_bytes,
+                                              int* status_dev, dwba_stream_t stream) {
+  if (n_forms <= 0) return DWBA_OK;
+  if (!forms_dev || !r_dev || !diag_scale_host || !grad_dev || !workspace || !status_dev || n_grid < 2 ||
+      L_max < 0 || L_max > DWBA_MAX_L || (n_terms != 2 && n_terms != 3) || n_grid > (1 << 24))
+    return DWBA_ERR_INVALID_ARG;
+  const int64_t need = dwba_tc_backward_workspace_bytes(n_forms, n_grid, L_max, n_terms);
+  if (need < 0 || workspace_bytes < need) return DWBA_ERR_WORKSPACE;
+  if (((uintptr_t)workspace & 255) != 0) return DWBA_ERR_INVALID_ARG;
+  const int bn = n_terms == 2 ? TC_BN2 : TC_BN3;
+  const int n_L = L_max + 1;
+  GemmParams P;
+  P.n_grid = n_grid;
+  P.n_pad = (n_grid + BK - 1) / BK * BK;
+  P.f_pad = (n_forms + bn - 1) / bn * bn;
+  P.n_iblk = (n_grid + BM - 1) / BM;
+  P.L_max = L_max;
+  P.r = r_dev;
+  P.n_forms = n_forms;
+  P.status = status_dev;
+  P.gw = grad_dev;
+  P.n_Ltot = n_L;
+  P.partial = nullptr;
+  for (int l = 0; l <= DWBA_MAX_L; ++l) P.diag[l] = l <= L_max ? diag_scale_host[l] : 0.0;
+  if (P.f_pad / bn > 65535) return DWBA_ERR_INVALID_ARG;
+  uint8_t* ws = (uint8_t*)workspace;
+  __nv_bfloat16* bterms = (__nv_bfloat16*)ws;
+  ws += align256((int64_t)n_terms * P.f_pad * P.n_pad * 2);
+  P.gpart = (double*)ws;
+  ws += align256((int64_t)n_L * P.f_pad * P.n_pad * 8);
+  int* bexp = (int*)ws;
+  P.bexp = bexp;
+  ws += align256((int64_t)P.f_pad * 4);
+  double* lg = (double*)ws;
+  P.lg = lg;
+  ws += align256((int64_t)P.n_pad * 8);
+  P.n_kb = P.n_pad / BK;
+  float* vt = (float*)ws;
+  ws += align256(2LL * n_L * P.n_pad * 4);
+  float* stab = (float*)ws;
+  ws += align256((int64_t)n_L * P.n_iblk * P.n_kb * 4);
+  dwba_form_t* for_a = (dwba_form_t*)ws;
+  ws += align256((int64_t)n_forms * (int64_t)sizeof(dwba_form_t));
+  dwba_form_t* for_b = (dwba_form_t*)ws;
+  P.vt = vt;
+  P.st = stab;
+  cudaStream_t st = (cudaStream_t)stream;
+  tc_grad_forms_kernel<<<dwba_grid_1d(n_forms, 256), 256, 0, st>>>(forms_dev, n_forms, for_a, for_b);
+  DWBA_CHECK_LAUNCH();
+  tc_log2_kernel<<<dwba_grid_1d(n_grid, 256), 256, 0, st>>>(r_dev, n_grid, lg);
+  DWBA_CHECK_LAUNCH();
+  {
+    const int64_t n_fac = 2LL * n_L * P.n_pad + (int64_t)n_L * P.n_iblk * P.n_kb;
+    tc_factors_kernel<<<dwba_grid_1d(n_fac, 256, 65535), 256, 0, st>>>(lg, n_grid, P.n_pad, P.n_kb, P.n_iblk, n_L,
+                                                                       vt, stab);
+    DWBA_CHECK_LAUNCH();
+  }
+  const int64_t total = (int64_t)P.f_pad * P.n_pad;
+  for (int which = 0; which < 2; ++which) {
+    const dwba_form_t* fs = which == 0 ? for_a : for_b;
+    P.forms = fs;
+    tc_scale_kernel<<<n_forms, 256, 0, st>>>(fs, n_forms, bexp);
+    DWBA_CHECK_LAUNCH();
+    if (n_terms == 2)
+      tc_prepare_kernel<2><<<dwba_grid_1d(total, 256, 65535), 256, 0, st>>>(fs, n_forms, P.n_pad, P.f_pad, bexp,
+                                                                            bterms);
+    else
+      tc_prepare_kernel<3><<<dwba_grid_1d(total, 256, 65535), 256, 0, st>>>(fs, n_forms, P.n_pad, P.f_pad, bexp,
+                                                                            bterms);
+    DWBA_CHECK_LAUNCH();
+    int rc = n_terms == 2 ? launch_tc<2, TC_BN2, true>(P, bterms, n_L, st)
+                          : launch_tc<3, TC_BN3, true>(P, bterms, n_L, st);
+    if (rc != DWBA_OK) return rc;
+    tc_grad_reduce_kernel<<<dwba_grid_1d((int64_t)n_forms * P.n_pad, 256, 65535), 256, 0, st>>>(
+        P.gpart, forms_dev, n_forms, P.f_pad, P.n_pad, n_L, which);
+    DWBA_CHECK_LAUNCH();
+  }
   return DWBA_OK;
 }

@@ -227,6 +227,18 @@ int dwba_bilinear_semisep_backward_fp64(const dwba_form_grad_t* forms_dev, int n
                                         const double* diag_scale_host, const double* grad_dev, double r_min_all,
                                         double r_max_all, dwba_stream_t stream);
 
+/* The same gradients through the split-BF16 tensor-core form (no reference counterpart):
+ * ga_f = sum_L g_L (K_L b_f), gb_f = sum_L g_L (K_L a_f), each K_L B product on tcgen05 with
+ * K_L and the operand split into n_terms bf16 terms and FP32 accumulation (as
+ * dwba_bilinear_tc_bf16), the g_L weighting and the sum over L in FP64. All forms share r_dev
+ * (n_grid points). workspace: dwba_tc_backward_workspace_bytes(...) bytes, 256-byte aligned.
+ * status_dev: one int, zero on entry; set to 2 if a bounded wait expired (the gradients are then
+ * invalid). */
+int64_t dwba_tc_backward_workspace_bytes(int n_forms, int n_grid, int L_max, int n_terms);
+int dwba_bilinear_tc_bf16_backward(const dwba_form_grad_t* forms_dev, int n_forms, const double* r_dev, int n_grid,
+                                   int L_max, int n_terms, const double* diag_scale_host, const double* grad_dev,
+                                   void* workspace, int64_t workspace_bytes, int* status_dev, dwba_stream_t stream);
+
 /* Adjoint of dwba_fold: z = Op^T y for the banded operator of a fold (same op layout), i.e.
  * dLoss/d(f .* g) for y = dLoss/d(out). z gets n_src values. No reference counterpart. */
 typedef struct {

@@ -37,7 +37,7 @@ __device__ __forceinline__ double ipow(double x, int e) {
 //   I_L = sum_s [LOC_s + A0_s SY_s + B0_s SX_s] + sum_p X_p Y_p d_L / r_p.
 // The prefixes over segments come from warp shuffles and a per-warp table in shared memory.
 template <int NL>
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(THREADS, 4)
 semisep_kernel(const dwba_form_t* __restrict__ forms, int L0, int n_ltot, DiagScale ds, double* __restrict__ out) {
   constexpr int NW = THREADS / 32;
   __shared__ double wtot[2 * NL][NW];
@@ -53,10 +53,18 @@ semisep_kernel(const dwba_form_t* __restrict__ forms, int L0, int n_ltot, DiagSc
 #pragma unroll
   for (int l = 0; l < NL; ++l) A[l] = B[l] = SX[l] = SY[l] = LOC[l] = 0.0;
   double dsum = 0.0;
+  // the operands of point p+1 are loaded while point p is accumulated (one point of lead hides
+  // the load latency of the thread's strided walk; 128 registers keep four CTAs per SM)
+  auto ldx = [&](int p) { return p < F.n_rows ? __ldg(F.a_dev + p) : 0.0; };
+  auto ldy = [&](int p) { return p < F.n_cols ? __ldg(F.b_dev + p) : 0.0; };
+  double Xn = p0 < p1 ? ldx(p0) : 0.0, Yn = p0 < p1 ? ldy(p0) : 0.0, rn = p0 < p1 ? __ldg(F.r_dev + p0) : 1.0;
   for (int p = p0; p < p1; ++p) {
-    const double X = p < F.n_rows ? F.a_dev[p] : 0.0;
-    const double Y = p < F.n_cols ? F.b_dev[p] : 0.0;
-    const double r = F.r_dev[p];
+    const double X = Xn, Y = Yn, r = rn;
+    if (p + 1 < p1) {
+      Xn = ldx(p + 1);
+      Yn = ldy(p + 1);
+      rn = __ldg(F.r_dev + p + 1);
+    }
     const double inv = 1.0 / r;
     double pw = L0 > 0 ? ipow(r, L0) : 1.0;
     double ip = L0 > 0 ? ipow(inv, L0 + 1) : inv;

@@ -707,7 +707,10 @@ class PreparedJob:
             mB["n_f"], mB["half_band"] = cnt, 2
             mB["n_out"], mB["n_src"], mB["n_clear"] = nb_a[first], N, nb_a[first]
             forms["a"][fo_a] = adir_a[first][gid]
-            multi = np.concatenate([mT, mB])
+            # T and B multi-folds of one pair launched next to each other, so that the continuum
+            # wave both read (chi_f) is still in L2 for the second
+            multi = np.empty(2 * G, dtype=_lib.FOLD_MULTI_DTYPE)
+            multi[0::2], multi[1::2] = mT, mB
         self.multi_host = multi
         self.n_multi = len(multi)
         self.multi_d = _dev(multi.view(np.uint8), dev) if len(multi) else None

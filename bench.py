@@ -713,7 +713,7 @@ def main():
     # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu capture of
     # the default workload (profiles/launches_semisep_synthetic_batch_N15000.md); other sizes: null
     default_size = args.n_cont == N_CONT
-    traffic = {"nodeset_rows_kernel": 1.945e9, "fold_kernel": 4.894e9, "semisep_kernel": 3.223e9}
+    traffic = {"nodeset_rows_kernel": 1.929e9, "fold_kernel": 4.654e9, "semisep_kernel": 3.214e9}
 
     def hbm_roof(kernel, nbytes, t_ms, note):
         ach = nbytes / (t_ms * 1e-3) / 1e9

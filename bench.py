@@ -515,7 +515,7 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- reference / CPU baseline
-def cpu_sample(seconds_hint=20.0, N=N_GRID):
+def cpu_sample(seconds_hint=20.0, N=N_GRID, block=64):
     """Bounded sample of the reference algorithm (oracle port) on this workload.
 
     The reference's CPU path (dwba_matrix_elements.py:1057-1116 with oscillatory_integrals.py:2555-2777)
@@ -540,7 +540,6 @@ def cpu_sample(seconds_hint=20.0, N=N_GRID):
     iL = iR - 1
     wR = (X - r[iL]) / (r[iR] - r[iL] + 1e-30)
     wL = 1.0 - wR
-    block = 64
     rows = 0
     t0 = time.perf_counter()
     i0 = 0
@@ -569,10 +568,12 @@ def run_reference(args):
         return 0
     cores = os.cpu_count()
     vals = []
+    # about a minute of CPU work in total, whatever the step count (short steps use 16-row blocks)
     for _ in range(args.warmup):
-        cpu_sample(seconds_hint=2.0)
+        cpu_sample(seconds_hint=0.5, block=16)
     for _ in range(args.steps):
-        ips, dt, rows = cpu_sample(seconds_hint=max(2.0, min(20.0, 120.0 / max(1, args.steps))))
+        hint = max(0.2, min(20.0, 60.0 / max(1, args.steps)))
+        ips, dt, rows = cpu_sample(seconds_hint=hint, block=16 if hint < 2.0 else 64)
         vals.append(ips)
     v = float(np.median(vals))
     line = {"metric": METRIC, "value": v, "unit": "integrals/s", "impl": "reference", "n_gpus": args.gpus,

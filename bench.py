@@ -464,6 +464,59 @@ def gradient_run(reps=3):
                     "tests/test_gpu_autograd.py"}
 
 
+# ----------------------------------------------------------------------------- drop-in calls
+def dropin_run():
+    """H 1s->2p at 50 eV (N = 3000, 128 (l_i, l_f) pairs, L = 0..4; the reference's own solver outputs
+    stored in tests/golden/config1.npz): the reference driver's loop of one radial_ME_all_L_gpu call per
+    pair, timed per call, and the same pairs in one radial_ME_all_L_batch call."""
+    import torch
+    from dataclasses import dataclass
+    from dwba_b200.dwba_matrix_elements import radial_ME_all_L_batch, radial_ME_all_L_gpu, GPUCache
+
+    @dataclass(frozen=True)
+    class Wave:
+        l: int
+        k_au: float
+        chi_of_r: np.ndarray
+        phase_shift: float
+        idx_match: int = -1
+        eta: float = 0.0
+        sigma_l: float = 0.0
+    z = np.load(os.path.join(ROOT, "tests", "golden", "config1.npz"))
+    meta = json.loads(bytes(z["meta_json"]).decode())
+    g = _Grid(z["r"], z["dr"], z["w_trapz"], z["w_simpson"])
+    bi, bf = _Bound(0, z["u_i"]), _Bound(1, z["u_f"])
+
+    def wave(m, chi):
+        l, k, d, im, eta, sig = m
+        return Wave(int(l), float(k), chi, float(d), int(im), float(eta), float(sig))
+    wi = {int(l): wave(v, z["chi_i"][int(l)]) for l, v in meta["waves_i"].items()}
+    wf = {int(l): wave(v, z["chi_f"][int(l)]) for l, v in meta["waves_f"].items()}
+    pairs = [(wi[a], wf[b]) for a, b in meta["pairs"]]
+    L = meta["L_max"]
+    cache = GPUCache.from_grid(g)
+
+    def loop():
+        return [radial_ME_all_L_gpu(g, z["V_core"], z["U_i"], bi, bf, ci, cf, L, U_f_array=z["U_f"], gpu_cache=cache)
+                for ci, cf in pairs]
+
+    def batch():
+        return radial_ME_all_L_batch(g, z["V_core"], z["U_i"], bi, bf, pairs, L, U_f_array=z["U_f"], gpu_cache=cache)
+    loop(), batch()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loop()
+    t1 = time.perf_counter()
+    for _ in range(3):
+        batch()
+    t2 = time.perf_counter()
+    return {"workload": "H 1s->2p 50 eV, N=3000, 128 pairs, L=0..4 (the reference's solver outputs)",
+            "per_pair_call_ms": (t1 - t0) * 1e3 / len(pairs), "all_pairs_loop_ms": (t1 - t0) * 1e3,
+            "batch_call_ms": (t2 - t1) * 1e3 / 3, "integrals": len(pairs) * 2 * (L + 1),
+            "note": "wall time from host NumPy inputs to result dicts (the node sets of the grid cached "
+                    "across calls, as GPUCache does for the reference's driver)"}
+
+
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
@@ -828,9 +881,10 @@ def main():
                 "note": "TCS of every (energy, transition) point from each engine's integrals against the exact "
                         "FP64 semiseparable engine's (which agrees with the oracle to 1e-12 per integral)"}
 
-    grad = None
+    grad = dropin = None
     if rank == 0 and world == 1 and not args.no_ragged and args.engine in ("semisep", "dense"):
         grad = gradient_run()
+        dropin = dropin_run()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -853,7 +907,7 @@ def main():
                 "config": {"workload": WORKLOAD, "engine": args.engine, "integrals_per_step_per_gpu": n_int,
                            "l2": "inputs larger than L2 (operands ~1 GB/step)", "parallelism": f"dp{world}"},
                 "split_ms": split, "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu,
-                "engines": compare, "ragged_sweep": ragged, "gradient": grad,
+                "engines": compare, "ragged_sweep": ragged, "gradient": grad, "dropin": dropin,
                 "gpu_launches": n_launch * args.steps, "results_finite": bool(finite and nonzero), "clocks": clk.summary()}
         print(json.dumps(line))
     if world > 1:

@@ -71,14 +71,17 @@ __global__ void fold_multi_kernel(const dwba_fold_multi_t* __restrict__ folds) {
   }
 }
 
+#ifndef DWBA_FOLD_THREADS
+#define DWBA_FOLD_THREADS 128
+#endif
 #ifndef DWBA_FOLD_FILL
-#define DWBA_FOLD_FILL 128 // CTAs per SM the launch aims for
+#define DWBA_FOLD_FILL 512 // CTAs per SM the launch aims for
 #endif
 // Row blocks per fold: enough CTAs in total to fill the GPU (DWBA_FOLD_FILL per SM),
 // never more than the longest fold needs. The kernels stride over the rows of their fold, so a
 // batch of folds of very different lengths launches no CTAs that find no rows.
 int fold_grid_x(int max_rows, int n_folds) {
-  const int need = (max_rows + 255) / 256;
+  const int need = (max_rows + DWBA_FOLD_THREADS - 1) / DWBA_FOLD_THREADS;
   const int fill = (int)(((int64_t)148 * DWBA_FOLD_FILL + n_folds - 1) / n_folds);
   return need < fill ? (need > 0 ? need : 1) : (fill > 0 ? fill : 1);
 }
@@ -89,7 +92,7 @@ extern "C" int dwba_fold_multi(const dwba_fold_multi_t* folds_dev, int n_folds, 
   if (n_folds <= 0) return DWBA_OK;
   if (!folds_dev || max_rows < 0 || n_folds > 65535) return DWBA_ERR_INVALID_ARG;
   dim3 grid(fold_grid_x(max_rows, n_folds), n_folds);
-  fold_multi_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(folds_dev);
+  fold_multi_kernel<<<grid, DWBA_FOLD_THREADS, 0, (cudaStream_t)stream>>>(folds_dev);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;
 }
@@ -98,7 +101,7 @@ extern "C" int dwba_fold(const dwba_fold_t* folds_dev, int n_folds, int max_rows
   if (n_folds <= 0) return DWBA_OK;
   if (!folds_dev || max_rows < 0 || n_folds > 65535) return DWBA_ERR_INVALID_ARG;
   dim3 grid(fold_grid_x(max_rows, n_folds), n_folds);
-  fold_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(folds_dev);
+  fold_kernel<<<grid, DWBA_FOLD_THREADS, 0, (cudaStream_t)stream>>>(folds_dev);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;
 }

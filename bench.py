@@ -780,7 +780,8 @@ def main():
                  "node set; the kernel is issue/latency bound (per-row loops over the CC nodes, FP64 log "
                  "per node visit)"),
         hbm_roof("fold_kernel", sum(p.fold_bytes() for p in preps), split["folds_ms"],
-                 "algorithmic bytes = 8*((2h+1)*n_out + 2*n_src + n_clear) per fold"),
+                 "algorithmic bytes = every distinct operand array (band operators, continuum waves, bound "
+                 "states) read once over its longest use + every output written"),
     ]
     if tc:
         t_ms = split["forms_exchange_tensor_ms"]

@@ -851,17 +851,31 @@ class PreparedJob:
         return float(np.sum(2.0 * f["n_rows"].astype(np.float64) * f["n_cols"])) * self.nl
 
     def fold_bytes(self) -> float:
-        """Bytes the folds must move: (2h+1) operator taps per output row, the factors over n_src,
-        the outputs over n_clear (a multi-fold reads its operator and shared factor once)."""
+        """Bytes the fold launches must move at least once: every distinct operand array (band
+        operator, density factors) read over its longest use, and every output written. Arrays
+        several folds share (a bound state, one pair's operator) count once."""
+        reads: Dict[int, float] = {}
+        writes = 0.0
+
+        def rd(ptrs, lengths):
+            for p_, n_ in zip(np.asarray(ptrs).ravel().tolist(), np.asarray(lengths, dtype=np.float64).ravel().tolist()):
+                if p_ and n_ > reads.get(p_, 0.0):
+                    reads[p_] = n_
         f = self.folds_host
-        taps = (2.0 * f["half_band"].astype(np.float64) + 1.0) * f["n_out"]
-        b = float(np.sum(8.0 * (taps + 2.0 * f["n_src"] + f["n_clear"])))
+        if len(f):
+            rd(f["op"], (2.0 * f["half_band"] + 1.0) * f["n_out"])
+            rd(f["f"], f["n_src"])
+            rd(f["g"], f["n_src"])
+            writes += float(np.sum(f["n_clear"].astype(np.float64)))
         m = self.multi_host
         if len(m):
-            taps = (2.0 * m["half_band"].astype(np.float64) + 1.0) * m["n_out"]
-            nf = m["n_f"].astype(np.float64)
-            b += float(np.sum(8.0 * (taps + (1.0 + nf) * m["n_src"] + nf * m["n_clear"])))
-        return b
+            rd(m["op"], (2.0 * m["half_band"] + 1.0) * m["n_out"])
+            rd(m["g"], m["n_src"])
+            for t in range(_lib.FOLD_MULTI):
+                use = m["n_f"] > t
+                rd(m["f"][use, t], m["n_src"][use])
+                writes += float(np.sum(m["n_clear"][use].astype(np.float64)))
+        return 8.0 * (sum(reads.values()) + writes)
 
     def algorithmic_bytes(self) -> float:
         """Operand bytes of the semiseparable evaluation: a, b and r read once per form."""

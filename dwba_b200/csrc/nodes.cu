@@ -69,6 +69,23 @@ __device__ __forceinline__ int interval_floor(const SetView& s, double x) {
   return m;
 }
 
+// log(1 + u) for 0 <= u <= 1/64 by its Taylor series (12 terms: truncation below 1e-24 relative)
+__device__ __forceinline__ double log1p_small(double u) {
+  double p = -1.0 / 12.0;
+  p = fma(p, u, 1.0 / 11.0);
+  p = fma(p, u, -1.0 / 10.0);
+  p = fma(p, u, 1.0 / 9.0);
+  p = fma(p, u, -1.0 / 8.0);
+  p = fma(p, u, 1.0 / 7.0);
+  p = fma(p, u, -1.0 / 6.0);
+  p = fma(p, u, 1.0 / 5.0);
+  p = fma(p, u, -1.0 / 4.0);
+  p = fma(p, u, 1.0 / 3.0);
+  p = fma(p, u, -0.5);
+  p = fma(p, u, 1.0);
+  return p * u;
+}
+
 // reciprocal width of interpolation interval j (log r or r), zero past the grid
 __device__ __forceinline__ double recip_width(const SetView& s, int j, bool lg) {
   if (j < 0 || j + 1 > s.n_grid - 1) return 0.0;
@@ -131,7 +148,7 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
       const double rg = r[g], rg1 = r[g + 1];
       const double lo = g == 0 ? -1.0e308 : rg;  // exclusive lower end of the owned interval
       bool first = true;
-      double iT0 = 0.0, iT1 = 0.0, iB0 = 0.0, iB1 = 0.0, iW = 0.0, lg = 0.0, lg1 = 0.0;
+      double iT0 = 0.0, iT1 = 0.0, iB0 = 0.0, iB1 = 0.0, iW = 0.0, lg = 0.0, lg1 = 0.0, irg = 0.0;
       for (int m = interval_floor(s, rg); m < s.n_int; ++m) {
         double a, b;
         interval(s, m, a, b);
@@ -152,11 +169,20 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
             iW = 1.0 / (rg1 - rg + 1e-30);
             lg = s.lr[g];
             lg1 = s.lr[g + 1];
+            irg = 1.0 / rg;
             first = false;
           }
           const double w = rn_mul(ccw[sl], hw);
-          const double lx = (s.log1 || s.log2) ? log(x) : 0.0;
           const bool at_top = x >= rg1;  // floor index in the full grid: g + 1 at r_{g+1}, else g
+          // log x - log r_g: from the series of log(1 + (x - r_g)/r_g) when the grid step is small
+          // (it then equals the difference of the two logs to a few ulps of that difference), else
+          // as the difference; log x - log r_{g+1} only for a node exactly at r_{g+1}
+          double dl = 0.0, dl_up = 0.0;
+          if (s.log1 || s.log2) {
+            const double u = (x - rg) * irg;
+            dl = u <= 0.015625 ? log1p_small(u) : log(x) - lg;
+            if (at_top) dl_up = log(x) - lg1;
+          }
           // --- T: rows j1 and j1 + 1, j1 in {g, g+1}
           int j1;
           double t1;
@@ -167,7 +193,7 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
               j1 = (at_top && g + 1 <= n1 - 2) ? g + 1 : g;
               const bool up = j1 != g;
               const double inv = up ? iT1 : iT0;
-              t1 = s.log1 ? (lx - (up ? lg1 : lg)) * inv : (x - (up ? rg1 : rg)) * inv;
+              t1 = s.log1 ? (up ? dl_up : dl) * inv : (x - (up ? rg1 : rg)) * inv;
             }
             const double v_di0 = w * (1.0 - t1) * (1.0 - t1), v_up0 = w * (1.0 - t1) * t1;
             const double v_di1 = w * t1 * t1, v_lo1 = w * t1 * (1.0 - t1);
@@ -192,7 +218,7 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
               j2 = (at_top && g + 1 <= N - 2) ? g + 1 : g;
               const bool up = j2 != g;
               const double inv = up ? iB1 : iB0;
-              t2 = s.log2 ? (lx - (up ? lg1 : lg)) * inv : (x - (up ? rg1 : rg)) * inv;
+              t2 = s.log2 ? (up ? dl_up : dl) * inv : (x - (up ? rg1 : rg)) * inv;
             }
             const double wr = (x - rg) * iW;
             const double q0 = 1.0 - wr, q1 = wr;

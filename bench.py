@@ -496,23 +496,27 @@ def dropin_run():
     L = meta["L_max"]
     cache = GPUCache.from_grid(g)
 
-    def loop():
-        return [radial_ME_all_L_gpu(g, z["V_core"], z["U_i"], bi, bf, ci, cf, L, U_f_array=z["U_f"], gpu_cache=cache)
-                for ci, cf in pairs]
+    def loop(engine):
+        return [radial_ME_all_L_gpu(g, z["V_core"], z["U_i"], bi, bf, ci, cf, L, U_f_array=z["U_f"], gpu_cache=cache,
+                                    engine=engine) for ci, cf in pairs]
 
-    def batch():
-        return radial_ME_all_L_batch(g, z["V_core"], z["U_i"], bi, bf, pairs, L, U_f_array=z["U_f"], gpu_cache=cache)
-    loop(), batch()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    loop()
-    t1 = time.perf_counter()
-    for _ in range(3):
-        batch()
-    t2 = time.perf_counter()
+    def batch(engine):
+        return radial_ME_all_L_batch(g, z["V_core"], z["U_i"], bi, bf, pairs, L, U_f_array=z["U_f"], gpu_cache=cache,
+                                     engine=engine)
+    out = {}
+    for engine in ("dense", "semisep"):
+        loop(engine), batch(engine)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loop(engine)
+        t1 = time.perf_counter()
+        for _ in range(3):
+            batch(engine)
+        t2 = time.perf_counter()
+        out[engine] = {"per_pair_call_ms": (t1 - t0) * 1e3 / len(pairs), "all_pairs_loop_ms": (t1 - t0) * 1e3,
+                       "batch_call_ms": (t2 - t1) * 1e3 / 3}
     return {"workload": "H 1s->2p 50 eV, N=3000, 128 pairs, L=0..4 (the reference's solver outputs)",
-            "per_pair_call_ms": (t1 - t0) * 1e3 / len(pairs), "all_pairs_loop_ms": (t1 - t0) * 1e3,
-            "batch_call_ms": (t2 - t1) * 1e3 / 3, "integrals": len(pairs) * 2 * (L + 1),
+            **out, "integrals": len(pairs) * 2 * (L + 1),
             "note": "wall time from host NumPy inputs to result dicts (the node sets of the grid cached "
                     "across calls, as GPUCache does for the reference's driver)"}
 

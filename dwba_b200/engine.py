@@ -34,12 +34,6 @@ def _stream() -> int:
     return int(torch.cuda.current_stream().cuda_stream)
 
 
-def _require_device():
-    if not torch.cuda.is_available():
-        raise RuntimeError("dwba_b200: no CUDA device is available (the engine has no CPU fallback)")
-    _lib.load()
-
-
 def _dev(x: np.ndarray, device) -> torch.Tensor:
     return torch.from_numpy(np.ascontiguousarray(x)).to(device, non_blocking=False)
 
@@ -898,13 +892,6 @@ class PreparedJob:
         I_exc = res[1:nf:2].reshape(T, P, nl).copy()
         self.add_host_terms(I_dir, I_exc, res[nf:])
         return I_dir, I_exc
-
-
-def run_job(job: Job, dg: DeviceGrid, engine: str = "dense"):
-    """Evaluate every (transition, pair) of a job: (I_dir, I_exc) of shape (T, P, L_max+1)."""
-    pj = PreparedJob(job, dg, engine)
-    pj.launch()
-    return pj.collect()
 
 
 class MultiPrepared:

@@ -832,9 +832,27 @@ def main():
         uniq_waves = len({id(w) for pr in pairs for w in pr})
         h2d = (uniq_waves + 2 * len(bounds)) * N_GRID * 8
         d2h = len(bounds) * len(pairs) * 2 * (L_MAX + 1) * 8
+        # the same call returning the two result arrays instead of a result object per pair
+        def e2e_arrays():
+            cache.clear()
+            return radial_ME_all_L_batch(g, zeros, zeros, b_i, b_f, pairs, L_MAX, U_f_array=zeros,
+                                         gpu_cache=cache, engine=args.engine, as_arrays=True)
+        e2e_arrays()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            e2e_arrays()
+        barrier()
+        a_ms = (time.perf_counter() - t0) * 1e3 / e_steps
+        if world > 1:
+            tt = torch.tensor([a_ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            a_ms = float(tt.item())
         e2e = {"value": world * n_int / (e_ms * 1e-3), "unit": "integrals/s", "ms_per_step": e_ms,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "path": "radial_ME_all_L_batch (4 transitions x 2048 pairs) from pinned host NumPy inputs"}
+               "path": "radial_ME_all_L_batch (4 transitions x 2048 pairs) from pinned host NumPy inputs to one "
+                       "RadialDWBAIntegrals per (transition, pair)",
+               "as_arrays_ms_per_step": a_ms, "as_arrays_value": world * n_int / (a_ms * 1e-3)}
 
     # the same batch through the split-BF16 tensor-core form and the plain FP64 kernel (whole step,
     # node sets rebuilt), so the line carries the split-BF16 vs FP64 comparison of the metric

@@ -230,8 +230,10 @@ def _results(I_dir: np.ndarray, I_exc: np.ndarray):
 
 
 @_no_gc
-def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, gpu_cache, engine):
-    """Evaluate a job; returns results[t][p] (a list of RadialDWBAIntegrals per transition)."""
+def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, gpu_cache, engine,
+         as_arrays: bool = False):
+    """Evaluate a job; returns results[t][p] (a list of RadialDWBAIntegrals per transition), or
+    the (T, P, L_max+1) arrays (I_dir, I_exc) with ``as_arrays``."""
     if not HAS_CUPY:
         raise RuntimeError("dwba_b200 engine library is not available (build it with python -m dwba_b200.build)")
     import torch
@@ -255,6 +257,8 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
             pj = PreparedJob(job, cache.dg, eng, plans=plans)
             pj.launch()
             I_dir, I_exc = pj.collect()
+    if as_arrays:
+        return I_dir, I_exc
     return _results(I_dir, I_exc)
 
 
@@ -293,19 +297,28 @@ def radial_ME_all_L_batch(grid, V_core_array, U_i_array, bound_i, bound_f,
                           CC_nodes: int = 5, phase_increment: float = 1.5708, min_grid_fraction: float = 0.10,
                           k_threshold: float = 0.5, U_f_array: Optional[np.ndarray] = None,
                           gpu_cache: Optional[GPUCache] = None,
-                          engine: Optional[str] = None) -> List[RadialDWBAIntegrals]:
+                          engine: Optional[str] = None, as_arrays: bool = False):
     """Batched entry point (new): the same values as calling ``radial_ME_all_L`` per pair.
 
     All pairs share one grid and the potentials. With single ``bound_i``/``bound_f`` objects the
     result is one ``RadialDWBAIntegrals`` per pair; with equal-length sequences of them (several
-    transitions, e.g. one per ejected wave in ionization) it is a list per transition."""
+    transitions, e.g. one per ejected wave in ionization) it is a list per transition. With
+    ``as_arrays=True`` the same values come as two float64 arrays (I_direct, I_exchange) of shape
+    (P, L_max+1), or (T, P, L_max+1) for several transitions, without building a result object
+    per pair."""
     kw = dict(use_oscillatory_quadrature=use_oscillatory_quadrature, oscillatory_method=oscillatory_method,
               CC_nodes=CC_nodes, phase_increment=phase_increment, min_grid_fraction=min_grid_fraction,
               k_threshold=k_threshold)
     multi = isinstance(bound_i, (list, tuple))
     if len(pairs) == 0:
+        if as_arrays:
+            shape = ((len(bound_i),) if multi else ()) + (0, L_max + 1)
+            return np.zeros(shape), np.zeros(shape)
         return [[] for _ in bound_i] if multi else []
-    res = _run(grid, V_core_array, U_i_array, bound_i, bound_f, list(pairs), L_max, U_f_array, kw, gpu_cache, engine)
+    res = _run(grid, V_core_array, U_i_array, bound_i, bound_f, list(pairs), L_max, U_f_array, kw, gpu_cache, engine,
+               as_arrays=as_arrays)
+    if as_arrays:
+        return res if multi else (res[0][0], res[1][0])
     return res if multi else res[0]
 
 

@@ -59,6 +59,14 @@ def test_gpu_signature_with_cache_and_batch_agree():
         assert s.I_L_direct == b.I_L_direct and s.I_L_exchange == b.I_L_exchange  # same kernels, same order
         cpu_sig = radial_ME_all_L(*c["args"], **c["kwargs"])
         assert cpu_sig.I_L_direct == s.I_L_direct
+    # the same batch as two arrays (no result object per pair)
+    d, e = radial_ME_all_L_batch(a[0], a[1], a[2], a[3], a[4], pairs, advanced[0]["L_max"],
+                                 U_f_array=advanced[0]["kwargs"]["U_f_array"], gpu_cache=cache, as_arrays=True)
+    L = advanced[0]["L_max"]
+    assert d.shape == e.shape == (len(pairs), L + 1)
+    for p, b in enumerate(batch):
+        assert list(d[p]) == [b.I_L_direct[l] for l in range(L + 1)]
+        assert list(e[p]) == [b.I_L_exchange[l] for l in range(L + 1)]
     cache.clear()
 
 

@@ -69,8 +69,18 @@ __device__ __forceinline__ int interval_floor(const SetView& s, double x) {
   return m;
 }
 
-// log(1 + u) for 0 <= u <= 1/64 by its Taylor series (12 terms: truncation below 1e-24 relative)
+// log(1 + u) for 0 <= u <= 1/64 by its Taylor series: 6 terms for u <= 2^-9, else 12 (the
+// truncation stays below 1e-17 relative either way)
 __device__ __forceinline__ double log1p_small(double u) {
+  if (u <= 0.001953125) {
+    double q = -1.0 / 6.0;
+    q = fma(q, u, 1.0 / 5.0);
+    q = fma(q, u, -1.0 / 4.0);
+    q = fma(q, u, 1.0 / 3.0);
+    q = fma(q, u, -0.5);
+    q = fma(q, u, 1.0);
+    return q * u;
+  }
   double p = -1.0 / 12.0;
   p = fma(p, u, 1.0 / 11.0);
   p = fma(p, u, -1.0 / 10.0);

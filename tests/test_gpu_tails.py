@@ -159,3 +159,32 @@ def test_dropin_device_tails_equal_host_tails(monkeypatch):
         db = np.array([b.I_L_direct[l] for l in range(L + 1)])
         assert np.all(np.abs(da - db) <= 1e-13 * np.abs(db) + 1e-18), (call["label"], da, db)
         assert all(a.I_L_exchange[l] == b.I_L_exchange[l] for l in range(L + 1))
+
+
+def test_many_multipoles_in_several_chunks():
+    """L_max = 19: the device kernel takes the multipoles in chunks of eight (1..8, 9..16, 17..19);
+    every entry of every chunk equals the host path (Levin records to round-off times the condition
+    number of their collocation systems, as in test_random_records_match_host), and zero moments
+    give zero tails."""
+    rng = np.random.default_rng(21)
+    n, L_max = 40, 19
+    ki = rng.uniform(0.5, 3.0, n)
+    kf = ki * rng.uniform(0.3, 0.9, n)
+    eta = np.where(rng.random(n) < 0.5, 0.0, -rng.uniform(0.1, 1.0, n))
+    waves = np.stack([ki, rng.integers(0, 15, n), rng.uniform(-1, 1, n), eta / ki, rng.uniform(-2, 2, n),
+                      kf, rng.integers(0, 15, n), rng.uniform(-1, 1, n), eta / kf, rng.uniform(-2, 2, n)], axis=1)
+    r_m = rng.uniform(10.0, 40.0, n)
+    r_max = r_m + rng.uniform(20.0, 200.0, n)
+    moms = rng.normal(size=(n, L_max + 1)) * 10.0 ** rng.uniform(-2, 1, (n, 1))
+    moms[::5, 9:17] = 0.0  # a whole chunk of zero moments
+    assert all(_lib.tail_on_device(w, a, b) for w, a, b in zip(waves, r_m, r_max))
+    cond = np.array([_levin_condition(w, a, b) for w, a, b in zip(waves, r_m, r_max)])
+    for mode in (0, 1):
+        got = _device_tails(waves, r_m, r_max, moms, mode, L_max)
+        for k in range(n):
+            host = _lib.outer_tails(waves[k], r_m[k], r_max[k], L_max, moms[k], mode, SEG, DPHI)
+            scale = np.abs(moms[k]) / r_m[k] ** (np.arange(L_max + 1) + 1) * (r_max[k] - r_m[k])
+            rel = 1e-14 + (1e-16 * cond[k] if mode == 0 else 0.0)
+            assert got[k, 0] == 0.0
+            assert np.all(np.abs(got[k] - host) <= 1e-13 * np.abs(host) + rel * scale), (mode, k, cond[k], got[k], host)
+        assert np.all(got[::5, 9:17] == 0.0)

@@ -147,6 +147,25 @@ def test_engine_vs_oracle_larger_grid():
             assert np.all(np.abs(ge - e) <= 1e-12 * np.abs(e) + 3e-14 * se), engine
 
 
+def test_engine_vs_oracle_two_multipole_chunks():
+    """L_max = 12 (the FP64 kernels take multipoles 0..8 and 9..12 in two launches) on N = 2001:
+    dense and semiseparable engines against the oracle's folded operands."""
+    from dwba_b200.dwba_matrix_elements import radial_ME_all_L_batch
+    grid, z, bi, bf, pairs, L_max = _synthetic(2001, 200.0, 3, seed=13, L_max=12)
+    for engine in ("dense", "semisep"):
+        res = radial_ME_all_L_batch(grid, z, z, bi, bf, pairs, L_max, U_f_array=z, engine=engine)
+        for (ci, cf), rr in zip(pairs, res):
+            fp = fold_pair(grid, z, z, bi, bf, ci, cf, L_max, U_f_array=z)
+            d = semiseparable_eval(grid.r, fp["a_dir"], fp["b_dir"], L_max)
+            e = semiseparable_eval(grid.r, fp["a_ex"], fp["b_ex"], L_max)
+            sd = semiseparable_eval(grid.r, np.abs(fp["a_dir"]), np.abs(fp["b_dir"]), L_max)
+            se = semiseparable_eval(grid.r, np.abs(fp["a_ex"]), np.abs(fp["b_ex"]), L_max)
+            gd = np.array([rr.I_L_direct[l] for l in range(L_max + 1)])
+            ge = np.array([rr.I_L_exchange[l] for l in range(L_max + 1)])
+            assert np.all(np.abs(gd - d) <= 1e-12 * np.abs(d) + 3e-14 * sd), engine
+            assert np.all(np.abs(ge - e) <= 1e-12 * np.abs(e) + 3e-14 * se), engine
+
+
 def test_semiseparable_overflow_guard():
     from dwba_b200 import _lib
     from dwba_b200.dwba_matrix_elements import radial_ME_all_L

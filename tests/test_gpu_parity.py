@@ -166,6 +166,21 @@ def test_engine_vs_oracle_two_multipole_chunks():
             assert np.all(np.abs(ge - e) <= 1e-12 * np.abs(e) + 3e-14 * se), engine
 
 
+@pytest.mark.parametrize("engine", ["tc_bf16x3", "tc_bf16x6"])
+def test_tensor_core_engines_many_multipoles(engine):
+    """The split-BF16 forms at L_max = 12 on N = 2001: every integral within 1e-5 of the scale
+    S_L = |a|^T K_L |b| of the oracle's folded operands (FP32-accumulated products)."""
+    from dwba_b200.dwba_matrix_elements import radial_ME_all_L_batch
+    grid, z, bi, bf, pairs, L_max = _synthetic(2001, 200.0, 3, seed=17, L_max=12)
+    res = radial_ME_all_L_batch(grid, z, z, bi, bf, pairs, L_max, U_f_array=z, engine=engine)
+    for (ci, cf), rr in zip(pairs, res):
+        fp = fold_pair(grid, z, z, bi, bf, ci, cf, L_max, U_f_array=z)
+        e = semiseparable_eval(grid.r, fp["a_ex"], fp["b_ex"], L_max)
+        se = semiseparable_eval(grid.r, np.abs(fp["a_ex"]), np.abs(fp["b_ex"]), L_max)
+        ge = np.array([rr.I_L_exchange[l] for l in range(L_max + 1)])
+        assert np.all(np.abs(ge - e) <= 1e-5 * se), (engine, np.max(np.abs(ge - e) / se))
+
+
 def test_semiseparable_overflow_guard():
     from dwba_b200 import _lib
     from dwba_b200.dwba_matrix_elements import radial_ME_all_L

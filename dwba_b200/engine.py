@@ -475,11 +475,23 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
             keys = np.stack([n1[cand].astype(np.float64), k_total[cand], d[cand], eta_total[cand]], axis=1)
             uk, inv = np.unique(keys, axis=0, return_inverse=True)
             pos = np.empty(len(uk), dtype=np.int64)
+            # breakpoint counts of the linspace (eta == 0) sets for all keys at once, with the
+            # arithmetic of plan_nodeset; Coulomb sets go through plan_nodeset one by one
+            u_n1 = uk[:, 0].astype(np.int64)
+            span = r[u_n1 - 1] - r[0]
+            with np.errstate(divide="ignore", invalid="ignore"):
+                n_lin = np.ceil(span / (uk[:, 2] / uk[:, 1])) + 1
+                step = span / (n_lin - 1)
+            lin_ok = (uk[:, 1] >= 1e-10) & (n_lin >= 2) & (step > 1e-12)
             for u, rec in enumerate(uk.tolist()):
                 key = NodeSetKey(id(g), int(rec[0]), rec[1], rec[2], rec[3], int(job.CC_nodes))
                 q = ns_pos.get(key)
                 if q is None:
-                    nsp = plan_nodeset(g, key)
+                    if abs(rec[3]) < 1e-10:
+                        nsp = (NodeSetPlan(key, int(n_lin[u]), None, g.log_prefix(key.n1), g.log_full)
+                               if lin_ok[u] else None)
+                    else:
+                        nsp = plan_nodeset(g, key)
                     q = -1 if nsp is None else len(nodesets)
                     if nsp is not None:
                         nodesets.append(nsp)

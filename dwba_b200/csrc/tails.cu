@@ -227,8 +227,11 @@ __device__ __forceinline__ void filon_segment_all(const double* m, int L0, int n
 
 // Levin collocation on one segment (8 nodes) for every multipole of the chunk: the system matrix
 // does not depend on L, so it is factorised once and solved for each envelope
+// res[q]: the segment's contribution to multipole L0 + q (zero where there is none); a separate
+// result array keeps the caller's accumulators out of local memory
 __device__ __noinline__ void levin_segment_all(const double* m, int L0, int nl, const PhaseD& ph, double a, double b,
-                                  KSum* acc) {
+                                  double* res) {
+  for (int q = 0; q < LC; ++q) res[q] = 0.0;
   const LevinD& lv = s_lv;
   cplx A[8][8];
   double x[8];
@@ -283,7 +286,7 @@ __device__ __noinline__ void levin_segment_all(const double* m, int L0, int nl, 
       for (int j = i + 1; j < 8; ++j) sum = csub(sum, cmul(A[i][j], u[j]));
       u[i] = cdiv(sum, A[i][i]);
     }
-    acc[q].add(csub(cmul(u[7], e7), cmul(u[0], e0)).re);
+    res[q] = csub(cmul(u[7], e7), cmul(u[0], e0)).re;
   }
 }
 
@@ -315,7 +318,11 @@ __device__ __noinline__ void outer_branch_all(const double* m, int L0, int nl, c
     const int nseg = (int)max(1.0, ceil((rmax - rm) / h));
     for (int s = lane; s < nseg; s += 32) {
       const double a = lin(rm, rmax, nseg + 1, s), b = lin(rm, rmax, nseg + 1, s + 1);
-      levin_segment_all(m, L0, nl, ph, a, b, acc);
+      double res[LC];
+      levin_segment_all(m, L0, nl, ph, a, b, res);
+#pragma unroll
+      for (int q = 0; q < LC; ++q)
+        if (q < nl) acc[q].add(res[q]);
     }
   }
 #pragma unroll

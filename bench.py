@@ -154,7 +154,7 @@ def make_ragged_points(n_energy=64, l_max_wave=40, r_max=200.0, seed=3):
     return points
 
 
-def ragged_sweep(engine, L_max=6, replays=5, n_energy=64, points=None):
+def ragged_sweep(engine, L_max=6, replays=5, n_energy=64, points=None, split=True):
     """Device time of the ragged sweep (node sets, folds, forms and tails of all points in shared
     launches, replayed from a CUDA graph). Returns (summary, [(I_dir, I_exc) per point])."""
     import torch
@@ -183,15 +183,18 @@ def ragged_sweep(engine, L_max=6, replays=5, n_energy=64, points=None):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / replays
     # per-stage device time of one more (un-captured) launch sequence, with each stage's bytes
-    marks = []
-    mp.launch(marks)
-    torch.cuda.synchronize()
-    split = {f"{b[0]}_ms": a[1].elapsed_time(b[1]) for a, b in zip(marks[:-1], marks[1:])}
-    stage_bytes = {"nodesets_ms": sum(p.nodesets.algorithmic_bytes() for p in parts if p.nodesets.n),
-                   "folds_ms": sum(p.fold_bytes() for p in parts)}
-    if engine == "semisep":
-        stage_bytes["forms_ms"] = sum(p.algorithmic_bytes() for p in parts)
-    gbs = {k.replace("_ms", "_gbs"): stage_bytes[k] / (split[k] * 1e-3) / 1e9 for k in stage_bytes if split.get(k)}
+    stages, gbs = None, None
+    if split:
+        marks = []
+        mp.launch(marks)
+        torch.cuda.synchronize()
+        stages = {f"{b[0]}_ms": a[1].elapsed_time(b[1]) for a, b in zip(marks[:-1], marks[1:])}
+        stage_bytes = {"nodesets_ms": sum(p.nodesets.algorithmic_bytes() for p in parts if p.nodesets.n),
+                       "folds_ms": sum(p.fold_bytes() for p in parts)}
+        if engine == "semisep":
+            stage_bytes["forms_ms"] = sum(p.algorithmic_bytes() for p in parts)
+        gbs = {k.replace("_ms", "_gbs"): stage_bytes[k] / (stages[k] * 1e-3) / 1e9 for k in stage_bytes
+               if stages.get(k)}
     outs = mp.collect()
     finite = all(np.isfinite(d).all() and np.isfinite(e).all() for d, e in outs)
     n_int = sum(2 * p.T * p.P * p.nl for p in parts)
@@ -207,7 +210,7 @@ def ragged_sweep(engine, L_max=6, replays=5, n_energy=64, points=None):
             "engine": engine, "energies": n_energy, "points": len(points), "N_min": min(Ns), "N_max": max(Ns),
             "integrals": n_int, "ms_per_sweep": ms, "ms_per_energy": ms / n_energy,
             "integrals_per_s": n_int / (ms * 1e-3), "graph": True, "replays": replays,
-            "split_ms": split, "split_algorithmic_gbs": gbs, "tail_records": n_tail,
+            "split_ms": stages, "split_algorithmic_gbs": gbs, "tail_records": n_tail,
             "results_finite": bool(finite)}, outs
 
 
@@ -889,10 +892,10 @@ def main():
         points = make_ragged_points()
         ragged, ref_outs = ragged_sweep("semisep", points=points)
         if not args.no_compare:
-            r_x3, x3_outs = ragged_sweep("tc_bf16x3", replays=3, points=points)
+            r_x3, x3_outs = ragged_sweep("tc_bf16x3", replays=3, points=points, split=False)
             worst, med = sweep_tcs_errors(points, ref_outs, x3_outs)
             del x3_outs
-            r_dense, dense_outs = ragged_sweep("dense", replays=1, points=points)
+            r_dense, dense_outs = ragged_sweep("dense", replays=1, points=points, split=False)
             worst_d, _ = sweep_tcs_errors(points, ref_outs, dense_outs)
             del dense_outs
             ragged["engines"] = {

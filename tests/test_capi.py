@@ -52,3 +52,24 @@ def test_invalid_args_rejected_without_gpu_work():
     pre = np.zeros(3, dtype=np.int64)
     assert lib.dwba_dense_chunk_prefix(m.ctypes.data, 2, pre.ctypes.data) == 4 + 2
     assert list(pre) == [0, 4, 6]
+
+
+def test_tensor_core_backward_host_checks():
+    """The split-BF16 backward's workspace query and argument checks run on the host."""
+    lib = _lib.load()
+    assert lib.dwba_tc_backward_workspace_bytes(10, 1, 4, 2) == -1  # grid too short
+    assert lib.dwba_tc_backward_workspace_bytes(10, 100, 4, 4) == -1  # 2 or 3 terms only
+    # more forms, more grid points or more multipoles never need less workspace
+    base = lib.dwba_tc_backward_workspace_bytes(300, 3001, 6, 2)
+    assert base > 0 and base % 256 == 0
+    assert lib.dwba_tc_backward_workspace_bytes(600, 3001, 6, 2) > base
+    assert lib.dwba_tc_backward_workspace_bytes(300, 6001, 6, 2) > base
+    assert lib.dwba_tc_backward_workspace_bytes(300, 3001, 9, 2) > base
+    assert lib.dwba_tc_backward_workspace_bytes(300, 3001, 6, 3) > base
+    # the gradient partials alone: (L_max+1) x padded forms x padded grid doubles
+    assert base >= 7 * 512 * 3008 * 8
+    ds = np.ones(7)
+    assert lib.dwba_bilinear_tc_bf16_backward(None, 1, None, 3001, 6, 2, ds.ctypes.data, None, None, 0, None,
+                                              None) == _lib.DWBA_ERR_INVALID_ARG
+    assert lib.dwba_bilinear_tc_bf16_backward(None, 0, None, 3001, 6, 2, ds.ctypes.data, None, None, 0, None,
+                                              None) == _lib.DWBA_OK  # nothing to do

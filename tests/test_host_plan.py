@@ -127,3 +127,29 @@ def test_invalid_arguments_raise_value_error():
         _lib.check(_lib.DWBA_ERR_INVALID_ARG, "x")
     with pytest.raises(_lib.DWBAError):
         _lib.check(_lib.DWBA_ERR_CUDA, "x")
+
+
+def test_node_set_plans_equal_single_key_planning():
+    """plan_job's node sets (linspace counts for all keys at once, Coulomb sets one by one) equal
+    plan_nodeset for each key, on the golden calls and on synthetic batch waves."""
+    import bench
+    from dwba_b200.plan import plan_nodeset
+    jobs = []
+    for call in gc.all_calls():
+        grid, V, Ui, bi, bf, ci, cf, L_max = call["args"]
+        kw = dict(call["kwargs"])
+        Uf = kw.pop("U_f_array")
+        jobs.append(dme._make_job(grid, V, Ui, bi, bf, [(ci, cf)], L_max, Uf, kw, _Cache(grid)))
+    g, z, bounds, pairs = bench.make_workload(N=4001, n_cont=64, n_bound=2)
+    jobs.append(dme._make_job(g, z, z, [b[0] for b in bounds], [b[1] for b in bounds], pairs, 4, z, {}, _Cache(g)))
+    n = 0
+    for job in jobs:
+        for ns in plan_job(job).nodesets:
+            ref = plan_nodeset(job.grid, ns.key)
+            assert ref is not None and ref.n_breaks == ns.n_breaks
+            assert (ref.log1, ref.log2) == (ns.log1, ns.log2)
+            assert (ref.breaks is None) == (ns.breaks is None)
+            if ref.breaks is not None:
+                assert np.array_equal(ref.breaks, ns.breaks)
+            n += 1
+    assert n >= 64

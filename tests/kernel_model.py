@@ -31,12 +31,27 @@ def node_arrays(r, n1, n_breaks, breaks, n_cc):
     return x, w
 
 
+def _log1p_small(u):
+    """Taylor series of log(1 + u) as nodes.cu evaluates it (6 terms for u <= 2^-9, else 12)."""
+    p6 = np.zeros_like(u)
+    for k in range(6, 0, -1):
+        p6 = p6 * u + (1.0 if k % 2 else -1.0) / k
+    p12 = np.zeros_like(u)
+    for k in range(12, 0, -1):
+        p12 = p12 * u + (1.0 if k % 2 else -1.0) / k
+    return np.where(u <= 2.0 ** -9, p6, p12) * u
+
+
 def interp_taps(r, n, log_grid, x):
     j = np.clip(np.searchsorted(r[:n], x, side="right") - 1, 0, n - 2)
     lo = x <= r[0]
     hi = x >= r[n - 1]
     if log_grid:
-        t = (np.log(np.maximum(x, r[0])) - np.log(r[j])) / (np.log(r[j + 1]) - np.log(r[j]))
+        # log x - log r_j: the series of log(1 + (x - r_j)/r_j) for steps below 1/64, as the kernel
+        xx = np.maximum(x, r[0])
+        u = (xx - r[j]) / r[j]
+        dl = np.where(u <= 1.0 / 64.0, _log1p_small(np.clip(u, 0.0, 1.0 / 64.0)), np.log(xx) - np.log(r[j]))
+        t = dl / (np.log(r[j + 1]) - np.log(r[j]))
     else:
         t = (x - r[j]) / (r[j + 1] - r[j])
     j = np.where(hi, n - 2, np.where(lo, 0, j))

@@ -111,19 +111,23 @@ def make_workload(N=N_GRID, n_cont=N_CONT, n_bound=N_BOUND, seed_shift=0, pinned
     return g, zeros, bounds, pairs
 
 
-def make_ragged_points(n_energy=64, l_max_wave=40, r_max=200.0, seed=3):
+def make_ragged_points(n_energy=64, l_max_wave=40, r_max=200.0, seed=3, select=None):
     """Ragged multi-energy sweep with the shapes of the He+ 1s->2s / 1s->2p study: energies
     geomspace(45, 1000, n_energy) eV, one grid per energy with N_e = round(2000 * 7.5^(e/(n-1))) points,
     l_i, l_f <= l_max_wave (parity-filtered per transition), Coulomb-like waves (z = 1: eta = -1/k,
     matching index inside the grid, so n1 < N and the outer tails take part), hydrogenic Z = 2 bound
     states. Synthetic (seeded) stand-ins for the reference's solver outputs. One point per
-    (energy, transition)."""
+    (energy, transition). ``select``: indices of the energies to build (the others only advance the
+    random stream, so a selected point equals the same point of the full sweep)."""
     rng = np.random.default_rng(seed)
     Z, hartree = 2.0, 27.211386245988
     dE = {"2s": 0.75 * Z * Z / 2 * hartree, "2p": 0.75 * Z * Z / 2 * hartree}
     points = []
     energies = np.geomspace(45.0, 1000.0, n_energy)
     for e, E in enumerate(energies):
+        if select is not None and e not in select:
+            rng.uniform(size=2 * 2 * 2 * (l_max_wave + 1))  # the draws of this energy's waves
+            continue
         N = int(round(2000 * 7.5 ** (e / max(1, n_energy - 1))))
         g = make_grid(N, 1e-5, r_max)
         r = g.r
@@ -248,11 +252,12 @@ class _Continuum(_Wave):
         return self.chi_of_r
 
 
-def make_ionization_points(n_ej=40, l_max=30, N=8000, r_max=200.0, seed=5):
+def make_ionization_points(n_ej=40, l_max=30, N=8000, r_max=200.0, seed=5, select=None):
     """H 1s ionization at 200 eV with the shapes of the reference's SDCS loop (ionization.py:526-608):
     per ejected energy, one transition per ejected partial wave l_ej, all (l_i, l_f) pairs with
     l_i + l_f = l_ej (mod 2); the two parity classes are two points on the one grid. Coulomb-like
-    synthetic waves (z = 1, matching index inside the grid) stand in for the solver's."""
+    synthetic waves (z = 1, matching index inside the grid) stand in for the solver's. ``select``:
+    indices of the ejected energies to build (the others only advance the random stream)."""
     rng = np.random.default_rng(seed)
     hartree, E, IP = 27.211386245988, 200.0, 13.605693
     g = make_grid(N, 1e-5, r_max)
@@ -272,7 +277,10 @@ def make_ionization_points(n_ej=40, l_max=30, N=8000, r_max=200.0, seed=5):
     k_i = np.sqrt(2.0 * E / hartree)
     incident = [wave(l, k_i) for l in range(l_max + 1)]
     points = []
-    for E_ej in np.linspace(0.5, 99.0, n_ej):
+    for e, E_ej in enumerate(np.linspace(0.5, 99.0, n_ej)):
+        if select is not None and e not in select:
+            rng.uniform(size=2 * 2 * (l_max + 1))  # the draws of this energy's scattered and ejected waves
+            continue
         k_ej = np.sqrt(2.0 * E_ej / hartree)
         k_s = np.sqrt(2.0 * (E - IP - E_ej) / hartree)
         scat = [wave(l, k_s) for l in range(l_max + 1)]
@@ -404,14 +412,11 @@ def ionization_run(compare=True):
 
 
 # ----------------------------------------------------------------------------- gradients
-def gradient_run(reps=3):
-    """Forward and forward+backward through the differentiable integrals (RadialIntegrals) at the
-    differentiation config's sizes: N = 6000 on [1e-5, 200], l_i, l_f <= 25 with l_i + l_f odd
-    (338 pairs, one s->p transition), L = 0..4, live L=0 correction (V_core != U_i). Inputs are
-    CUDA tensors; the time includes the host planning that every call repeats."""
-    import torch
-    from dwba_b200.autograd import RadialIntegrals
-    rng = np.random.default_rng(9)
+def make_gradient_inputs(seed=9):
+    """Inputs at the differentiation config's sizes: N = 6000 on [1e-5, 200], an s->p transition with
+    l_i, l_f <= 25, l_i + l_f odd (338 pairs), a parametric SAE-like V_core and U_i = V_core + 0.3 e^-r
+    (live L=0 correction), synthetic waves. Returns (grid, V, U, bound_i, bound_f, pairs, rng)."""
+    rng = np.random.default_rng(seed)
     g = make_grid(6000, 1e-5, 200.0)
     r = g.r
     V = -(1.0 + 10.0 * np.exp(-3.0 * r) + 2.0 * r * np.exp(-1.5 * r) + np.exp(-0.8 * r)) / r
@@ -427,6 +432,17 @@ def gradient_run(reps=3):
     wi = [wave(l, k_i) for l in range(26)]
     wf = [wave(l, k_f) for l in range(26)]
     pairs = [(wi[a], wf[b]) for a in range(26) for b in range(26) if (a + b) % 2 == 1]
+    return g, V, U, bi, bf, pairs, rng
+
+
+def gradient_run(reps=3):
+    """Forward and forward+backward through the differentiable integrals (RadialIntegrals) at the
+    differentiation config's sizes: N = 6000 on [1e-5, 200], l_i, l_f <= 25 with l_i + l_f odd
+    (338 pairs, one s->p transition), L = 0..4, live L=0 correction (V_core != U_i). Inputs are
+    CUDA tensors; the time includes the host planning that every call repeats."""
+    import torch
+    from dwba_b200.autograd import RadialIntegrals
+    g, V, U, bi, bf, pairs, rng = make_gradient_inputs()
     model = RadialIntegrals(g, bi, bf, pairs, 4, U_f_array=U, engine="semisep")
     model_tc = RadialIntegrals(g, bi, bf, pairs, 4, U_f_array=U, engine="semisep", backward="tc_bf16x3",
                                gpu_cache=model.cache)

@@ -1,7 +1,7 @@
 """Config-1 fixture: H 1s->2p at 50 eV, N = 3000 on r in [1e-5, 200], l_i, l_f = 0..15, L = 0..4.
 
-Runs only where the reference source tree is available (``DWBA_REFERENCE_PATH``, default
-``/root/reference``). It builds the inputs with the reference's own solvers (exponential grid,
+Runs only where the reference source tree is available (its directory in the environment
+variable ``DWBA_REFERENCE_PATH``, which must be set). It builds the inputs with the reference's own solvers (exponential grid,
 eigensolver bound states, static distorting potentials, distorted waves), evaluates
 ``radial_ME_all_L`` for all 128 parity-allowed pairs, and turns the integrals into amplitudes,
 the DCS on 181 angles and the TCS with the reference's ``dwba_coupling`` and ``sigma_total``
@@ -22,7 +22,9 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("DWBA_REFERENCE_PATH", "/root/reference")
+REF = os.environ.get("DWBA_REFERENCE_PATH")
+if not REF:
+    sys.exit("set DWBA_REFERENCE_PATH to the reference source tree (the directory holding dwba_matrix_elements.py)")
 
 import scipy.special as _ss  # noqa: E402
 

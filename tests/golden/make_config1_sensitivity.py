@@ -10,8 +10,8 @@ and stores the exact gradients dDCS/dI (at 19 angles) and dTCS/dI (TCS through
 ``integrate_dcs_over_angles``, sigma_total.py:179-217). With them a test on a machine without the
 reference turns per-integral errors dI into DCS/TCS errors: dTCS = g . dI + O(|dI|^2).
 
-Runs only where the reference source tree is available (``DWBA_REFERENCE_PATH``, default
-``/root/reference``). Usage:  python tests/golden/make_config1_sensitivity.py
+Runs only where the reference source tree is available (its directory in the environment
+variable ``DWBA_REFERENCE_PATH``, which must be set). Usage:  python tests/golden/make_config1_sensitivity.py
 """
 from __future__ import annotations
 
@@ -23,7 +23,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("DWBA_REFERENCE_PATH", "/root/reference")
+REF = os.environ.get("DWBA_REFERENCE_PATH")
+if not REF:
+    sys.exit("set DWBA_REFERENCE_PATH to the reference source tree (the directory holding dwba_matrix_elements.py)")
 
 import scipy.special as _ss  # noqa: E402
 

@@ -1,7 +1,8 @@
 """Generate the golden I_L fixtures by running the reference implementation.
 
 This script runs only where the reference source tree is available (it is
-imported from ``DWBA_REFERENCE_PATH``, default ``/root/reference``). It writes
+imported from the directory named by the environment variable ``DWBA_REFERENCE_PATH``,
+which must be set). It writes
 small ``.npz`` fixtures next to itself; the tests read those fixtures and never
 touch the reference.
 
@@ -25,7 +26,9 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("DWBA_REFERENCE_PATH", "/root/reference")
+REF = os.environ.get("DWBA_REFERENCE_PATH")
+if not REF:
+    sys.exit("set DWBA_REFERENCE_PATH to the reference source tree (the directory holding dwba_matrix_elements.py)")
 
 import scipy.special as _ss  # noqa: E402
 
@@ -190,6 +193,49 @@ def case_synthetic_batch():
                wi, wf, calls)
 
 
+def case_large_grid():
+    """Synthetic waves on N = 5001 points to r = 400 at L = 0..8: the largest grid the reference's
+    CPU path evaluates here in reasonable time and memory (its exchange gather holds n1 x N_cc
+    temporaries), a high partial wave (l = 63), and a Coulomb-like pair (eta != 0, matching point
+    inside the grid) whose outer tails are active."""
+    rng = np.random.default_rng(7)
+    N = 5001
+    grid = make_r_grid(1e-5, 400.0, N)
+    r = grid.r
+    bounds = []
+    for _ in range(2):
+        a = int(rng.integers(1, 3))
+        b = float(rng.uniform(0.5, 2.0))
+        c = rng.uniform(-1, 1, size=3)
+        u = r ** a * np.exp(-b * r) * (c[0] + c[1] * r + c[2] * r * r)
+        u /= np.sqrt(np.sum(grid.w_trapz * u * u))
+        bounds.append(u)
+    im = int(np.searchsorted(r, 240.0))
+    wi, wf = {}, {}
+    for idx, (l1, k1, l2, k2, coul) in enumerate([(0, 0.7, 63, 1.3, False), (5, 2.0, 6, 1.5, False),
+                                                  (2, 1.1, 3, 0.9, True)]):
+        d1, d2 = rng.uniform(0, np.pi, size=2)
+        if coul:
+            s1, s2 = rng.uniform(-1, 1, size=2)
+            e1, e2 = -1.0 / k1, -1.0 / k2
+            c1 = np.sin(k1 * r - 0.5 * l1 * np.pi + e1 * np.log(2 * k1 * r) + s1 + d1) * \
+                (1.0 - np.exp(-(r * k1 / (l1 + 1)) ** (l1 + 1)))
+            c2 = np.sin(k2 * r - 0.5 * l2 * np.pi + e2 * np.log(2 * k2 * r) + s2 + d2) * \
+                (1.0 - np.exp(-(r * k2 / (l2 + 1)) ** (l2 + 1)))
+            wi[idx] = ContinuumWave(l=l1, k_au=k1, chi_of_r=c1, phase_shift=float(d1), idx_match=im, eta=e1,
+                                    sigma_l=float(s1))
+            wf[idx] = ContinuumWave(l=l2, k_au=k2, chi_of_r=c2, phase_shift=float(d2), idx_match=im, eta=e2,
+                                    sigma_l=float(s2))
+        else:
+            wi[idx] = ContinuumWave(l=l1, k_au=k1, chi_of_r=_synthetic_wave(r, k1, l1, d1, (l1 + 1) / k1),
+                                    phase_shift=float(d1))
+            wf[idx] = ContinuumWave(l=l2, k_au=k2, chi_of_r=_synthetic_wave(r, k2, l2, d2, (l2 + 1) / k2),
+                                    phase_shift=float(d2))
+    V = -1.0 / r
+    calls = [dict(li=i, lf=i, L_max=8, kw={}) for i in range(3)]
+    _save_case("large_grid_n5001", grid, V, V, V, bounds[0], bounds[1], False, None, wi, wf, calls)
+
+
 def case_low_k():
     """k_i + k_f <= k_threshold: standard Simpson path; non-orthogonal u_f makes the L=0 correction live."""
     N = 801
@@ -255,9 +301,9 @@ def unit_fixtures():
 
 
 if __name__ == "__main__":
-    unit_fixtures()
-    case_low_k()
-    case_synthetic_batch()
-    case_h_excitation()
-    case_heplus_ionic()
-    case_ionization()
+    CASES = {"unit": unit_fixtures, "low_k": case_low_k, "synthetic_batch": case_synthetic_batch,
+             "h_excitation": case_h_excitation, "heplus_ionic": case_heplus_ionic, "ionization": case_ionization,
+             "large_grid": case_large_grid}
+    # python tests/golden/make_golden.py [case ...]   (all cases without arguments)
+    for name in (sys.argv[1:] or list(CASES)):
+        CASES[name]()

@@ -93,3 +93,42 @@ def rel_err(x, ref):
     x = np.asarray(x, dtype=float)
     ref = np.asarray(ref, dtype=float)
     return np.abs(x - ref) / np.maximum(np.abs(ref), 1e-300)
+
+
+def levin_condition(w, r_m, r_max):
+    """Largest condition number of the 8-node Levin collocation systems a record solves (0 when
+    both phase branches take Filon). The reference builds them with the differentiation matrix of
+    descending Chebyshev points on ascending nodes (oscillatory_integrals.py:970-1095); these
+    systems reach condition numbers of 1e10, so two correct LU solves agree only to ~1e-16 cond."""
+    ka, la, _, ea, _, kb, lb, _, eb, _ = w
+    n = 8
+    x = np.cos(np.pi * np.arange(n) / (n - 1))
+    c = np.ones(n)
+    c[0] = c[-1] = 2.0
+    D = np.zeros((n, n))
+    for i in range(n):
+        for j in range(n):
+            if i != j:
+                D[i, j] = (c[i] / c[j]) * (-1.0) ** (i + j) / (x[i] - x[j])
+        D[i, i] = -D[i].sum()
+    worst = 0.0
+    for sgn in (-1, 1):
+        def d1(r):
+            v = (ka - kb if sgn < 0 else ka + kb) + ea / r + (-eb / r if sgn < 0 else eb / r)
+            v = v + la * (la + 1) / (2 * ka * r * r)
+            t = lb * (lb + 1) / (2 * kb * r * r)
+            return v - t if sgn < 0 else v + t
+
+        def d2(r):
+            v = -ea / r ** 2 + (eb / r ** 2 if sgn < 0 else -eb / r ** 2) - la * (la + 1) / (ka * r ** 3)
+            t = lb * (lb + 1) / (kb * r ** 3)
+            return v + t if sgn < 0 else v - t
+        mid = (r_m + r_max) / 2
+        h = np.pi / 4 / abs(d1(mid))
+        if abs(d2(mid)) * h * h < 0.1:
+            continue
+        bnd = np.linspace(r_m, r_max, int(max(1, np.ceil((r_max - r_m) / h))) + 1)
+        for a, b in zip(bnd[:-1], bnd[1:]):
+            xs = 0.5 * (b - a) * (x[::-1] + 1) + a
+            worst = max(worst, np.linalg.cond(D * (2 / (xs[-1] - xs[0])) + np.diag(1j * d1(xs))))
+    return worst

@@ -7,6 +7,7 @@ import pytest
 import torch
 
 from dwba_b200 import _lib
+from golden_cases import levin_condition
 
 pytestmark = pytest.mark.gpu
 
@@ -57,45 +58,6 @@ def test_unit_fixture_tails(mode):
         assert np.all(got[k, others] == 0.0)
 
 
-def _levin_condition(w, r_m, r_max):
-    """Largest condition number of the 8-node Levin collocation systems a record solves (0 when
-    both phase branches take Filon). The reference builds them with the differentiation matrix of
-    descending Chebyshev points on ascending nodes (oscillatory_integrals.py:970-1095); these
-    systems reach condition numbers of 1e10, so two correct LU solves agree only to ~1e-16 cond."""
-    ka, la, _, ea, _, kb, lb, _, eb, _ = w
-    n = 8
-    x = np.cos(np.pi * np.arange(n) / (n - 1))
-    c = np.ones(n)
-    c[0] = c[-1] = 2.0
-    D = np.zeros((n, n))
-    for i in range(n):
-        for j in range(n):
-            if i != j:
-                D[i, j] = (c[i] / c[j]) * (-1.0) ** (i + j) / (x[i] - x[j])
-        D[i, i] = -D[i].sum()
-    worst = 0.0
-    for sgn in (-1, 1):
-        def d1(r):
-            v = (ka - kb if sgn < 0 else ka + kb) + ea / r + (-eb / r if sgn < 0 else eb / r)
-            v = v + la * (la + 1) / (2 * ka * r * r)
-            t = lb * (lb + 1) / (2 * kb * r * r)
-            return v - t if sgn < 0 else v + t
-
-        def d2(r):
-            v = -ea / r ** 2 + (eb / r ** 2 if sgn < 0 else -eb / r ** 2) - la * (la + 1) / (ka * r ** 3)
-            t = lb * (lb + 1) / (kb * r ** 3)
-            return v + t if sgn < 0 else v - t
-        mid = (r_m + r_max) / 2
-        h = np.pi / 4 / abs(d1(mid))
-        if abs(d2(mid)) * h * h < 0.1:
-            continue
-        bnd = np.linspace(r_m, r_max, int(max(1, np.ceil((r_max - r_m) / h))) + 1)
-        for a, b in zip(bnd[:-1], bnd[1:]):
-            xs = 0.5 * (b - a) * (x[::-1] + 1) + a
-            worst = max(worst, np.linalg.cond(D * (2 / (xs[-1] - xs[0])) + np.diag(1j * d1(xs))))
-    return worst
-
-
 def test_random_records_match_host():
     """Coulomb and neutral waves, l up to 20, short and long outer intervals, Filon and Levin branches.
     Filon records agree to round-off; Levin records to round-off times the system's condition number."""
@@ -124,7 +86,7 @@ def test_random_records_match_host():
     moms[::7, 2] = 0.0  # moments below the cut-off give a zero tail
     keep = np.array([_lib.tail_on_device(w, a, b) for w, a, b in zip(waves, r_m, r_max)])
     assert keep.all()
-    cond = np.array([_levin_condition(w, a, b) for w, a, b in zip(waves, r_m, r_max)])
+    cond = np.array([levin_condition(w, a, b) for w, a, b in zip(waves, r_m, r_max)])
     assert (cond == 0).sum() >= 20 and (cond > 0).sum() >= 10  # both branches exercised
     for mode in (0, 1):
         got = _device_tails(waves, r_m, r_max, moms, mode, L_max)
@@ -178,7 +140,7 @@ def test_many_multipoles_in_several_chunks():
     moms = rng.normal(size=(n, L_max + 1)) * 10.0 ** rng.uniform(-2, 1, (n, 1))
     moms[::5, 9:17] = 0.0  # a whole chunk of zero moments
     assert all(_lib.tail_on_device(w, a, b) for w, a, b in zip(waves, r_m, r_max))
-    cond = np.array([_levin_condition(w, a, b) for w, a, b in zip(waves, r_m, r_max)])
+    cond = np.array([levin_condition(w, a, b) for w, a, b in zip(waves, r_m, r_max)])
     for mode in (0, 1):
         got = _device_tails(waves, r_m, r_max, moms, mode, L_max)
         for k in range(n):

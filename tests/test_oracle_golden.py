@@ -10,7 +10,7 @@ from oracle.tails import analytical_multipole_tail, outer_integral_1d
 
 UNIT = np.load(gc.GOLDEN_DIR + "/unit_quadrature.npz")
 # The full restatement materialises N x N_cc exchange temporaries like the reference: keep it to small cases.
-FAST = [c for c in gc.all_calls() if not c["label"].startswith("synthetic")]
+FAST = [c for c in gc.all_calls() if not c["label"].startswith(("synthetic", "large_grid"))]
 
 
 def _gate(x, ref, scale, rel=1e-12, abs_scale=1e-14):

@@ -80,6 +80,7 @@ def _declare(lib):
         "dwba_cross_sections": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_dbl,
                                         c_vp, c_vp, c_vp]),
         "dwba_outer_tail_on_device": (c_int, [c_vp, c_dbl, c_dbl]),
+        "dwba_tc_set_wait_cycles": (c_int, [c_i64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

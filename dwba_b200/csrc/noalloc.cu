@@ -27,19 +27,43 @@ static __device__ __align__(256) double g_noalloc_partials[DWBA_NOALLOC_SCRATCH_
 constexpr int MAX_DEVICES = 64;
 std::mutex g_mutex;
 double* g_scratch[MAX_DEVICES] = {nullptr};
+void* g_scratch_ctx[MAX_DEVICES] = {nullptr};
 
-// Device address of the scratch array on the current device (set up once per device).
+// The calling thread's current driver context (through the runtime's driver entry point, so
+// the library needs no link against the driver library); nullptr if it cannot be read.
+void* current_context() {
+  using ctx_fn = int (*)(void**);
+  static ctx_fn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<ctx_fn>(p);
+    tried = true;
+  }
+  void* ctx = nullptr;
+  if (fn == nullptr || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
+
+// Device address of the scratch array on the current device, looked up once per device and
+// context: a device reset (cudaDeviceReset) ends the context and reloads this module, so the
+// address is looked up again in the new context.
 int scratch_ptr(double** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return DWBA_ERR_CUDA;
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (g_scratch[dev] == nullptr) {
+  void* ctx = current_context();
+  if (g_scratch[dev] == nullptr || ctx == nullptr || ctx != g_scratch_ctx[dev]) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || p == nullptr) {
       cudaGetLastError();
       return DWBA_ERR_CUDA;
     }
     g_scratch[dev] = static_cast<double*>(p);
+    g_scratch_ctx[dev] = current_context();
   }
   *out = g_scratch[dev];
   return DWBA_OK;
@@ -178,7 +202,8 @@ noalloc_tri_kernel(const dwba_form_t* __restrict__ forms, int max_chunks, int L0
   }
 }
 
-// Adds each form's partials in chunk order; a form larger than max_m gets NaN.
+// Adds each form's partials in chunk order; a form larger than max_m gets NaN, an empty form
+// (no rows and no columns) the empty sum 0.
 __global__ void noalloc_reduce_kernel(const dwba_form_t* __restrict__ forms, int n_forms, int max_chunks, int n_ltot,
                                       const double* __restrict__ partials, double* __restrict__ out) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -186,8 +211,12 @@ __global__ void noalloc_reduce_kernel(const dwba_form_t* __restrict__ forms, int
   const int f = (int)(idx / n_ltot), l = (int)(idx - (int64_t)f * n_ltot);
   const dwba_form_t F = forms[f];
   const int M = F.n_rows > F.n_cols ? F.n_rows : F.n_cols;
-  const int nc = M >= 1 ? chunks_of(M) : 0;
-  if (nc > max_chunks || M < 1) {
+  if (M < 1) {
+    out[idx] = 0.0;
+    return;
+  }
+  const int nc = chunks_of(M);
+  if (nc > max_chunks) {
     out[idx] = __longlong_as_double(0x7ff8000000000000LL);
     return;
   }

@@ -25,6 +25,8 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "common.cuh"
 
 namespace {
@@ -53,6 +55,7 @@ struct GemmParams {
   int* status;                 // error word
   const double* gw;            // gradient mode: dLoss/dI per (form, L), [n_forms][n_Ltot]
   double* gpart;               // gradient mode: g_f,L (K_L b_f)_i per L, [n_L][f_pad][n_pad]
+  long long wait_cycles;       // bound of every pipeline wait (SM clocks)
   int n_grid, n_pad, f_pad, n_iblk, L_max, n_forms, n_kb, n_Ltot;
   double diag[DWBA_MAX_L + 1];
 };
@@ -79,12 +82,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
       : "memory");
   return ok != 0;
 }
-// bounded wait (about a second of SM clocks); returns false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+// bounded wait (limit in SM clocks; the pipeline passes P.wait_cycles, the error-path drain the
+// default of about a second); returns false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, long long limit) {
   const long long t0 = clock64();
   while (true) {
     if (mbar_try_wait(bar, phase)) return true;
-    if (clock64() - t0 > WAIT_CYCLES) return false;
+    if (clock64() - t0 > limit) return false;
   }
 }
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
@@ -299,8 +303,8 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
       for (int step = 0; step < n_kb; ++step) {
         const int s = step % S;
         const uint32_t par = (uint32_t)((step / S) & 1);
-        good = mbar_wait(&bar_a[s], par) && !s_abort;
-        if (good) good = mbar_wait(&bar_b[s], par);
+        good = mbar_wait(&bar_a[s], par, P.wait_cycles) && !s_abort;
+        if (good) good = mbar_wait(&bar_b[s], par, P.wait_cycles);
         if (!good) break;
         b_pending[s] = false;
         tc_fence_after();
@@ -325,7 +329,7 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
           // block n_issued = step + S - 1 goes into the stage of block step-1, free once its
           // products completed
           const int sp = n_issued % S;
-          if (step >= 1) good = mbar_wait(&bar_mma[sp], (uint32_t)(((step - 1) / S) & 1));
+          if (step >= 1) good = mbar_wait(&bar_mma[sp], (uint32_t)(((step - 1) / S) & 1), P.wait_cycles);
           if (!good) break;
           issue_tma(sp, order.next(), n_issued);
           ++n_issued;
@@ -367,7 +371,7 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
       const int kb_next = step + 1 < n_kb ? order.next() : -1;
       if (kb_next >= 0) load_factors(kb_next, v_nxt, s_nxt);  // in flight while this block is generated
       // stage s is free once the products of block step-S completed
-      if (step >= S) good = mbar_wait(&bar_mma[s], (uint32_t)(((step - S) / S) & 1));
+      if (step >= S) good = mbar_wait(&bar_mma[s], (uint32_t)(((step - S) / S) & 1), P.wait_cycles);
       good = __all_sync(0xffffffffu, good && !s_abort);  // warp-uniform: the warp arrives all or none
       if (!good) break;
       tc_fence_after();
@@ -418,15 +422,19 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
       s_cur = s_nxt;
     }
     // every product has completed once the last commit arrived (commits track all prior MMAs)
-    if (good) good = mbar_wait(&bar_mma[(n_kb - 1) % S], (uint32_t)(((n_kb - 1) / S) & 1));
+    if (good) good = mbar_wait(&bar_mma[(n_kb - 1) % S], (uint32_t)(((n_kb - 1) / S) & 1), P.wait_cycles);
     if (!good) s_abort = 1;
   }
   __syncthreads();
-  // error path (thread 0): wait, bounded, for the copies still in flight and the last commit
+  // error path (thread 0, the issuer): wait, bounded by the default limit whatever the pipeline's,
+  // for the copies still in flight and the last commit. Each barrier waited on here is at most one
+  // phase behind the one named: a stage's copy is issued only after the previous copy into it
+  // was consumed, and the last commit follows the completion of the stage's previous commit
+  // (the generators waited for it before writing the block the issuer committed)
   if (tid == 0 && s_abort) {
     for (int q = 0; q < S; ++q)
-      if (b_pending[q]) mbar_wait(&bar_b[q], (uint32_t)((b_step[q] / S) & 1));
-    if (last_commit >= 0) mbar_wait(&bar_mma[last_commit % S], (uint32_t)((last_commit / S) & 1));
+      if (b_pending[q]) mbar_wait(&bar_b[q], (uint32_t)((b_step[q] / S) & 1), WAIT_CYCLES);
+    if (last_commit >= 0) mbar_wait(&bar_mma[last_commit % S], (uint32_t)((last_commit / S) & 1), WAIT_CYCLES);
     atomicExch(P.status, 2);
   }
   __syncthreads();
@@ -614,6 +622,14 @@ __global__ void tc_grad_reduce_kernel(const double* __restrict__ gpart, const dw
   }
 }
 
+// bound of the pipeline waits of the next launches (process-wide; 0 = WAIT_CYCLES)
+std::atomic<long long> g_wait_cycles{0};
+
+long long wait_cycles() {
+  const long long c = g_wait_cycles.load();
+  return c > 0 ? c : WAIT_CYCLES;
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -691,6 +707,7 @@ extern "C" int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, 
   P.status = status_dev;
   P.gw = nullptr;
   P.gpart = nullptr;
+  P.wait_cycles = wait_cycles();
   P.n_Ltot = L_max + 1;
   for (int l = 0; l <= DWBA_MAX_L; ++l) P.diag[l] = l <= L_max ? diag_scale_host[l] : 0.0;
   uint8_t* ws = (uint8_t*)workspace;
@@ -776,6 +793,7 @@ extern "C" int dwba_bilinear_tc_bf16_backward(const dwba_form_grad_t* forms_dev,
   P.n_forms = n_forms;
   P.status = status_dev;
   P.gw = grad_dev;
+  P.wait_cycles = wait_cycles();
   P.n_Ltot = n_L;
   P.partial = nullptr;
   for (int l = 0; l <= DWBA_MAX_L; ++l) P.diag[l] = l <= L_max ? diag_scale_host[l] : 0.0;
@@ -832,5 +850,11 @@ extern "C" int dwba_bilinear_tc_bf16_backward(const dwba_form_grad_t* forms_dev,
         P.gpart, forms_dev, n_forms, P.f_pad, P.n_pad, n_L, which);
     DWBA_CHECK_LAUNCH();
   }
+  return DWBA_OK;
+}
+
+extern "C" int dwba_tc_set_wait_cycles(int64_t cycles) {
+  if (cycles < 0) return DWBA_ERR_INVALID_ARG;
+  g_wait_cycles.store((long long)cycles);
   return DWBA_OK;
 }

@@ -154,11 +154,12 @@ int dwba_bilinear_dense_fp64(const dwba_form_t* forms_dev, int n_forms, int L_ma
  * which synchronise the device. Inputs and the output are still the caller's;
  * the partial sums live in a fixed array of DWBA_NOALLOC_SCRATCH_DOUBLES doubles
  * (8 MiB) inside the library, held by every GPU that loads it until exit.
- * max_m must be >= max(n_rows, n_cols) of every form (a form above it gets NaN);
- * requests needing more than the array, n_forms * ceil(ceil(max_m/128)/2) *
- * (L_max+1) doubles, return DWBA_ERR_WORKSPACE. The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress), so make that first call
- * before any stream capture. All calls share the array: calls that overlap on
+ * max_m must be >= max(n_rows, n_cols) of every form (a form above it gets NaN;
+ * an empty form, no rows and no columns, gets the empty sum 0); requests needing
+ * more than the array, n_forms * ceil(ceil(max_m/128)/2) * (L_max+1) doubles,
+ * return DWBA_ERR_WORKSPACE. The first call on a device (and the first after a
+ * device reset) looks up the array's device address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture. All calls share the array: calls that overlap on
  * the GPU race and must be ordered by the caller (e.g. one stream). Results
  * equal dwba_bilinear_dense_fp64's (same tiles and summation order). */
 #define DWBA_NOALLOC_SCRATCH_DOUBLES (1 << 20)
@@ -238,6 +239,15 @@ int64_t dwba_tc_backward_workspace_bytes(int n_forms, int n_grid, int L_max, int
 int dwba_bilinear_tc_bf16_backward(const dwba_form_grad_t* forms_dev, int n_forms, const double* r_dev, int n_grid,
                                    int L_max, int n_terms, const double* diag_scale_host, const double* grad_dev,
                                    void* workspace, int64_t workspace_bytes, int* status_dev, dwba_stream_t stream);
+
+/* Bound of every pipeline wait of the tensor-core kernels (dwba_bilinear_tc_bf16 and its backward)
+ * launched after this call, in SM clock cycles; 0 restores the default (about one second). No
+ * reference counterpart: it lets a test make a wait run out on a normal input. A wait that runs
+ * out sets the call's status word to 2; its CTA then waits, with the default bound, for its own
+ * copies and products in flight, frees its tensor memory and returns, and CTAs that start after
+ * the status was set skip their work, so the next call runs normally. The setting is process-wide
+ * and read when a call launches. */
+int dwba_tc_set_wait_cycles(int64_t cycles);
 
 /* Adjoint of dwba_fold: z = Op^T y for the banded operator of a fold (same op layout), i.e.
  * dLoss/d(f .* g) for y = dLoss/d(out). z gets n_src values. No reference counterpart. */

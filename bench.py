@@ -436,51 +436,69 @@ def make_gradient_inputs(seed=9):
 
 
 def gradient_run(reps=3):
-    """Forward and forward+backward through the differentiable integrals (RadialIntegrals) at the
-    differentiation config's sizes: N = 6000 on [1e-5, 200], l_i, l_f <= 25 with l_i + l_f odd
-    (338 pairs, one s->p transition), L = 0..4, live L=0 correction (V_core != U_i). Inputs are
-    CUDA tensors; the time includes the host planning that every call repeats."""
+    """The differentiation config end to end: Na-like 3s -> 3p in the parametric SAE core potential
+    V = -[1 + 10 e^{-a1 r} + a2 r e^{-a3 r} + a4 e^{-a5 r}]/r (a seeded within +-10 % of
+    (3.0, 2.0, 1.5, 1.0, 0.8)), N = 6000 on [1e-5, 200], E = 20 eV, l_i, l_f <= 25 (338 pairs), L = 0..4.
+    The inputs come from dwba_b200/sae.py's solvers; dTCS/d(a1..a5) is the CUDA backward (FP64, and the
+    split-BF16 tensor-core backward with FP32 accumulation) contracted with the solvers' central-
+    difference tangents, against central differences of the TCS (h = 1e-6 relative). Times: the
+    integrals' forward and forward+backward from CUDA tensors (host planning included), and one whole
+    parameter gradient (11 solver runs, forward, backward, contraction)."""
     import torch
+    from dwba_b200 import sae
     from dwba_b200.autograd import RadialIntegrals
-    g, V, U, bi, bf, pairs, rng = make_gradient_inputs()
-    model = RadialIntegrals(g, bi, bf, pairs, 4, U_f_array=U, engine="semisep")
-    model_tc = RadialIntegrals(g, bi, bf, pairs, 4, U_f_array=U, engine="semisep", backward="tc_bf16x3",
+    from dwba_b200.coupling import CouplingTables
+    from dwba_b200.fit import CouplingCrossSection
+    g = make_grid(6000, 1e-5, 200.0)
+    p = np.random.default_rng(2).uniform(0.9, 1.1, 5) * np.array([3.0, 2.0, 1.5, 1.0, 0.8])
+    prob = sae.SAEProblem(g, sae.Transition(E_eV=20.0, l_max=25, L_max=4), p,
+                          full_params=lambda q: np.concatenate([[10.0], q]))
+    x0 = prob.inputs(p)
+    bi, bf, pairs = prob.wave_objects(x0)
+    model = RadialIntegrals(g, bi, bf, pairs, 4, U_f_array=x0.U_f, engine="semisep")
+    model_tc = RadialIntegrals(g, bi, bf, pairs, 4, U_f_array=x0.U_f, engine="semisep", backward="tc_bf16x3",
                                gpu_cache=model.cache)
-    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")  # noqa: E731
-    x = dict(V_core=t(V), U_i=t(U), u_i=t(bi.u_of_r), u_f=t(bf.u_of_r),
-             chi_i=t(np.stack([p[0].chi_of_r for p in pairs])), chi_f=t(np.stack([p[1].chi_of_r for p in pairs])))
-    c = t(rng.normal(size=(len(pairs), 2, 5)))
+    xs = CouplingCrossSection(CouplingTables(np.linspace(0.0, np.pi, 181), prob.pairs_l, 4, prob.k_i, prob.k_f, 0, 1))
+    x = prob.torch_inputs(x0)
 
     def fwd():
         with torch.no_grad():
-            return float((model(**x) * c).sum())
+            return float(xs.tcs(model(**x)))
 
     def fwd_bwd(m=model):
-        xs = {k: v.clone().requires_grad_(True) for k, v in x.items()}
-        loss = (m(**xs) * c).sum()
+        xg = {k: v.clone().requires_grad_(True) for k, v in x.items()}
+        loss = xs.tcs(m(**xg))
         loss.backward()
-        return {k: v.grad for k, v in xs.items()}
+        return {k: v.grad for k, v in xg.items()}
     g64 = fwd_bwd()
     gtc = fwd_bwd(model_tc)
-    rel = {k: float(torch.linalg.norm(gtc[k] - g64[k]) / torch.linalg.norm(g64[k])) for k in g64}
+    rel_in = {k: float(torch.linalg.norm(gtc[k] - g64[k]) / torch.linalg.norm(g64[k])) for k in g64}
+    tcs, grad, fd = sae.value_and_grad(prob, model, xs.tcs, p, with_fd=True)
+    _, grad_tc = sae.value_and_grad(prob, model_tc, xs.tcs, p)
     fwd()
     torch.cuda.synchronize()
     out = {}
     for name, fn in (("forward_ms", fwd), ("forward_backward_ms", fwd_bwd),
-                     ("forward_backward_tc_bf16x3_ms", lambda: fwd_bwd(model_tc))):
+                     ("forward_backward_tc_bf16x3_ms", lambda: fwd_bwd(model_tc)),
+                     ("parameter_gradient_ms", lambda: sae.value_and_grad(prob, model, xs.tcs, p))):
         t0 = time.perf_counter()
         for _ in range(reps):
             fn()
         torch.cuda.synchronize()
         out[name] = (time.perf_counter() - t0) * 1e3 / reps
-    return {"workload": "differentiation sizes: N=6000 exp grid r in [1e-5,200], 338 (l_i, l_f <= 25) pairs of one "
-                        "s->p transition, L=0..4, parametric SAE-like V_core, synthetic waves",
-            "integrals": len(pairs) * 2 * 5, "gradient_inputs": "V_core, U_i, u_i, u_f, chi_i, chi_f",
-            **out, "tc_bf16x3_vs_fp64_gradient_rel_err": rel,
-            "note": "wall time per call through RadialIntegrals (host planning, FP64 forward, exact FP64 backward "
-                    "kernels, or the split-BF16 tensor-core backward with FP32 accumulation); rel err = |g_tc - "
-                    "g_fp64| / |g_fp64| per input; the FP64 gradients are checked against central differences in "
-                    "tests/test_gpu_autograd.py"}
+    return {"workload": "differentiation config: Na-like 3s->3p, parametric SAE potential, N=6000 exp grid r in "
+                        "[1e-5,200], E=20 eV, 338 (l_i, l_f <= 25) pairs, L=0..4, inputs from the parameters by "
+                        "dwba_b200/sae.py's solvers",
+            "integrals": len(pairs) * 2 * 5, "parameters": [float(v) for v in p], "tcs_au": tcs,
+            "dtcs_dparams": [float(v) for v in grad], "dtcs_dparams_central_fd": [float(v) for v in fd],
+            "dtcs_dparams_rel_err_vs_fd_max": float(np.max(np.abs(grad - fd) / np.abs(fd))),
+            "dtcs_dparams_tc_bf16x3_rel_err_max": float(np.max(np.abs(grad_tc - grad) / np.abs(grad))),
+            **out, "tc_bf16x3_vs_fp64_input_gradient_rel_err": rel_in,
+            "note": "forward/backward wall time per call through RadialIntegrals + the torch TCS (host planning, "
+                    "FP64 forward, exact FP64 backward kernels, or the split-BF16 tensor-core backward with FP32 "
+                    "accumulation); dTCS/da by the backward chained with central-difference solver tangents, "
+                    "against central differences of the TCS (h = 1e-6 relative); input gradient rel err = "
+                    "|g_tc - g_fp64| / |g_fp64| per input function"}
 
 
 # ----------------------------------------------------------------------------- drop-in calls

@@ -36,6 +36,10 @@ FOLD_MULTI = 8
 FOLD_MULTI_DTYPE = np.dtype([("op", "<u8"), ("g", "<u8"), ("f", "<u8", (FOLD_MULTI,)), ("out", "<u8", (FOLD_MULTI,)),
                              ("n_f", "<i4"), ("half_band", "<i4"), ("n_out", "<i4"), ("n_src", "<i4"),
                              ("n_clear", "<i4"), ("pad", "<i4")])
+POTENTIAL_DTYPE = np.dtype([("r", "<u8"), ("b", "<u8"), ("phi", "<u8"), ("n_rows", "<i4"), ("n_cols", "<i4"),
+                            ("stride", "<i4"), ("pad", "<i4")])
+DOT_DTYPE = np.dtype([("a", "<u8"), ("phi", "<u8"), ("out", "<u8"), ("n_rows", "<i4"), ("stride", "<i4")])
+DOT_RUN = 16  # descriptors per run sharing one potential (dwba_dot_forms)
 TAIL_DTYPE = np.dtype([("wave", "<f8", (10,)), ("r_m", "<f8"), ("r_max", "<f8"), ("moments", "<u8"), ("out", "<u8"),
                        ("mode", "<i4"), ("pad", "<i4")])
 
@@ -81,6 +85,8 @@ def _declare(lib):
                                         c_vp, c_vp, c_vp]),
         "dwba_outer_tail_on_device": (c_int, [c_vp, c_dbl, c_dbl]),
         "dwba_tc_set_wait_cycles": (c_int, [c_i64]),
+        "dwba_multipole_potentials": (c_int, [c_vp, c_int, c_int, c_vp, c_dbl, c_dbl, c_vp]),
+        "dwba_dot_forms": (c_int, [c_vp, c_int, c_int, c_vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -100,10 +106,11 @@ def load():
     lib = _declare(ctypes.CDLL(LIB_PATH))
     if lib.dwba_abi_version() != 1:
         raise ImportError("libdwba_b200.so ABI version mismatch")
-    sizes = (ctypes.c_int64 * 7)()
-    lib.dwba_struct_sizes(sizes, 7)
+    sizes = (ctypes.c_int64 * 9)()
+    lib.dwba_struct_sizes(sizes, 9)
     want = (NODESET_DTYPE.itemsize, FOLD_DTYPE.itemsize, FORM_DTYPE.itemsize, TAIL_DTYPE.itemsize,
-            FORM_GRAD_DTYPE.itemsize, FOLD_ADJ_DTYPE.itemsize, FOLD_MULTI_DTYPE.itemsize)
+            FORM_GRAD_DTYPE.itemsize, FOLD_ADJ_DTYPE.itemsize, FOLD_MULTI_DTYPE.itemsize,
+            POTENTIAL_DTYPE.itemsize, DOT_DTYPE.itemsize)
     if tuple(sizes) != want:
         raise ImportError(f"struct layout mismatch: library {tuple(sizes)} vs binding {want}")
     _lib = lib

@@ -460,6 +460,8 @@ extern "C" int dwba_struct_sizes(int64_t* sizes, int n) {
   if (n >= 5) sizes[4] = (int64_t)sizeof(dwba_form_grad_t);
   if (n >= 6) sizes[5] = (int64_t)sizeof(dwba_fold_adj_t);
   if (n >= 7) sizes[6] = (int64_t)sizeof(dwba_fold_multi_t);
+  if (n >= 8) sizes[7] = (int64_t)sizeof(dwba_potential_t);
+  if (n >= 9) sizes[8] = (int64_t)sizeof(dwba_dot_t);
   return DWBA_OK;
 }
 

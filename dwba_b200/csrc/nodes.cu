@@ -102,6 +102,22 @@ __device__ __forceinline__ double recip_width(const SetView& s, int j, bool lg) 
   return lg ? 1.0 / (s.lr[j + 1] - s.lr[j]) : 1.0 / (s.r[j + 1] - s.r[j]);
 }
 
+// log(1 + u) for 0 <= u <= 1/64 by its Taylor series in Estrin form (shorter dependency chains
+// than Horner): 6 terms for u <= 2^-9, 12 terms up to 1/64 (truncation below 1e-17 relative).
+__device__ __forceinline__ double log1p_series6(double u) {
+  const double u2 = u * u;
+  const double e0 = fma(-0.5, u, 1.0), e1 = fma(-0.25, u, 1.0 / 3.0), e2 = fma(-1.0 / 6.0, u, 0.2);
+  return u * fma(fma(e2, u2, e1), u2, e0);
+}
+__device__ __forceinline__ double log1p_series12(double u) {
+  const double u2 = u * u, u4 = u2 * u2;
+  const double e0 = fma(-0.5, u, 1.0), e1 = fma(-0.25, u, 1.0 / 3.0), e2 = fma(-1.0 / 6.0, u, 0.2);
+  const double e3 = fma(-0.125, u, 1.0 / 7.0), e4 = fma(-0.1, u, 1.0 / 9.0), e5 = fma(-1.0 / 12.0, u, 1.0 / 11.0);
+  const double lo = fma(fma(e2, u2, e1), u2, e0);
+  const double hi = fma(fma(e5, u2, e4), u2, e3);
+  return u * fma(hi, u4 * u2, lo);
+}
+
 // One warp per CTA covers OWN_ROWS consecutive grid rows. Lane j owns grid interval
 // g = k0 - 2 + j: the CC nodes whose kernel-column interval (searchsorted left, clipped) is
 // il = g, i.e. x in (r_g, r_{g+1}] (g = 0: [r_0, r_1]). Each node is evaluated once, by its
@@ -109,6 +125,14 @@ __device__ __forceinline__ double recip_width(const SetView& s, int j, bool lg) 
 // sums them per target row in ascending node order, and row k adds the sums of lanes k-2,
 // k-1 and k in that order through warp shuffles. Lanes 0 and 1 are the halo of the first two
 // rows (their own rows are written by the previous CTA).
+//
+// Per node, a node strictly inside its interval (and inside r[:n1], with a log step below 1/64)
+// takes the fast path: both interpolations use interval g, so with t the (log-)interpolation
+// weight, wr the linear column weight and w the CC weight,
+//   T: row g += w(1-t)^2 (diagonal), w(1-t)t (upper); row g+1 += wt^2 (diagonal), wt(1-t) (lower)
+//   B: row g += (1-wr) w(1-t2), (1-wr) w t2 (taps 0, 1); row g+1 += wr w(1-t2), wr w t2 (taps -1, 0)
+// from the shared products w(1-t) and wt. Nodes on a grid point or outside those bounds take the
+// general path, which handles every case the reference's clipping and searchsorted produce.
 constexpr int OWN_ROWS = 30;
 #ifndef DWBA_NODESET_FILL
 #define DWBA_NODESET_FILL 32 // resident-CTA waves the launch aims for
@@ -116,11 +140,13 @@ constexpr int OWN_ROWS = 30;
 #ifndef DWBA_NODESET_MIN_BLOCKS
 #define DWBA_NODESET_MIN_BLOCKS 24
 #endif
+template <int NCC>  // CC nodes per interval known at compile time (0: n_cc at run time)
 __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets,
                                                               const double* __restrict__ ccx_g,
-                                                              const double* __restrict__ ccw_g, int n_cc,
+                                                              const double* __restrict__ ccw_g, int n_cc_rt,
                                                               int* status) {
   __shared__ double ccw[MAX_CC], ccx1[MAX_CC];
+  const int n_cc = NCC > 0 ? NCC : n_cc_rt;
   if (threadIdx.x < n_cc) {
     ccw[threadIdx.x] = ccw_g[threadIdx.x];
     ccx1[threadIdx.x] = rn_add(ccx_g[threadIdx.x], 1.0);
@@ -145,6 +171,7 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
   const double r_first = r[0], r_lim = r[n1 - 1], r_last = r[N - 1];
   // with n1 == N and one spacing test for both, the B taps of a node are its T taps
   const bool shared = s.log1 == s.log2 && n1 == N;
+  const bool any_log = s.log1 || s.log2;
 
   for (int k0 = blockIdx.x * OWN_ROWS; k0 < N; k0 += gridDim.x * OWN_ROWS) {
     const int g = k0 - 2 + lane;
@@ -157,20 +184,26 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
     if (g >= 0 && g <= n1 - 2) {
       const double rg = r[g], rg1 = r[g + 1];
       const double lo = g == 0 ? -1.0e308 : rg;  // exclusive lower end of the owned interval
-      bool first = true;
+      bool first = true, done = false, short6 = true;
       double iT0 = 0.0, iT1 = 0.0, iB0 = 0.0, iB1 = 0.0, iW = 0.0, lg = 0.0, lg1 = 0.0, irg = 0.0;
-      for (int m = interval_floor(s, rg); m < s.n_int; ++m) {
+      for (int m = interval_floor(s, rg); m < s.n_int && !done; ++m) {
         double a, b;
         interval(s, m, a, b);
         if (a > rg1) break;
         const double width = rn_sub(b, a);
         if (!(width > 1e-12)) continue;
         const double hw = rn_mul(0.5, width);
-        for (int sl = n_cc - 1; sl >= 0; --sl) {  // ascending positions within the interval
+#pragma unroll
+        for (int q = 0; q < (NCC > 0 ? NCC : MAX_CC); ++q) {  // ascending positions within the interval
+          if (NCC == 0 && q >= n_cc) break;
+          const int sl = n_cc - 1 - q;
           double x = rn_add(rn_mul(hw, ccx1[sl]), a);
           x = fmin(fmax(x, a), b);  // the top node can round one ulp past b
           if (!(x > lo)) continue;
-          if (x > rg1) break;
+          if (x > rg1) {
+            done = true;
+            break;
+          }
           if (first) {  // reciprocal widths of the intervals j in {g, g+1} a node of this owner uses
             iT0 = recip_width(s, g, s.log1);
             iT1 = recip_width(s, g + 1, s.log1);
@@ -180,16 +213,42 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
             lg = s.lr[g];
             lg1 = s.lr[g + 1];
             irg = 1.0 / rg;
+            short6 = (rg1 - rg) * irg <= 0.001953125;
             first = false;
           }
           const double w = rn_mul(ccw[sl], hw);
+          const double dx = x - rg;
+          const double u = dx * irg;
+          if (x < rg1 && x > r_first && x < r_lim && (shared || x < r_last) && (!any_log || u <= 0.015625)) {
+            // fast path: j1 = j2 = g
+            double dl = 0.0;
+            if (any_log) dl = short6 ? log1p_series6(u) : log1p_series12(u);
+            const double t = s.log1 ? dl * iT0 : dx * iT0;
+            const double omt = 1.0 - t;
+            double wo = w * omt, wt = w * t;
+            o_di = fma(wo, omt, o_di);
+            o_up = fma(wo, t, o_up);
+            x_di = fma(wt, t, x_di);
+            x_lo = fma(wt, omt, x_lo);
+            if (!shared) {
+              const double t2 = s.log2 ? dl * iB0 : dx * iB0;
+              wo = w * (1.0 - t2);
+              wt = w * t2;
+            }
+            const double q1 = dx * iW, q0 = 1.0 - q1;
+            o_b2 = fma(q0, wo, o_b2);
+            o_b3 = fma(q0, wt, o_b3);
+            x_b1 = fma(q1, wo, x_b1);
+            x_b2 = fma(q1, wt, x_b2);
+            continue;
+          }
+          // general path
           const bool at_top = x >= rg1;  // floor index in the full grid: g + 1 at r_{g+1}, else g
           // log x - log r_g: from the series of log(1 + (x - r_g)/r_g) when the grid step is small
           // (it then equals the difference of the two logs to a few ulps of that difference), else
           // as the difference; log x - log r_{g+1} only for a node exactly at r_{g+1}
           double dl = 0.0, dl_up = 0.0;
-          if (s.log1 || s.log2) {
-            const double u = (x - rg) * irg;
+          if (any_log) {
             dl = u <= 0.015625 ? log1p_small(u) : log(x) - lg;
             if (at_top) dl_up = log(x) - lg1;
           }
@@ -230,7 +289,7 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
               const double inv = up ? iB1 : iB0;
               t2 = s.log2 ? (up ? dl_up : dl) * inv : (x - (up ? rg1 : rg)) * inv;
             }
-            const double wr = (x - rg) * iW;
+            const double wr = dx * iW;
             const double q0 = 1.0 - wr, q1 = wr;
             if (j2 == g) {  // row g: taps 0, 1 (band 2, 3); row g+1: taps -1, 0 (band 1, 2)
               o_b2 += q0 * w * (1.0 - t2); o_b3 += q0 * w * t2;
@@ -281,7 +340,10 @@ extern "C" int dwba_build_nodesets(const dwba_nodeset_t* sets_dev, int n_sets, i
   const int need = (max_grid + OWN_ROWS - 1) / OWN_ROWS;
   const int fill = (int)(((int64_t)148 * 24 * DWBA_NODESET_FILL + n_sets - 1) / n_sets);
   dim3 grid(need < fill ? need : fill, n_sets);
-  nodeset_rows_kernel<<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc, status_dev);
+  if (n_cc == 5)
+    nodeset_rows_kernel<5><<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc, status_dev);
+  else
+    nodeset_rows_kernel<0><<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc, status_dev);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;
 }

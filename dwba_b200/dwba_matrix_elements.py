@@ -169,12 +169,18 @@ def _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f
         raise ValueError("bound_i and bound_f must have the same number of transitions")
     trans = [Transition(u_i=_fit(bi.u_of_r, N, "Bound state u_i"), u_f=_fit(bf.u_of_r, N, "u_f"),
                         excitation=is_excitation(bf)) for bi, bf in zip(bis, bfs)]
-    wp = []
-    cache_w: Dict[int, _WaveView] = {}
-    for ci, cf in pairs:
-        vi = cache_w.get(id(ci)) or cache_w.setdefault(id(ci), _WaveView(ci, N, "cont_i.chi"))
-        vf = cache_w.get(id(cf)) or cache_w.setdefault(id(cf), _WaveView(cf, N, "cont_f.chi"))
-        wp.append((vi, vf))
+    cache_w: Dict[int, object] = {}
+
+    def view(w, what):
+        # a wave whose chi is already N float64 values is used as it is; others get a truncated view
+        v = cache_w.get(id(w))
+        if v is None:
+            chi = getattr(w, "chi_of_r", None)
+            ok = (type(chi) is np.ndarray and chi.dtype == np.float64 and chi.ndim == 1 and len(chi) == N and
+                  hasattr(w, "l") and hasattr(w, "k_au"))
+            v = cache_w[id(w)] = w if ok else _WaveView(w, N, what)
+        return v
+    wp = [(view(ci, "cont_i.chi"), view(cf, "cont_f.chi")) for ci, cf in pairs]
     meth = kw.get("oscillatory_method", "advanced")
     if meth not in ("legacy", "advanced", "full_split"):
         meth = "advanced"  # the reference treats any other value as "advanced" (dwba_matrix_elements.py:1183)

@@ -212,17 +212,25 @@ class Job:
     tails_per_unit_moment: bool = False
 
 
+def _wave_scalars(w):
+    return (float(w.k_au), int(w.l), int(getattr(w, "idx_match", -1)), float(getattr(w, "eta", 0.0)),
+            float(getattr(w, "phase_shift", 0.0)), float(getattr(w, "sigma_l", 0.0)))
+
+
 def _pair_arrays(pairs):
-    def col(get):
-        return np.array([get(c) for c in pairs])
-    return dict(
-        k_i=col(lambda p: float(p[0].k_au)), k_f=col(lambda p: float(p[1].k_au)),
-        l_i=col(lambda p: int(p[0].l)), l_f=col(lambda p: int(p[1].l)),
-        im_i=col(lambda p: int(getattr(p[0], "idx_match", -1))), im_f=col(lambda p: int(getattr(p[1], "idx_match", -1))),
-        e_i=col(lambda p: float(getattr(p[0], "eta", 0.0))), e_f=col(lambda p: float(getattr(p[1], "eta", 0.0))),
-        d_i=col(lambda p: float(getattr(p[0], "phase_shift", 0.0))),
-        d_f=col(lambda p: float(getattr(p[1], "phase_shift", 0.0))),
-        s_i=col(lambda p: float(getattr(p[0], "sigma_l", 0.0))), s_f=col(lambda p: float(getattr(p[1], "sigma_l", 0.0))))
+    """Scalar metadata of every pair's two waves as arrays (each distinct wave read once)."""
+    memo: Dict[int, tuple] = {}
+
+    def sc(w):
+        v = memo.get(id(w))
+        if v is None:
+            v = memo[id(w)] = _wave_scalars(w)
+        return v
+    a = np.array([sc(ci) + sc(cf) for ci, cf in pairs], dtype=np.float64).reshape(len(pairs), 12)
+    out = dict(k_i=a[:, 0], l_i=a[:, 1].astype(np.int64), im_i=a[:, 2].astype(np.int64), e_i=a[:, 3], d_i=a[:, 4],
+               s_i=a[:, 5], k_f=a[:, 6], l_f=a[:, 7].astype(np.int64), im_f=a[:, 8].astype(np.int64), e_f=a[:, 9],
+               d_f=a[:, 10], s_f=a[:, 11])
+    return {k: np.ascontiguousarray(v) for k, v in out.items()}
 
 
 def _idx_limits(job: Job, pa, t: Transition) -> np.ndarray:
@@ -566,6 +574,112 @@ def expand_multi(multi: np.ndarray) -> np.ndarray:
     return out
 
 
+@dataclass
+class DirectPlan:
+    """How the exact engines evaluate the forms of one prepared job (indices into its forms).
+
+    A direct form whose column operand is its transition's full-grid b = w u_f u_i (the Filon
+    direct term and the no-interval branch) is a dot product of the pair's folded density with
+    the transition's multipole potential phi_L = K_L b, the reference's inner integral int_r2
+    (oscillatory_integrals.py:2571), which every pair of the transition shares. ``pot_b``: device
+    address of each transition's b (0 when no form of it takes this path); ``dot_fo`` / ``dot_t``:
+    those forms and their transitions; ``ss_fo``: the forms left to the semiseparable kernel."""
+    pot_b: np.ndarray
+    dot_fo: np.ndarray
+    dot_t: np.ndarray
+    ss_fo: np.ndarray
+
+
+class FormLaunch:
+    """Device descriptors of the exact forms of one or several prepared jobs: one multipole potential
+    per transition with Filon direct forms, the dot forms against them (runs of ``DOT_RUN`` sharing a
+    potential, padded with empty descriptors) and the remaining forms as semiseparable forms, whose
+    results go to a compact buffer scattered into the result rows. ``entries``: per job
+    (forms_host, plan, N, r_ptr, dot_rows, ss_rows) with dot_rows / ss_rows the result rows (of
+    ``out``) of plan.dot_fo / plan.ss_fo."""
+
+    def __init__(self, entries, out: torch.Tensor, nl: int, dev):
+        self.out, self.nl = out, nl
+        row = np.uint64(8 * nl)
+        out_p = np.uint64(_ptr(out))
+        phi_len = [int(np.count_nonzero(pl.pot_b)) * nl * N for _, pl, N, _, _, _ in entries]
+        self.phi = torch.empty(max(1, sum(phi_len)), dtype=torch.float64, device=dev)
+        base = np.uint64(_ptr(self.phi))
+        pots, dots, ss_forms, ss_rows = [], [], [], []
+        off = 0
+        for (fh, pl, N, r_ptr, dot_rows, ss_out), ln in zip(entries, phi_len):
+            used = np.nonzero(pl.pot_b)[0]
+            phi_t = np.zeros(len(pl.pot_b), dtype=np.uint64)
+            phi_t[used] = base + np.uint64(8) * (np.uint64(off) + np.uint64(nl * N) * np.arange(len(used), dtype=np.uint64))
+            off += ln
+            p = np.zeros(len(used), dtype=_lib.POTENTIAL_DTYPE)
+            p["r"], p["b"], p["phi"] = r_ptr, pl.pot_b[used], phi_t[used]
+            p["n_rows"] = p["n_cols"] = p["stride"] = N
+            pots.append(p)
+            if len(pl.dot_fo):
+                # group by transition, each group padded to whole runs of DOT_RUN
+                order = np.argsort(pl.dot_t, kind="stable")
+                t_s = pl.dot_t[order]
+                cnt = np.bincount(t_s, minlength=len(pl.pot_b))
+                padded = (cnt + _lib.DOT_RUN - 1) // _lib.DOT_RUN * _lib.DOT_RUN
+                start = np.concatenate([[0], np.cumsum(padded)[:-1]])
+                first = np.concatenate([[0], np.cumsum(cnt)[:-1]])
+                pos = start[t_s] + (np.arange(len(t_s)) - first[t_s])
+                d = np.zeros(int(padded.sum()), dtype=_lib.DOT_DTYPE)
+                fo = pl.dot_fo[order]
+                d["a"][pos] = fh["a"][fo]
+                d["phi"][pos] = phi_t[t_s]
+                d["out"][pos] = out_p + row * np.asarray(dot_rows, dtype=np.uint64)[order]
+                d["n_rows"][pos] = fh["n_rows"][fo]
+                d["stride"] = N
+                dots.append(d)
+            if len(pl.ss_fo):
+                ss_forms.append(fh[pl.ss_fo])
+                ss_rows.append(np.asarray(ss_out, dtype=np.int64))
+        pots = np.concatenate(pots) if pots else np.zeros(0, dtype=_lib.POTENTIAL_DTYPE)
+        dots = np.concatenate(dots) if dots else np.zeros(0, dtype=_lib.DOT_DTYPE)
+        self.n_pots, self.n_dots = len(pots), len(dots)
+        self.pots_d = _dev(pots.view(np.uint8), dev) if len(pots) else None
+        self.dots_d = _dev(dots.view(np.uint8), dev) if len(dots) else None
+        self.n_ss = int(sum(len(f) for f in ss_forms))
+        if self.n_ss:
+            self.ss_forms_host = np.concatenate(ss_forms)
+            self.ss_forms_d = _dev(self.ss_forms_host.view(np.uint8), dev)
+            self.ss_rows_d = _dev(np.concatenate(ss_rows), dev)
+            self.out_ss = torch.empty((self.n_ss, nl), dtype=torch.float64, device=dev)
+        self.pots_host, self.dots_host = pots, dots
+
+    def launch(self, lib, L_max: int, ds: np.ndarray, r_min: float, r_max: float) -> None:
+        st = _stream()
+        if self.n_pots:
+            _lib.check(lib.dwba_multipole_potentials(_ptr(self.pots_d), self.n_pots, L_max, ds.ctypes.data, r_min, r_max,
+                                                     st), "dwba_multipole_potentials")
+        if self.n_dots:
+            _lib.check(lib.dwba_dot_forms(_ptr(self.dots_d), self.n_dots, L_max, st), "dwba_dot_forms")
+        if self.n_ss:
+            _lib.check(lib.dwba_bilinear_semisep_fp64(_ptr(self.ss_forms_d), self.n_ss, L_max, ds.ctypes.data, r_min,
+                                                      r_max, _ptr(self.out_ss), st), "dwba_bilinear_semisep_fp64")
+            self.out.index_copy_(0, self.ss_rows_d, self.out_ss)
+
+    def algorithmic_bytes(self) -> float:
+        """Operand bytes: each potential reads b and r and writes (L_max+1) rows; each dot form reads a
+        (the potential's tiles are read once per run); each semiseparable form reads a, b and r."""
+        b = 0.0
+        if self.n_pots:
+            p = self.pots_host
+            b += float(np.sum(8.0 * (2.0 * p["n_cols"] + self.nl * p["n_rows"].astype(np.float64))))
+        if self.n_dots:
+            d = self.dots_host
+            b += float(np.sum(8.0 * d["n_rows"].astype(np.float64)))
+            runs = d[::_lib.DOT_RUN]
+            b += float(np.sum(8.0 * self.nl * runs["stride"].astype(np.float64)))
+        if self.n_ss:
+            f = self.ss_forms_host
+            m = np.maximum(f["n_rows"], f["n_cols"]).astype(np.float64)
+            b += float(np.sum(8.0 * (f["n_rows"].astype(np.float64) + f["n_cols"] + m)))
+        return b
+
+
 class PreparedJob:
     """A job planned on the host with its inputs and descriptors resident on the device.
 
@@ -738,12 +852,26 @@ class PreparedJob:
             self.tails_d = _dev(self.tail_records(_ptr(self.out), self.n_forms).view(np.uint8), dev)
         self.ds = diag_scale(job.L_max)
         self.forms_host = forms
+        # the direct forms on a transition's full-grid b go through its multipole potential
+        b_full_p = Op + row * (np.uint64(SL * T * P) + np.arange(T, dtype=np.uint64))
+        d_rows = np.arange(0, 2 * T * P, 2, dtype=np.int64)
+        d_t = d_rows // (2 * P)
+        via_pot = (forms["b"][d_rows] == b_full_p[d_t]) & (forms["n_cols"][d_rows] == N) & (forms["n_rows"][d_rows] > 0)
+        pot_b = np.where(np.bincount(d_t[via_pot], minlength=T) > 0, b_full_p, np.uint64(0))
+        tc = engine in TC_TERMS
+        ss_fo = d_rows[~via_pot] if tc else np.sort(np.concatenate([d_rows[~via_pot], d_rows + 1]))
+        self.direct_plan = DirectPlan(pot_b=pot_b, dot_fo=d_rows[via_pot], dot_t=d_t[via_pot], ss_fo=ss_fo)
+        if engine == "semisep":
+            dp = self.direct_plan
+            self.form_launch = FormLaunch([(forms, dp, N, _ptr(dg.r), dp.dot_fo, dp.ss_fo)], self.out, nl, dev)
         if engine in TC_TERMS:
-            # direct forms share b per transition: exact FP64 O(N L); exchange forms: tensor cores
-            self.forms_dir_d = _dev(np.ascontiguousarray(forms[0::2]).view(np.uint8), dev)
+            # direct forms: potentials and dot products, the rest exact O(N L); exchange forms: tensor cores
             self.forms_ex_d = _dev(np.ascontiguousarray(forms[1::2]).view(np.uint8), dev)
             self.out_dir = torch.empty((T * P, nl), dtype=torch.float64, device=dev)
             self.out_ex = torch.empty((T * P, nl), dtype=torch.float64, device=dev)
+            dp = self.direct_plan
+            self.form_launch = FormLaunch([(forms, dp, N, _ptr(dg.r), dp.dot_fo // 2, dp.ss_fo // 2)], self.out_dir,
+                                          nl, dev)
             ws = int(lib.dwba_tc_workspace_bytes(T * P, N, job.L_max, TC_TERMS[engine]))
             if ws < 0:
                 raise ValueError("invalid tensor-core form sizes")
@@ -801,11 +929,10 @@ class PreparedJob:
                                            self.job.grid.N, _stream()), "dwba_fold_multi")
 
     def launch_forms_direct(self) -> None:
-        """Tensor-core engines: the direct forms share b per transition and use the exact FP64 O(N L) form."""
-        job, g = self.job, self.job.grid
-        _lib.check(self.lib.dwba_bilinear_semisep_fp64(_ptr(self.forms_dir_d), self.T * self.P, job.L_max,
-                                                       self.ds.ctypes.data, float(g.r[0]), float(g.r[-1]),
-                                                       _ptr(self.out_dir), _stream()), "dwba_bilinear_semisep_fp64")
+        """Tensor-core engines: the direct forms share b per transition and take the exact FP64 path
+        (multipole potentials and dot products; semiseparable forms for the rest)."""
+        g = self.job.grid
+        self.form_launch.launch(self.lib, self.job.L_max, self.ds, float(g.r[0]), float(g.r[-1]))
 
     def launch_forms_exchange(self) -> None:
         """Tensor-core engines: exchange forms on tcgen05 (split bf16 K_L B, FP64 epilogue)."""
@@ -840,10 +967,7 @@ class PreparedJob:
                                                     self.partial.numel(), _ptr(self.out), _stream()),
                        "dwba_bilinear_dense_fp64")
         else:
-            _lib.check(lib.dwba_bilinear_semisep_fp64(_ptr(self.forms_d), self.n_forms, job.L_max,
-                                                      self.ds.ctypes.data, float(job.grid.r[0]),
-                                                      float(job.grid.r[-1]), _ptr(self.out), _stream()),
-                       "dwba_bilinear_semisep_fp64")
+            self.form_launch.launch(lib, job.L_max, self.ds, float(job.grid.r[0]), float(job.grid.r[-1]))
 
     def launch(self) -> None:
         self.nodesets.launch()
@@ -884,7 +1008,11 @@ class PreparedJob:
         return 8.0 * (sum(reads.values()) + writes)
 
     def algorithmic_bytes(self) -> float:
-        """Operand bytes of the semiseparable evaluation: a, b and r read once per form."""
+        """Operand bytes of the exact evaluation: potentials (b and r read, rows written), dot forms
+        (a read once, each potential tile once per run) and semiseparable forms (a, b and r)."""
+        fl = getattr(self, "form_launch", None)
+        if fl is not None and self.engine == "semisep":
+            return fl.algorithmic_bytes()
         f = self.forms_host
         m = np.maximum(f["n_rows"], f["n_cols"]).astype(np.float64)
         return float(np.sum(8.0 * (f["n_rows"].astype(np.float64) + f["n_cols"] + m)))
@@ -970,7 +1098,12 @@ class MultiPrepared:
             self.prefix_d = _dev(prefix, dev)
             self.partial = torch.empty(self.n_cta * self.nl, dtype=torch.float64, device=dev)
         self.graph = None
-        # tensor-core engines: the direct forms of every job in one semiseparable launch (each
+        if self.engine == "semisep":
+            # one potential launch, one dot-form launch and one semiseparable launch for all jobs
+            ent = [(p.forms_host, p.direct_plan, p.job.grid.N, _ptr(p.dg.r), self.offsets[k] + p.direct_plan.dot_fo,
+                    self.offsets[k] + p.direct_plan.ss_fo) for k, p in enumerate(parts)]
+            self.form_launch = FormLaunch(ent, self.out, self.nl, dev)
+        # tensor-core engines: the direct forms of every job in one exact launch sequence (each
         # descriptor names its own grid); the exchange forms of all jobs on equal grids (e.g. the
         # transitions of one energy) in one tensor-core launch, so that their forms share the
         # 256-wide form tiles; those launches and the jobs' tails go round-robin (largest grid
@@ -984,10 +1117,12 @@ class MultiPrepared:
             nt = TC_TERMS[self.engine]
             self.side_streams = [torch.cuda.Stream(device=dev) for _ in range(min(4, len(parts)))]
             self.tc_order = sorted(range(len(parts)), key=lambda k: -parts[k].job.grid.N)
-            fd = np.concatenate([np.ascontiguousarray(p.forms_host[0::2]) for p in parts])
-            self.tc_n_dir = len(fd)
-            self.tc_dir_d = _dev(fd.view(np.uint8), dev)
-            self.tc_out_dir = torch.empty((len(fd), self.nl), dtype=torch.float64, device=dev)
+            n_dir = int(sum(p.T * p.P for p in parts))
+            self.tc_out_dir = torch.empty((n_dir, self.nl), dtype=torch.float64, device=dev)
+            d_off = np.cumsum([0] + [p.T * p.P for p in parts])
+            ent = [(p.forms_host, p.direct_plan, p.job.grid.N, _ptr(p.dg.r), d_off[k] + p.direct_plan.dot_fo // 2,
+                    d_off[k] + p.direct_plan.ss_fo // 2) for k, p in enumerate(parts)]
+            self.form_launch = FormLaunch(ent, self.tc_out_dir, self.nl, dev)
             by_grid: Dict[tuple, List[int]] = {}
             off = 0
             for k, p in enumerate(parts):
@@ -1050,9 +1185,7 @@ class MultiPrepared:
                                                     self.partial.numel(), _ptr(self.out), st),
                        "dwba_bilinear_dense_fp64")
         elif self.engine == "semisep":
-            _lib.check(lib.dwba_bilinear_semisep_fp64(_ptr(self.forms_d), self.n_forms, self.L_max, self.ds.ctypes.data,
-                                                      self.r_min, self.r_max, _ptr(self.out), st),
-                       "dwba_bilinear_semisep_fp64")
+            self.form_launch.launch(lib, self.L_max, self.ds, self.r_min, self.r_max)
         else:
             main = torch.cuda.current_stream()
             nt = TC_TERMS[self.engine]
@@ -1061,10 +1194,7 @@ class MultiPrepared:
                     sd.wait_stream(main)
                 if stage == "forms":
                     # direct forms on the main stream, beside the tensor-core groups
-                    _lib.check(lib.dwba_bilinear_semisep_fp64(_ptr(self.tc_dir_d), self.tc_n_dir, self.L_max,
-                                                              self.ds.ctypes.data, self.r_min, self.r_max,
-                                                              _ptr(self.tc_out_dir), st),
-                               "dwba_bilinear_semisep_fp64")
+                    self.form_launch.launch(lib, self.L_max, self.ds, self.r_min, self.r_max)
                     for q, g in enumerate(self.tc_groups):
                         sd = self.side_streams[q % len(self.side_streams)]
                         _lib.check(lib.dwba_bilinear_tc_bf16(_ptr(g["forms"]), g["n"], _ptr(g["r"]), g["N"], self.L_max,

@@ -23,7 +23,7 @@ import torch
 
 from .autograd import RadialIntegrals
 
-__all__ = ["CrossSection", "fit_to_cross_section"]
+__all__ = ["CrossSection", "CouplingCrossSection", "fit_to_cross_section"]
 
 
 class CrossSection:
@@ -47,6 +47,31 @@ class CrossSection:
         g = torch.einsum("mkplt,pkl->mt", self.G, Ic)
         d = 0.25 * (f + g).abs() ** 2 + 0.75 * (f - g).abs() ** 2
         return torch.clamp(self.pref * d.sum(0), min=0.0)
+
+    def tcs(self, I: torch.Tensor) -> torch.Tensor:
+        return 2.0 * np.pi * torch.trapezoid(torch.sin(self.theta) * self.dcs(I), self.theta)
+
+
+class CouplingCrossSection:
+    """DCS/TCS as torch functions of the integrals I (P, 2, L_max+1) with the angular coupling of
+    ``coupling.CouplingTables`` (the reference's ``calculate_amplitude_contribution``,
+    dwba_coupling.py:285-634, and ``dcs_dwba`` / ``integrate_dcs_over_angles``, sigma_total.py:147-217):
+    the same values as ``CouplingTables.dcs`` / ``.tcs``, differentiable in I."""
+
+    def __init__(self, tables, device="cuda"):
+        t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=device)  # noqa: E731
+        self.cf, self.cg, self.yd, self.ye = t(tables.cf), t(tables.cg), t(tables.yd), t(tables.ye)
+        self.theta = t(tables.theta)
+        self.pref = float(tables.pref)
+
+    def dcs(self, I: torch.Tensor) -> torch.Tensor:
+        Ic = I.to(torch.complex128)
+        sd = torch.einsum("apl,pl->ap", self.cf, Ic[:, 0])
+        se = torch.einsum("apl,pl->ap", self.cg, Ic[:, 1])
+        f = torch.einsum("ap,apt->at", sd, self.yd.to(torch.complex128))
+        g = torch.einsum("ap,apt->at", se, self.ye.to(torch.complex128))
+        d = self.pref * (0.25 * (f + g).abs() ** 2 + 0.75 * (f - g).abs() ** 2)
+        return torch.clamp(d.sum(0), min=0.0)
 
     def tcs(self, I: torch.Tensor) -> torch.Tensor:
         return 2.0 * np.pi * torch.trapezoid(torch.sin(self.theta) * self.dcs(I), self.theta)

@@ -9,8 +9,7 @@ from __future__ import annotations
 
 import math
 import os
-from dataclasses import dataclass
-from typing import Optional, Tuple
+from typing import NamedTuple, Optional, Tuple
 
 import numpy as np
 
@@ -156,8 +155,8 @@ def adaptive_dphi(g: GridInfo, n1: int, k_total: float, requested: float, eta_to
     return float(min(max(d_eff, PI_16), PI_4))
 
 
-@dataclass(frozen=True)
-class NodeSetKey:
+class NodeSetKey(NamedTuple):
+    """Everything a node set's operators depend on (a tuple: cheap to build and hash per set)."""
     grid_id: int
     n1: int
     k_total: float
@@ -166,8 +165,7 @@ class NodeSetKey:
     n_cc: int
 
 
-@dataclass
-class NodeSetPlan:
+class NodeSetPlan(NamedTuple):
     key: NodeSetKey
     n_breaks: int
     breaks: Optional[np.ndarray]  # None => linspace on the device

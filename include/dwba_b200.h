@@ -135,6 +135,42 @@ typedef struct {
   int32_t n_cols;
 } dwba_form_t;
 
+/* Multipole potentials of column operands (all multipoles at once):
+ *   phi[L*stride + p] = sum_{q<n_cols} K_L(r_p, r_q) b_q ,   p < n_rows, L = 0..L_max,
+ * the inner integral int_r2 = K[:n1, :N] (rho2 w) of the reference's Filon direct term
+ * (oscillatory_integrals.py:2571; dwba_matrix_elements.py:1126-1206 calls it per L), which depends
+ * on the bound states only and is shared by every pair of a transition. Exact O(N L) FP64 with
+ * forward prefix and backward suffix sums; the same range rule as dwba_bilinear_semisep_fp64. */
+typedef struct {
+  const double* r_dev;  /* grid radii (>= max(n_rows, n_cols)) */
+  const double* b_dev;  /* column operand (n_cols values) */
+  double* phi_dev;      /* out: (L_max+1) rows of `stride` doubles; p < n_rows written */
+  int32_t n_rows;
+  int32_t n_cols;
+  int32_t stride;       /* >= n_rows */
+  int32_t pad;
+} dwba_potential_t;
+
+int dwba_multipole_potentials(const dwba_potential_t* pots_dev, int n, int L_max, const double* diag_scale_host,
+                              double r_min_all, double r_max_all, dwba_stream_t stream);
+
+/* Dot forms: out[L] = sum_{i<n_rows} a[i] phi[L*stride + i], L = 0..L_max: the outer CC sum of
+ * the Filon direct term (oscillatory_integrals.py:2609-2644, folded into a) against a potential
+ * of dwba_multipole_potentials. Each run of 16 consecutive descriptors (descriptors 16k..16k+15)
+ * must share phi_dev and stride: the kernel stages the potential's tiles in shared memory once
+ * for the run. Pad a run with empty descriptors (n_rows = 0, out_dev = NULL); the first
+ * descriptor of a run must not be empty unless the whole run is, and phi must hold at least the
+ * largest n_rows of its run. */
+typedef struct {
+  const double* a_dev;
+  const double* phi_dev;
+  double* out_dev;      /* L_max+1 values (NULL: empty descriptor) */
+  int32_t n_rows;
+  int32_t stride;
+} dwba_dot_t;
+
+int dwba_dot_forms(const dwba_dot_t* dots_dev, int n, int L_max, dwba_stream_t stream);
+
 /* Dense plain form: every K_L element is generated in registers (never stored),
  * operands are staged in shared memory, partial sums are reduced with warp
  * shuffles. Work is split into chunks (CTAs); dwba_dense_chunk_prefix fills
@@ -295,8 +331,8 @@ int dwba_abi_version(void);
 const char* dwba_status_string(int status);
 int dwba_device_probe(int* n_devices, int* cc_major, int* cc_minor);
 /* sizeof(dwba_nodeset_t), sizeof(dwba_fold_t), sizeof(dwba_form_t), sizeof(dwba_tail_t),
- * sizeof(dwba_form_grad_t), sizeof(dwba_fold_adj_t), sizeof(dwba_fold_multi_t) into
- * sizes[0..6] (the first n of them). */
+ * sizeof(dwba_form_grad_t), sizeof(dwba_fold_adj_t), sizeof(dwba_fold_multi_t),
+ * sizeof(dwba_potential_t), sizeof(dwba_dot_t) into sizes[0..8] (the first n of them). */
 int dwba_struct_sizes(int64_t* sizes, int n);
 
 #ifdef __cplusplus

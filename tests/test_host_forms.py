@@ -1,0 +1,129 @@
+"""Host logic of the exact engine's form launches, checked on the CPU.
+
+A prepared job is built on the CPU device (descriptors only, no kernel runs), its operand rows are
+filled with random values, and the launch sequence of the exact FP64 engine is emulated from the
+descriptors (multipole potentials, dot forms in padded runs, the remaining semiseparable forms and
+their scatter into the result rows). Every result row must equal the bilinear form a^T K_L b that
+the job's form descriptor names, evaluated by the oracle's semiseparable restatement. This pins the
+pointer and row bookkeeping of dwba_multipole_potentials / dwba_dot_forms without a GPU.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+import bench
+from dwba_b200 import _lib
+from oracle.folded import semiseparable_eval
+
+
+def _view(ptr, n):
+    return np.ctypeslib.as_array((ctypes.c_double * int(n)).from_address(int(ptr)))
+
+
+def _potential_model(r, b, n_cols, L_max):
+    """phi_L = K_L b (dense restatement of K_L on the grid, diagonal clamp included)."""
+    bb = np.zeros(len(r))
+    bb[:n_cols] = b[:n_cols]
+    rl = np.minimum(r[:, None], r[None, :])
+    rg = np.maximum(r[:, None], r[None, :])
+    lr = np.log(np.minimum(rl / rg, 1.0 - 1e-12) + 1e-300)
+    return np.stack([(1.0 / rg) * np.exp(L * lr) @ bb for L in range(L_max + 1)])
+
+
+def _job(engine):
+    from dwba_b200.dwba_matrix_elements import GPUCache, _make_job
+    from dwba_b200.engine import DeviceGrid, PreparedJob
+    from dwba_b200.plan import GridInfo
+    g, z, bounds, pairs = bench.make_workload(N=301, n_cont=9, n_bound=3, seed_shift=5)
+    r = g.r
+    # two low-k pairs (k_i + k_f <= 0.5): the standard Simpson branch, whose direct forms keep a
+    # truncated b and stay semiseparable forms
+    for l1, l2 in ((0, 1), (2, 3)):
+        w = [bench._Wave(l, 0.2, 0.3, np.sin(0.2 * r + 0.3) * (1 - np.exp(-(r * 0.2 / (l + 1)) ** (l + 1))))
+             for l in (l1, l2)]
+        pairs.append(tuple(w))
+
+    class Cache:  # the host side of GPUCache, on the CPU device
+        info = GridInfo(g.r, g.w_simpson, g.w_trapz)
+        dg = DeviceGrid(info, torch.device("cpu"))
+    job = _make_job(g, z, z, [b[0] for b in bounds], [b[1] for b in bounds], pairs, 5, z, {}, Cache)
+    return PreparedJob(job, Cache.dg, engine), r
+
+
+def _emulate(fl, L_max, r):
+    nl = L_max + 1
+    for p in fl.pots_host:
+        phi = _potential_model(r, _view(p["b"], p["n_cols"]), int(p["n_cols"]), L_max)
+        dst = _view(p["phi"], nl * int(p["stride"])).reshape(nl, int(p["stride"]))
+        dst[:, :p["n_rows"]] = phi[:, :p["n_rows"]]
+    runs = fl.dots_host.reshape(-1, _lib.DOT_RUN)
+    for run in runs:
+        assert run[0]["n_rows"] > 0 or np.all(run["n_rows"] == 0)  # a run starts with a real form
+        for d in run:
+            if d["n_rows"] == 0:
+                assert d["out"] == 0
+                continue
+            assert d["phi"] == run[0]["phi"] and d["stride"] == run[0]["stride"]
+            n = int(d["n_rows"])
+            phi = _view(d["phi"], nl * int(d["stride"])).reshape(nl, int(d["stride"]))
+            _view(d["out"], nl)[:] = phi[:, :n] @ _view(d["a"], n)
+    if fl.n_ss:
+        rows = fl.ss_rows_d.numpy()
+        out = fl.out.numpy()
+        for f, row in zip(fl.ss_forms_host, rows):
+            a = np.zeros(len(r))
+            b = np.zeros(len(r))
+            a[:f["n_rows"]] = _view(f["a"], f["n_rows"])
+            b[:f["n_cols"]] = _view(f["b"], f["n_cols"])
+            out[row] = semiseparable_eval(r, a, b, L_max)
+
+
+def _check(pj, out_rows_of_form, out, r):
+    L_max = pj.job.L_max
+    fh = pj.forms_host
+    for k, f in enumerate(fh):
+        a = np.zeros(len(r))
+        b = np.zeros(len(r))
+        a[:f["n_rows"]] = _view(f["a"], f["n_rows"])
+        b[:f["n_cols"]] = _view(f["b"], f["n_cols"])
+        want = semiseparable_eval(r, a, b, L_max)
+        scale = semiseparable_eval(r, np.abs(a), np.abs(b), L_max)
+        got = out[out_rows_of_form(k)]
+        assert np.all(np.abs(got - want) <= 1e-13 * scale + 1e-300), (k, got, want)
+
+
+def test_semisep_engine_form_launch():
+    pj, r = _job("semisep")
+    rng = np.random.default_rng(3)
+    pj.ops.copy_(torch.from_numpy(rng.normal(size=tuple(pj.ops.shape))))
+    pj.out.fill_(np.nan)
+    dp = pj.direct_plan
+    assert len(dp.dot_fo) > 0 and np.all(dp.dot_fo % 2 == 0)
+    assert np.any(dp.ss_fo % 2 == 0)  # the standard-branch direct forms stay semiseparable
+    assert np.count_nonzero(dp.pot_b) == pj.T
+    assert len(dp.dot_fo) + len(dp.ss_fo) == pj.n_forms
+    _emulate(pj.form_launch, pj.job.L_max, r)
+    _check(pj, lambda k: k, pj.out.numpy(), r)
+
+
+def test_tensor_core_engine_direct_launch():
+    """The direct forms of the split-BF16 engines take the same exact path into out_dir."""
+    pj, r = _job("tc_bf16x3")
+    rng = np.random.default_rng(4)
+    pj.ops.copy_(torch.from_numpy(rng.normal(size=tuple(pj.ops.shape))))
+    pj.out_dir.fill_(np.nan)
+    dp = pj.direct_plan
+    assert np.all(dp.ss_fo % 2 == 0) and len(dp.dot_fo) + len(dp.ss_fo) == pj.T * pj.P
+    _emulate(pj.form_launch, pj.job.L_max, r)
+    out = pj.out_dir.numpy()
+    L_max = pj.job.L_max
+    for k in range(0, pj.n_forms, 2):
+        f = pj.forms_host[k]
+        a = np.zeros(len(r))
+        b = np.zeros(len(r))
+        a[:f["n_rows"]] = _view(f["a"], f["n_rows"])
+        b[:f["n_cols"]] = _view(f["b"], f["n_cols"])
+        want = semiseparable_eval(r, a, b, L_max)
+        scale = semiseparable_eval(r, np.abs(a), np.abs(b), L_max)
+        assert np.all(np.abs(out[k // 2] - want) <= 1e-13 * scale + 1e-300), k

@@ -67,6 +67,7 @@ def _declare(lib):
         "dwba_dense_chunk_prefix": (c_i64, [c_vp, c_int, c_vp]),
         "dwba_bilinear_dense_fp64": (c_int, [c_vp, c_int, c_int, c_vp, c_vp, c_i64, c_vp, c_i64, c_vp, c_vp]),
         "dwba_bilinear_semisep_fp64": (c_int, [c_vp, c_int, c_int, c_vp, c_dbl, c_dbl, c_vp, c_vp]),
+        "dwba_bilinear_semisep_abs_fp64": (c_int, [c_vp, c_int, c_int, c_vp, c_dbl, c_dbl, c_vp, c_vp]),
         "dwba_bilinear_dense_fp64_noalloc": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp]),
         "dwba_tc_workspace_bytes": (c_i64, [c_int, c_int, c_int, c_int]),
         "dwba_bilinear_tc_bf16": (c_int, [c_vp, c_int, c_vp, c_int, c_int, c_int, c_vp, c_vp, c_i64, c_vp, c_vp,

@@ -36,7 +36,8 @@ __device__ __forceinline__ double ipow(double x, int e) {
 // and with the exclusive prefixes A0, B0 of TA, TB over the segments before it,
 //   I_L = sum_s [LOC_s + A0_s SY_s + B0_s SX_s] + sum_p X_p Y_p d_L / r_p.
 // The prefixes over segments come from warp shuffles and a per-warp table in shared memory.
-template <int NL>
+// ABS = true evaluates |a|^T K_L |b| (the cancellation scale S_L of the form) instead.
+template <int NL, bool ABS = false>
 __global__ void __launch_bounds__(THREADS, 4)
 semisep_kernel(const dwba_form_t* __restrict__ forms, int L0, int n_ltot, DiagScale ds, double* __restrict__ out) {
   constexpr int NW = THREADS / 32;
@@ -55,8 +56,8 @@ semisep_kernel(const dwba_form_t* __restrict__ forms, int L0, int n_ltot, DiagSc
   double dsum = 0.0;
   // the operands of point p+1 are loaded while point p is accumulated (one point of lead hides
   // the load latency of the thread's strided walk; 128 registers keep four CTAs per SM)
-  auto ldx = [&](int p) { return p < F.n_rows ? __ldg(F.a_dev + p) : 0.0; };
-  auto ldy = [&](int p) { return p < F.n_cols ? __ldg(F.b_dev + p) : 0.0; };
+  auto ldx = [&](int p) { return p < F.n_rows ? (ABS ? fabs(__ldg(F.a_dev + p)) : __ldg(F.a_dev + p)) : 0.0; };
+  auto ldy = [&](int p) { return p < F.n_cols ? (ABS ? fabs(__ldg(F.b_dev + p)) : __ldg(F.b_dev + p)) : 0.0; };
   double Xn = p0 < p1 ? ldx(p0) : 0.0, Yn = p0 < p1 ? ldy(p0) : 0.0, rn = p0 < p1 ? __ldg(F.r_dev + p0) : 1.0;
   for (int p = p0; p < p1; ++p) {
     const double X = Xn, Y = Yn, r = rn;
@@ -126,19 +127,20 @@ semisep_kernel(const dwba_form_t* __restrict__ forms, int L0, int n_ltot, DiagSc
   }
 }
 
-template <int NL>
+template <int NL, bool ABS>
 int launch(const dwba_form_t* forms, int n_forms, int L0, int n_ltot, const DiagScale& ds, double* out,
            cudaStream_t st) {
-  semisep_kernel<NL><<<n_forms, THREADS, 0, st>>>(forms, L0, n_ltot, ds, out);
+  semisep_kernel<NL, ABS><<<n_forms, THREADS, 0, st>>>(forms, L0, n_ltot, ds, out);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;
 }
 
+template <bool ABS>
 int launch_nl(int nl, const dwba_form_t* forms, int n_forms, int L0, int n_ltot, const DiagScale& ds, double* out,
               cudaStream_t st) {
   switch (nl) {
 #define DWBA_CASE(N) \
-  case N: return launch<N>(forms, n_forms, L0, n_ltot, ds, out, st);
+  case N: return launch<N, ABS>(forms, n_forms, L0, n_ltot, ds, out, st);
     DWBA_CASE(1) DWBA_CASE(2) DWBA_CASE(3) DWBA_CASE(4) DWBA_CASE(5) DWBA_CASE(6) DWBA_CASE(7) DWBA_CASE(8)
     DWBA_CASE(9)
 #undef DWBA_CASE
@@ -148,9 +150,9 @@ int launch_nl(int nl, const dwba_form_t* forms, int n_forms, int L0, int n_ltot,
 
 }  // namespace
 
-extern "C" int dwba_bilinear_semisep_fp64(const dwba_form_t* forms_dev, int n_forms, int L_max,
-                                          const double* diag_scale_host, double r_min_all, double r_max_all,
-                                          double* out_dev, dwba_stream_t stream) {
+template <bool ABS>
+static int semisep_entry(const dwba_form_t* forms_dev, int n_forms, int L_max, const double* diag_scale_host,
+                  double r_min_all, double r_max_all, double* out_dev, dwba_stream_t stream) {
   if (n_forms <= 0) return DWBA_OK;
   if (!forms_dev || !diag_scale_host || !out_dev || L_max < 0 || L_max > DWBA_MAX_L || !(r_min_all > 0.0) ||
       !(r_max_all >= r_min_all) || n_forms > 0x7fffffff)
@@ -164,8 +166,20 @@ extern "C" int dwba_bilinear_semisep_fp64(const dwba_form_t* forms_dev, int n_fo
   const int n_ltot = L_max + 1;
   for (int L0 = 0; L0 < n_ltot; L0 += NL_MAX) {
     const int nl = (n_ltot - L0) < NL_MAX ? (n_ltot - L0) : NL_MAX;
-    int rc = launch_nl(nl, forms_dev, n_forms, L0, n_ltot, ds, out_dev, (cudaStream_t)stream);
+    int rc = launch_nl<ABS>(nl, forms_dev, n_forms, L0, n_ltot, ds, out_dev, (cudaStream_t)stream);
     if (rc != DWBA_OK) return rc;
   }
   return DWBA_OK;
+}
+
+extern "C" int dwba_bilinear_semisep_fp64(const dwba_form_t* forms_dev, int n_forms, int L_max,
+                                          const double* diag_scale_host, double r_min_all, double r_max_all,
+                                          double* out_dev, dwba_stream_t stream) {
+  return semisep_entry<false>(forms_dev, n_forms, L_max, diag_scale_host, r_min_all, r_max_all, out_dev, stream);
+}
+
+extern "C" int dwba_bilinear_semisep_abs_fp64(const dwba_form_t* forms_dev, int n_forms, int L_max,
+                                              const double* diag_scale_host, double r_min_all, double r_max_all,
+                                              double* out_dev, dwba_stream_t stream) {
+  return semisep_entry<true>(forms_dev, n_forms, L_max, diag_scale_host, r_min_all, r_max_all, out_dev, stream);
 }

@@ -26,6 +26,57 @@ ENGINES = ("dense", "semisep", "tc_bf16x3", "tc_bf16x6")
 TC_TERMS = {"tc_bf16x3": 2, "tc_bf16x6": 3}
 
 
+def tc_route_ratio() -> float:
+    """Cancellation bound of the split-BF16 engines: an exchange form whose scale S_L = |a|^T K_L |b|
+    exceeds this multiple of |I_L| at any L is recomputed in FP64 (DWBA_B200_TC_ROUTE; <= 0 disables)."""
+    import os
+    try:
+        return float(os.environ.get("DWBA_B200_TC_ROUTE", "8"))
+    except ValueError:
+        return 8.0
+
+
+class TCGuard:
+    """Accuracy guard of the split-BF16 exchange forms of one launch (FP32 accumulation of K_L b).
+
+    After the tensor-core pass: the exact scale S_L of every form (semiseparable pass on |a|, |b|),
+    a flag for the forms with S_L > R |I_L| at some L (their FP32 rounding, about 1e-7 S_L, is then
+    not small against I_L), the flagged forms recomputed by the exact FP64 form (the others masked to
+    empty forms, which cost nothing) and merged into the result. Device-side only, no host sync, so
+    it is captured in CUDA graphs with the rest of the launch sequence."""
+
+    def __init__(self, forms_host: np.ndarray, forms_d: torch.Tensor, n: int, nl: int, dev, ratio: float):
+        self.n, self.ratio = n, ratio
+        self.forms_d = forms_d
+        self.desc32 = forms_d.view(torch.int32).view(n, _lib.FORM_DTYPE.itemsize // 4)
+        self.masked = torch.empty_like(forms_d)
+        self.masked32 = self.masked.view(torch.int32).view(n, _lib.FORM_DTYPE.itemsize // 4)
+        self.scale = torch.empty((n, nl), dtype=torch.float64, device=dev)
+        self.exact = torch.empty((n, nl), dtype=torch.float64, device=dev)
+        self.over = torch.empty((n, nl), dtype=torch.bool, device=dev)
+        self.flag = torch.zeros(n, dtype=torch.bool, device=dev)
+        self.rows = _lib.FORM_DTYPE.fields["n_rows"][1] // 4  # int32 column of n_rows (n_cols follows)
+
+    def launch(self, lib, L_max: int, ds: np.ndarray, r_min: float, r_max: float, out: torch.Tensor) -> None:
+        if self.ratio <= 0 or self.n == 0:
+            return
+        st = _stream()
+        _lib.check(lib.dwba_bilinear_semisep_abs_fp64(_ptr(self.forms_d), self.n, L_max, ds.ctypes.data, r_min, r_max,
+                                                      _ptr(self.scale), st), "dwba_bilinear_semisep_abs_fp64")
+        torch.gt(self.scale, self.ratio * out.abs(), out=self.over)
+        torch.any(self.over, dim=1, out=self.flag)
+        self.masked.copy_(self.forms_d)
+        keep = self.flag.to(torch.int32)
+        c = self.rows
+        self.masked32[:, c:c + 2] = self.desc32[:, c:c + 2] * keep[:, None]
+        _lib.check(lib.dwba_bilinear_semisep_fp64(_ptr(self.masked), self.n, L_max, ds.ctypes.data, r_min, r_max,
+                                                  _ptr(self.exact), st), "dwba_bilinear_semisep_fp64")
+        out.copy_(torch.where(self.flag[:, None], self.exact, out))
+
+    def n_routed(self) -> int:
+        return int(self.flag.sum().item()) if self.ratio > 0 else 0
+
+
 def _ptr(t: Optional[torch.Tensor]) -> int:
     return 0 if t is None else int(t.data_ptr())
 
@@ -869,6 +920,7 @@ class PreparedJob:
             self.forms_ex_d = _dev(np.ascontiguousarray(forms[1::2]).view(np.uint8), dev)
             self.out_dir = torch.empty((T * P, nl), dtype=torch.float64, device=dev)
             self.out_ex = torch.empty((T * P, nl), dtype=torch.float64, device=dev)
+            self.tc_guard = TCGuard(forms[1::2], self.forms_ex_d, T * P, nl, dev, tc_route_ratio())
             dp = self.direct_plan
             self.form_launch = FormLaunch([(forms, dp, N, _ptr(dg.r), dp.dot_fo // 2, dp.ss_fo // 2)], self.out_dir,
                                           nl, dev)
@@ -935,12 +987,14 @@ class PreparedJob:
         self.form_launch.launch(self.lib, self.job.L_max, self.ds, float(g.r[0]), float(g.r[-1]))
 
     def launch_forms_exchange(self) -> None:
-        """Tensor-core engines: exchange forms on tcgen05 (split bf16 K_L B, FP64 epilogue)."""
+        """Tensor-core engines: exchange forms on tcgen05 (split bf16 K_L B, FP64 epilogue), then the
+        accuracy guard (forms with strong cancellation recomputed in FP64)."""
         job, g = self.job, self.job.grid
         _lib.check(self.lib.dwba_bilinear_tc_bf16(_ptr(self.forms_ex_d), self.T * self.P, _ptr(self.dg.r), g.N,
                                                   job.L_max, TC_TERMS[self.engine], self.ds.ctypes.data,
                                                   _ptr(self.tc_ws), self.tc_ws.numel(), _ptr(self.tc_status),
                                                   _ptr(self.out_ex), _stream()), "dwba_bilinear_tc_bf16")
+        self.tc_guard.launch(self.lib, job.L_max, self.ds, float(g.r[0]), float(g.r[-1]), self.out_ex)
 
     def tensor_flops(self) -> Tuple[float, float]:
         """(dense-equivalent, executed) tensor flops of the exchange forms per launch."""
@@ -1140,7 +1194,9 @@ class MultiPrepared:
                 grp = {"forms": _dev(fe.view(np.uint8), dev), "n": len(fe), "N": N, "r": parts[ks[0]].dg.r,
                        "ws": torch.empty(max(ws, 256), dtype=torch.uint8, device=dev),
                        "status": torch.zeros(1, dtype=torch.int32, device=dev),
-                       "out": torch.empty((len(fe), self.nl), dtype=torch.float64, device=dev)}
+                       "out": torch.empty((len(fe), self.nl), dtype=torch.float64, device=dev),
+                       "r_lo": float(parts[ks[0]].job.grid.r[0]), "r_hi": float(parts[ks[0]].job.grid.r[-1])}
+                grp["guard"] = TCGuard(fe, grp["forms"], len(fe), self.nl, dev, tc_route_ratio())
                 off = 0
                 for k in ks:
                     p = parts[k]
@@ -1201,6 +1257,8 @@ class MultiPrepared:
                                                              nt, self.ds.ctypes.data, _ptr(g["ws"]), g["ws"].numel(),
                                                              _ptr(g["status"]), _ptr(g["out"]), int(sd.cuda_stream)),
                                    "dwba_bilinear_tc_bf16")
+                        with torch.cuda.stream(sd):
+                            g["guard"].launch(lib, self.L_max, self.ds, g["r_lo"], g["r_hi"], g["out"])
                 else:
                     for q, k in enumerate(self.tc_order):
                         with torch.cuda.stream(self.side_streams[q % len(self.side_streams)]):

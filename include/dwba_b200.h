@@ -209,6 +209,15 @@ int dwba_bilinear_semisep_fp64(const dwba_form_t* forms_dev, int n_forms, int L_
                                const double* diag_scale_host, double r_min_all, double r_max_all,
                                double* out_dev, dwba_stream_t stream);
 
+/* The cancellation scale of each form, S_L = sum_i sum_j |a_i| K_L(r_i, r_j) |b_j| (the same kernel on
+ * |a| and |b|), which bounds the rounding error of any evaluation of the form: |dI_L| <= c S_L. No
+ * reference counterpart; the split-BF16 engines use it to route forms whose cancellation exceeds
+ * their FP32 accumulation to the FP64 form. Same arguments and range rule as
+ * dwba_bilinear_semisep_fp64. */
+int dwba_bilinear_semisep_abs_fp64(const dwba_form_t* forms_dev, int n_forms, int L_max,
+                                   const double* diag_scale_host, double r_min_all, double r_max_all,
+                                   double* out_dev, dwba_stream_t stream);
+
 /* Split-BF16 tensor-core form (tcgen05.mma, TMEM accumulators, TMA-loaded operands):
  * for every form of one grid, I_L = sum_i a_i (K_L B)_i with K_L generated on the fly and
  * split into n_terms bf16 terms (2: hi+lo, three products; 3: hi+mid+lo, six products),

@@ -127,3 +127,59 @@ def test_tensor_core_engine_direct_launch():
         want = semiseparable_eval(r, a, b, L_max)
         scale = semiseparable_eval(r, np.abs(a), np.abs(b), L_max)
         assert np.all(np.abs(out[k // 2] - want) <= 1e-13 * scale + 1e-300), k
+
+
+class _EmulatedLib:
+    """The two semiseparable entry points of the guard, evaluated from their descriptors on the CPU."""
+
+    def __init__(self, r):
+        self.r = r
+
+    def _run(self, forms_ptr, n, L_max, out_ptr, absolute):
+        nl = L_max + 1
+        f = np.ctypeslib.as_array((ctypes.c_uint8 * (n * _lib.FORM_DTYPE.itemsize)).from_address(forms_ptr))
+        f = f.view(_lib.FORM_DTYPE)
+        out = _view(out_ptr, n * nl).reshape(n, nl)
+        for k, d in enumerate(f):
+            a = np.zeros(len(self.r))
+            b = np.zeros(len(self.r))
+            if d["n_rows"]:
+                a[:d["n_rows"]] = _view(d["a"], d["n_rows"])
+            if d["n_cols"]:
+                b[:d["n_cols"]] = _view(d["b"], d["n_cols"])
+            if absolute:
+                a, b = np.abs(a), np.abs(b)
+            out[k] = semiseparable_eval(self.r, a, b, L_max)
+        return 0
+
+    def dwba_bilinear_semisep_abs_fp64(self, forms, n, L_max, ds, r0, r1, out, st):
+        return self._run(forms, n, L_max, out, True)
+
+    def dwba_bilinear_semisep_fp64(self, forms, n, L_max, ds, r0, r1, out, st):
+        return self._run(forms, n, L_max, out, False)
+
+
+def test_tensor_core_guard_routes_cancelling_forms(monkeypatch):
+    """The guard recomputes exactly the exchange forms whose scale S_L exceeds R |I_L| at some L and
+    leaves the others as the tensor cores gave them."""
+    from dwba_b200 import engine
+    monkeypatch.setattr(engine, "_stream", lambda: 0)  # no CUDA stream on the CPU
+    pj, r = _job("tc_bf16x3")
+    rng = np.random.default_rng(6)
+    pj.ops.copy_(torch.from_numpy(rng.normal(size=tuple(pj.ops.shape))))
+    g = pj.tc_guard
+    n, nl = pj.T * pj.P, pj.nl
+    # stand-in tensor-core results: the exact values with a relative error of 1e-3
+    lib = _EmulatedLib(r)
+    exact = torch.zeros((n, nl), dtype=torch.float64)
+    lib.dwba_bilinear_semisep_fp64(g.forms_d.data_ptr(), n, pj.job.L_max, None, 0, 0, exact.data_ptr(), None)
+    out = exact * (1.0 + 1e-3)
+    before = out.clone()
+    scale = torch.zeros((n, nl), dtype=torch.float64)
+    lib.dwba_bilinear_semisep_abs_fp64(g.forms_d.data_ptr(), n, pj.job.L_max, None, 0, 0, scale.data_ptr(), None)
+    g.ratio = float(torch.median((scale / before.abs()).max(1).values))  # about half the forms cancel more
+    g.launch(lib, pj.job.L_max, pj.ds, float(r[0]), float(r[-1]), out)
+    want = (scale > g.ratio * before.abs()).any(1)
+    assert torch.equal(g.flag, want) and 0 < int(want.sum()) < n
+    assert torch.equal(out[want], exact[want]) and torch.equal(out[~want], before[~want])
+    assert torch.equal(g.forms_d, pj.forms_ex_d)  # the descriptors themselves are untouched

@@ -13,7 +13,7 @@ from __future__ import annotations
 import ctypes
 from dataclasses import dataclass, field
 import hashlib
-from typing import Dict, List, Optional, Sequence, Tuple
+from typing import Dict, List, NamedTuple, Optional, Sequence, Tuple
 
 import numpy as np
 import torch
@@ -104,8 +104,7 @@ class DeviceGrid:
         return sum(ns.nbytes for ns in self.nodesets.values()) + 3 * 8 * self.info.N
 
 
-@dataclass
-class DeviceNodeSet:
+class DeviceNodeSet(NamedTuple):
     """Operators of one node set: device addresses inside ``block`` (which keeps them alive)."""
     plan: NodeSetPlan
     block: torch.Tensor
@@ -147,15 +146,23 @@ class NodeSetBatch:
         self.dg, self.n_cc = dg, n_cc
         dev = dg.device
         N = dg.info.N
-        todo = list(plans) if rebuild else [p for p in plans if p.key not in dg.nodesets]
+        cache = dg.nodesets
+        plans = list(plans)
+        cached = [cache.get(p.key) for p in plans]
+        todo = plans if rebuild else [p for p, c in zip(plans, cached) if c is None]
         self.n = len(todo)
+        # operator addresses of every planned set, in the plans' order (and a 0 for "no set")
+        self.ta_all = np.zeros(len(plans) + 1, dtype=np.uint64)
+        self.bx_all = np.zeros(len(plans) + 1, dtype=np.uint64)
         if not todo:
+            self.ta_all[:-1] = [c.ta_ptr for c in cached]
+            self.bx_all[:-1] = [c.bx_ptr for c in cached]
             return
         self.ccx, self.ccw = CCTables.get(n_cc, dev)
         n = len(todo)
         self.keep = []
         # operators of the sets not cached yet: one allocation for the batch, addresses by offset
-        fresh_mask = np.array([p.key not in dg.nodesets for p in todo], dtype=bool)
+        fresh_mask = np.array([c is None for c in cached], dtype=bool) if rebuild else np.ones(n, dtype=bool)
         n1s = np.array([p.key.n1 for p in todo], dtype=np.int64)
         sizes = np.where(fresh_mask, 3 * n1s + 5 * N, 0)
         offs = np.concatenate([[0], np.cumsum(sizes)[:-1]])
@@ -176,13 +183,22 @@ class NodeSetBatch:
             br_off = np.concatenate([[0], np.cumsum(br_len)[:-1]])
             has = br_len > 0
             br_p[has] = np.uint64(_ptr(br_all)) + np.uint64(8) * br_off[has].astype(np.uint64)
+        nb = (8 * (3 * n1s + 5 * N)).tolist()
+        ta_l, bx_l = ta_p.tolist(), bx_p.tolist()
         for i, p in enumerate(todo):
             if fresh_mask[i]:
-                dg.nodesets[p.key] = DeviceNodeSet(p, block, int(ta_p[i]), int(bx_p[i]),
-                                                   8 * (3 * p.key.n1 + 5 * N))
-            else:
-                old = dg.nodesets[p.key]
-                ta_p[i], bx_p[i] = old.ta_ptr, old.bx_ptr
+                cache[p.key] = DeviceNodeSet(p, block, ta_l[i], bx_l[i], nb[i])
+        if rebuild and not fresh_mask.all():
+            old = [i for i in range(n) if not fresh_mask[i]]
+            ta_p[old] = [cached[i].ta_ptr for i in old]
+            bx_p[old] = [cached[i].bx_ptr for i in old]
+        if rebuild:
+            self.ta_all[:-1], self.bx_all[:-1] = ta_p, bx_p
+        else:
+            done = {id(p): i for i, p in enumerate(todo)}
+            for j, (p, c) in enumerate(zip(plans, cached)):
+                k = done.get(id(p))
+                self.ta_all[j], self.bx_all[j] = (ta_p[k], bx_p[k]) if k is not None else (c.ta_ptr, c.bx_ptr)
         recs = np.zeros(n, dtype=_lib.NODESET_DTYPE)
         recs["r"], recs["logr"] = _ptr(dg.r), _ptr(dg.logr)
         recs["breaks"], recs["ta"], recs["bx"] = br_p, ta_p, bx_p
@@ -350,32 +366,19 @@ class WaveMatrix:
 
     def __init__(self, N):
         self.N = N
-        self.idx: Dict[Tuple[int, int], int] = {}
         self.arrays: List[np.ndarray] = []
-        self.ptrs: List[int] = []
         self._uploaded: Dict[str, Tuple[int, torch.Tensor]] = {}
         self._by_id: Dict[int, int] = {}
         self._keep: List[object] = []
 
     def add(self, arr: np.ndarray) -> int:
+        """Row of ``arr`` (one row per distinct array object; the object is kept alive with it)."""
         i = self._by_id.get(id(arr))
-        if i is not None:
-            return i
-        i = self._add(arr)
-        self._by_id[id(arr)] = i
-        self._keep.append(arr)  # keeps id(arr) from being reused while the memo holds it
-        return i
-
-    def _add(self, arr: np.ndarray) -> int:
-        a = np.asarray(arr)
-        ptr = a.__array_interface__["data"][0]
-        key = (ptr, a.strides[0] if a.ndim else 0)
-        i = self.idx.get(key)
         if i is None:
-            i = len(self.arrays)
-            self.idx[key] = i
-            self.arrays.append(a[: self.N])
-            self.ptrs.append(ptr)
+            i = self._by_id[id(arr)] = len(self.arrays)
+            a = arr if type(arr) is np.ndarray else np.asarray(arr)
+            self.arrays.append(a if len(a) == self.N else a[: self.N])
+            self._keep.append(arr)  # keeps id(arr) from being reused while the memo holds it
         return i
 
     def matrix(self) -> np.ndarray:
@@ -415,8 +418,9 @@ class WaveMatrix:
         done = np.zeros(n, dtype=bool)
         groups: Dict[int, list] = {}
         base_ptrs: Dict[int, int] = {}
+        ptrs = [a.__array_interface__["data"][0] for a in self.arrays]
         for i, a in enumerate(self.arrays):
-            rb = self._row_of(a, N, self.ptrs[i], base_ptrs)
+            rb = self._row_of(a, N, ptrs[i], base_ptrs)
             if rb is not None:
                 groups.setdefault(id(rb[0]), [rb[0], [], []])
                 groups[id(rb[0])][1].append(i)
@@ -787,9 +791,7 @@ class PreparedJob:
                 wl_cache[n1] = t_
             return t_.data_ptr()
 
-        dns = [dg.nodesets[ns.key] for ns in plans.nodesets]
-        ta_ptr = np.array([d_.ta_ptr for d_ in dns] + [0], dtype=np.uint64)
-        bx_ptr = np.array([d_.bx_ptr for d_ in dns] + [0], dtype=np.uint64)
+        ta_ptr, bx_ptr = self.nodesets.ta_all, self.nodesets.bx_all
         w_ptr, r_ptr = np.uint64(_ptr(dg.w)), np.uint64(_ptr(dg.r))
         fold_parts, forms = [], np.zeros(2 * T * P, dtype=_lib.FORM_DTYPE)
         pidx = np.arange(P, dtype=np.int64)

@@ -8,6 +8,24 @@ from __future__ import annotations
 import numpy as np
 
 
+def cc_table_rule(n: int):
+    """The module-level table formula (``oscillatory_integrals.py:120-145``, and the CuPy path's
+    ``_init_gpu_cc_weights``, ``dwba_matrix_elements.py:1316-1347``, for every n): nodes cos(pi j/(n-1))
+    from +1 to -1, weights (2/(n-1)) (1 - 2 sum_j cos(2 j theta)/(4 j^2 - 1)), the last term halved
+    for odd n."""
+    theta = np.pi * np.arange(n) / (n - 1)
+    x = np.cos(theta)
+    jm = (n - 1) // 2
+    if jm > 0:
+        jv = np.arange(1, jm + 1)
+        sums = np.sum(np.cos(2 * jv[:, None] * theta[None, :]) / (4 * jv ** 2 - 1)[:, None], axis=0)
+        if (n - 1) % 2 == 0:
+            sums += 0.5 * np.cos(2 * jm * theta) / (4 * jm ** 2 - 1)
+    else:
+        sums = np.zeros(n)
+    return x, (2.0 / (n - 1)) * (1 - 2 * sums)
+
+
 def cc_reference(n: int):
     """Clenshaw-Curtis nodes/weights on [-1, 1] as ``_get_cc_ref`` (``:159-171``) returns them.
 
@@ -19,14 +37,7 @@ def cc_reference(n: int):
     if n < 2:
         raise ValueError("Clenshaw-Curtis requires n >= 2.")
     if n == 5:
-        theta = np.pi * np.arange(n) / (n - 1)
-        x = np.cos(theta)
-        jm = (n - 1) // 2
-        jv = np.arange(1, jm + 1)
-        sums = np.sum(np.cos(2 * jv[:, None] * theta[None, :]) / (4 * jv ** 2 - 1)[:, None], axis=0)
-        if (n - 1) % 2 == 0:
-            sums += 0.5 * np.cos(2 * jm * theta) / (4 * jm ** 2 - 1)
-        return x, (2.0 / (n - 1)) * (1 - 2 * sums)
+        return cc_table_rule(n)
     return clenshaw_curtis_nodes(n, -1.0, 1.0)
 
 

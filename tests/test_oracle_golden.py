@@ -132,3 +132,21 @@ def test_oracle_config1_sample():
         Ie[0] += fp["corr_ex"]
         for I, R in ((Id, z["I_dir"][p]), (Ie, z["I_exc"][p])):
             assert np.all(np.abs(I - R) <= 1e-12 * np.abs(R) + 1e-13 * np.max(np.abs(R))), (li, lf, I, R)
+
+
+CUPY = np.load(gc.GOLDEN_DIR + "/cupy_semantics.npz")
+
+
+@pytest.mark.parametrize("call", [c for c in gc.all_calls() if not c["label"].startswith("large_grid")],
+                         ids=[c["label"] for c in gc.all_calls() if not c["label"].startswith("large_grid")])
+def test_cupy_path_restatement_matches_reference_gpu_path(call):
+    """The oracle's restatement of the reference's CuPy path (oracle/cupy_path.py) against that path's
+    own outputs, recorded on the CPU through a NumPy stand-in for CuPy (tests/golden/make_cupy_golden.py)."""
+    from oracle.cupy_path import radial_me_all_L_cupy
+    name, idx = call["label"].rstrip("]").split("[")
+    d, e = radial_me_all_L_cupy(*call["args"], **call["kwargs"])
+    L = call["L_max"]
+    for got, key in ((d, f"{name}_{idx}_dir"), (e, f"{name}_{idx}_exc")):
+        ref = CUPY[key]
+        g = np.array([got[l] for l in range(L + 1)])
+        assert np.all(np.abs(g - ref) <= 1e-12 * np.abs(ref) + 1e-14 * np.max(np.abs(ref))), (key, g, ref)

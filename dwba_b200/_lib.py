@@ -40,6 +40,10 @@ POTENTIAL_DTYPE = np.dtype([("r", "<u8"), ("b", "<u8"), ("phi", "<u8"), ("n_rows
                             ("stride", "<i4"), ("pad", "<i4")])
 DOT_DTYPE = np.dtype([("a", "<u8"), ("phi", "<u8"), ("out", "<u8"), ("n_rows", "<i4"), ("stride", "<i4")])
 DOT_RUN = 16  # descriptors per run sharing one potential (dwba_dot_forms)
+CUPY_SET_DTYPE = np.dtype([("r", "<u8"), ("logr", "<u8"), ("ops", "<u8"), ("n1", "<i4"), ("n_breaks", "<i4"),
+                           ("L_max", "<i4"), ("pad", "<i4")])
+CUPY_FORM_DTYPE = np.dtype([("r", "<u8"), ("a", "<u8"), ("f", "<u8"), ("g", "<u8"), ("ops", "<u8"), ("out", "<u8"),
+                            ("n1", "<i4"), ("L_max", "<i4")])
 TAIL_DTYPE = np.dtype([("wave", "<f8", (10,)), ("r_m", "<f8"), ("r_max", "<f8"), ("moments", "<u8"), ("out", "<u8"),
                        ("mode", "<i4"), ("pad", "<i4")])
 
@@ -88,6 +92,8 @@ def _declare(lib):
         "dwba_tc_set_wait_cycles": (c_int, [c_i64]),
         "dwba_multipole_potentials": (c_int, [c_vp, c_int, c_int, c_vp, c_dbl, c_dbl, c_vp]),
         "dwba_dot_forms": (c_int, [c_vp, c_int, c_int, c_vp]),
+        "dwba_cupy_exchange_ops": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_int, c_vp]),
+        "dwba_cupy_exchange_forms": (c_int, [c_vp, c_int, c_int, c_dbl, c_dbl, c_vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -107,11 +113,11 @@ def load():
     lib = _declare(ctypes.CDLL(LIB_PATH))
     if lib.dwba_abi_version() != 1:
         raise ImportError("libdwba_b200.so ABI version mismatch")
-    sizes = (ctypes.c_int64 * 9)()
-    lib.dwba_struct_sizes(sizes, 9)
+    sizes = (ctypes.c_int64 * 11)()
+    lib.dwba_struct_sizes(sizes, 11)
     want = (NODESET_DTYPE.itemsize, FOLD_DTYPE.itemsize, FORM_DTYPE.itemsize, TAIL_DTYPE.itemsize,
             FORM_GRAD_DTYPE.itemsize, FOLD_ADJ_DTYPE.itemsize, FOLD_MULTI_DTYPE.itemsize,
-            POTENTIAL_DTYPE.itemsize, DOT_DTYPE.itemsize)
+            POTENTIAL_DTYPE.itemsize, DOT_DTYPE.itemsize, CUPY_SET_DTYPE.itemsize, CUPY_FORM_DTYPE.itemsize)
     if tuple(sizes) != want:
         raise ImportError(f"struct layout mismatch: library {tuple(sizes)} vs binding {want}")
     _lib = lib

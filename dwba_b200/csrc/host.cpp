@@ -462,6 +462,8 @@ extern "C" int dwba_struct_sizes(int64_t* sizes, int n) {
   if (n >= 7) sizes[6] = (int64_t)sizeof(dwba_fold_multi_t);
   if (n >= 8) sizes[7] = (int64_t)sizeof(dwba_potential_t);
   if (n >= 9) sizes[8] = (int64_t)sizeof(dwba_dot_t);
+  if (n >= 10) sizes[9] = (int64_t)sizeof(dwba_cupy_set_t);
+  if (n >= 11) sizes[10] = (int64_t)sizeof(dwba_cupy_form_t);
   return DWBA_OK;
 }
 

@@ -13,7 +13,9 @@ Both entry points evaluate the reference's CPU quadrature semantics on the
 GPU (sm_100a kernels behind ``libdwba_b200.so``); there is no CPU fallback, so
 without a usable GPU they raise ``RuntimeError`` like the reference's GPU path
 does without CuPy. ``radial_ME_all_L_batch`` is the added batched entry point:
-all (l_i, l_f) pairs of one energy point in one set of launches.
+all (l_i, l_f) pairs of one energy point in one set of launches. The GPU and
+batched entry points take ``semantics="cupy"`` for the quadrature of the
+reference's CuPy function instead (``cupy_mode.py``).
 
 Engine selection: ``DWBA_B200_ENGINE`` = ``dense`` (default; the plain FP64
 form that generates every kernel element) or ``semisep`` (exact FP64 O(N L)
@@ -31,6 +33,7 @@ import numpy as np
 from . import _lib
 
 OscillatoryMethod = Literal["legacy", "advanced", "full_split"]
+SEMANTICS = ("cpu", "cupy")
 
 try:
     _lib.load()
@@ -237,9 +240,12 @@ def _results(I_dir: np.ndarray, I_exc: np.ndarray):
 
 @_no_gc
 def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, gpu_cache, engine,
-         as_arrays: bool = False):
+         as_arrays: bool = False, semantics: str = "cpu"):
     """Evaluate a job; returns results[t][p] (a list of RadialDWBAIntegrals per transition), or
-    the (T, P, L_max+1) arrays (I_dir, I_exc) with ``as_arrays``."""
+    the (T, P, L_max+1) arrays (I_dir, I_exc) with ``as_arrays``. ``semantics``: "cpu" for the
+    quadrature of the reference's CPU path, "cupy" for that of its CuPy path (cupy_mode.py)."""
+    if semantics not in SEMANTICS:
+        raise ValueError(f"unknown semantics {semantics!r}; choose from {SEMANTICS}")
     if not HAS_CUPY:
         raise RuntimeError("dwba_b200 engine library is not available (build it with python -m dwba_b200.build)")
     import torch
@@ -251,6 +257,12 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
     job = _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, cache)
     eng = _engine_name(engine)
     with torch.cuda.device(cache.device):
+        if semantics == "cupy":
+            from .cupy_mode import CupyPreparedJob
+            pj = CupyPreparedJob(job, cache.dg)
+            pj.launch()
+            I_dir, I_exc = pj.collect()
+            return (I_dir, I_exc) if as_arrays else _results(I_dir, I_exc)
         plans = plan_job(job, _early_upload(job, cache.device))
         if tune.is_auto(eng):
             cands = tune.candidates(eng)
@@ -286,15 +298,22 @@ def radial_ME_all_L_gpu(grid, V_core_array, U_i_array, bound_i, bound_f, cont_i,
                         CC_nodes: int = 5, phase_increment: float = 1.5708, gpu_block_size=0,
                         min_grid_fraction: float = 0.10, k_threshold: float = 0.5, gpu_memory_mode: str = "auto",
                         gpu_memory_threshold: float = 0.8, gpu_cache: Optional[GPUCache] = None,
-                        U_f_array: Optional[np.ndarray] = None, engine: Optional[str] = None) -> RadialDWBAIntegrals:
+                        U_f_array: Optional[np.ndarray] = None, engine: Optional[str] = None,
+                        semantics: str = "cpu") -> RadialDWBAIntegrals:
     """GPU signature of the reference (``dwba_matrix_elements.py:1563``). ``gpu_block_size``,
     ``gpu_memory_mode`` and ``gpu_memory_threshold`` are accepted for compatibility: kernel tiles are
-    generated in registers, so device memory is O(N) per pair and no block-size policy is needed."""
+    generated in registers, so device memory is O(N) per pair and no block-size policy is needed.
+
+    ``semantics="cpu"`` (default) gives the values of the reference's CPU path ``radial_ME_all_L``,
+    which its drivers use as ground truth; ``semantics="cupy"`` reproduces the quadrature of the
+    reference's own GPU function (un-adapted phase step, linear interpolation on r[:idx_limit],
+    kernel at the CC nodes, ungated L=0 corrections), evaluated exactly in FP64 (``engine`` is
+    ignored there)."""
     kw = dict(use_oscillatory_quadrature=use_oscillatory_quadrature, oscillatory_method=oscillatory_method,
               CC_nodes=CC_nodes, phase_increment=phase_increment, min_grid_fraction=min_grid_fraction,
               k_threshold=k_threshold)
     return _run(grid, V_core_array, U_i_array, bound_i, bound_f, [(cont_i, cont_f)], L_max, U_f_array, kw,
-                gpu_cache, engine)[0][0]
+                gpu_cache, engine, semantics=semantics)[0][0]
 
 
 def radial_ME_all_L_batch(grid, V_core_array, U_i_array, bound_i, bound_f,
@@ -303,7 +322,7 @@ def radial_ME_all_L_batch(grid, V_core_array, U_i_array, bound_i, bound_f,
                           CC_nodes: int = 5, phase_increment: float = 1.5708, min_grid_fraction: float = 0.10,
                           k_threshold: float = 0.5, U_f_array: Optional[np.ndarray] = None,
                           gpu_cache: Optional[GPUCache] = None,
-                          engine: Optional[str] = None, as_arrays: bool = False):
+                          engine: Optional[str] = None, as_arrays: bool = False, semantics: str = "cpu"):
     """Batched entry point (new): the same values as calling ``radial_ME_all_L`` per pair.
 
     All pairs share one grid and the potentials. With single ``bound_i``/``bound_f`` objects the
@@ -311,7 +330,7 @@ def radial_ME_all_L_batch(grid, V_core_array, U_i_array, bound_i, bound_f,
     transitions, e.g. one per ejected wave in ionization) it is a list per transition. With
     ``as_arrays=True`` the same values come as two float64 arrays (I_direct, I_exchange) of shape
     (P, L_max+1), or (T, P, L_max+1) for several transitions, without building a result object
-    per pair."""
+    per pair. ``semantics`` as for ``radial_ME_all_L_gpu``."""
     kw = dict(use_oscillatory_quadrature=use_oscillatory_quadrature, oscillatory_method=oscillatory_method,
               CC_nodes=CC_nodes, phase_increment=phase_increment, min_grid_fraction=min_grid_fraction,
               k_threshold=k_threshold)
@@ -322,7 +341,7 @@ def radial_ME_all_L_batch(grid, V_core_array, U_i_array, bound_i, bound_f,
             return np.zeros(shape), np.zeros(shape)
         return [[] for _ in bound_i] if multi else []
     res = _run(grid, V_core_array, U_i_array, bound_i, bound_f, list(pairs), L_max, U_f_array, kw, gpu_cache, engine,
-               as_arrays=as_arrays)
+               as_arrays=as_arrays, semantics=semantics)
     if as_arrays:
         return res if multi else (res[0][0], res[1][0])
     return res if multi else res[0]

@@ -300,8 +300,10 @@ def _pair_arrays(pairs):
     return {k: np.ascontiguousarray(v) for k, v in out.items()}
 
 
-def _idx_limits(job: Job, pa, t: Transition) -> np.ndarray:
-    """Vectorised ``idx_limit`` (dwba_matrix_elements.py:909-1022) for every pair of one transition."""
+def _idx_limits(job: Job, pa, t: Transition, cupy: bool = False) -> np.ndarray:
+    """Vectorised ``idx_limit`` (dwba_matrix_elements.py:909-1022) for every pair of one transition.
+    ``cupy``: the CuPy path's rule (``:1676-1720``, ``_refine_idx_limit_physics`` :688-777), which counts the
+    final state's extent only for a bound final state."""
     g = job.grid
     N, r = g.N, g.r
     n1 = np.full(len(pa["k_i"]), N, dtype=np.int64)
@@ -318,8 +320,8 @@ def _idx_limits(job: Job, pa, t: Transition) -> np.ndarray:
     mgf = int(N * job.min_grid_fraction)
     min_idx = np.where(k_eff > 1e-3, np.minimum(np.maximum(idx_turn + 20, mgf), N), max(1, mgf))
     n1 = np.where(n1 < min_idx, min_idx, n1)
-    idx99 = max(0, g.extent99(t.u_i), g.extent99(t.u_f))
-    n1 = np.where(idx99 > n1, idx99 + 1, n1)
+    idx99 = max(0, g.extent99(t.u_i), g.extent99(t.u_f) if (t.excitation or not cupy) else 0)
+    n1 = np.where(idx99 > n1, min(N, idx99 + 1), n1)
     ke = 0.5 * kmin ** 2
     uabs = np.abs(job.U_i) if job.U_f is None else np.maximum(np.abs(job.U_i), np.abs(job.U_f))
     cent = lmax * (lmax + 1)

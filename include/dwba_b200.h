@@ -171,6 +171,47 @@ typedef struct {
 
 int dwba_dot_forms(const dwba_dot_t* dots_dev, int n, int L_max, dwba_stream_t stream);
 
+/* ---------------------------------------------------------------------------
+ * Exchange integrals with the quadrature of the reference's CuPy path (radial_ME_all_L_gpu,
+ * dwba_matrix_elements.py:1563-2549; _gpu_filon_exchange :1469-1560, kernel at the CC nodes from
+ * interpolated 1/r_> and log-ratio :2072-2091). Node set: linspace phase intervals on [r_0, r_{n1-1}],
+ * Clenshaw-Curtis nodes, everything interpolated linearly in r on r[:n1]. The kernel at a node x in
+ * (r_j, r_{j+1}] factorises per grid row i into r_i^-(L+1) G^L (i > j) or h r_i^L G^-L (i <= j), G and
+ * h the geometric and harmonic interpolations of r_j, r_{j+1}; dwba_cupy_exchange_ops sums, per node
+ * set, interval j and multipole, the node weights of those factors against the two interpolation
+ * taps of rho2: ops[((L n1) + j) 4 + {0,1,2,3}] = sum W G^L (1-t), W G^L t, W h G^-L (1-t), W h G^-L t.
+ * cc_x_dev/cc_w_dev: the CuPy path's reference CC table (:1316-1347). */
+typedef struct {
+  const double* r_dev;     /* grid radii (>= n1 values) */
+  const double* logr_dev;  /* log r */
+  double* ops_dev;         /* out: (L_max+1) x n1 x 4 doubles */
+  int32_t n1;
+  int32_t n_breaks;        /* breakpoints of the linspace on [r_0, r_{n1-1}] (>= 3) */
+  int32_t L_max;
+  int32_t pad;
+} dwba_cupy_set_t;
+
+int dwba_cupy_exchange_ops(const dwba_cupy_set_t* sets_dev, int n_sets, int max_n1, int L_max, const double* cc_x_dev,
+                           const double* cc_w_dev, int n_cc, dwba_stream_t stream);
+
+/* out[L] = sum_{i<n1} a_i [r_i^-(L+1) sum_{j<i} A_L(j) + r_i^L sum_{j>=i} B_L(j)], A_L(j), B_L(j) the ops of
+ * interval j against rho2_j, rho2_{j+1} (rho2 = f g, the CuPy path's unweighted chi_f u_i on r[:n1]) and a
+ * the node set's outer CC fold of rho1 (dwba_fold with the set's T): the CuPy path's exchange I_L. Exact
+ * O(n1 L) FP64; the range rule of dwba_bilinear_semisep_fp64. */
+typedef struct {
+  const double* r_dev;
+  const double* a_dev;     /* n1 values */
+  const double* f_dev;     /* n1 values */
+  const double* g_dev;     /* n1 values */
+  const double* ops_dev;   /* the node set's dwba_cupy_exchange_ops output */
+  double* out_dev;         /* L_max+1 values */
+  int32_t n1;
+  int32_t L_max;
+} dwba_cupy_form_t;
+
+int dwba_cupy_exchange_forms(const dwba_cupy_form_t* forms_dev, int n, int L_max, double r_min_all, double r_max_all,
+                             dwba_stream_t stream);
+
 /* Dense plain form: every K_L element is generated in registers (never stored),
  * operands are staged in shared memory, partial sums are reduced with warp
  * shuffles. Work is split into chunks (CTAs); dwba_dense_chunk_prefix fills
@@ -341,7 +382,8 @@ const char* dwba_status_string(int status);
 int dwba_device_probe(int* n_devices, int* cc_major, int* cc_minor);
 /* sizeof(dwba_nodeset_t), sizeof(dwba_fold_t), sizeof(dwba_form_t), sizeof(dwba_tail_t),
  * sizeof(dwba_form_grad_t), sizeof(dwba_fold_adj_t), sizeof(dwba_fold_multi_t),
- * sizeof(dwba_potential_t), sizeof(dwba_dot_t) into sizes[0..8] (the first n of them). */
+ * sizeof(dwba_potential_t), sizeof(dwba_dot_t), sizeof(dwba_cupy_set_t), sizeof(dwba_cupy_form_t) into
+ * sizes[0..10] (the first n of them). */
 int dwba_struct_sizes(int64_t* sizes, int n);
 
 #ifdef __cplusplus

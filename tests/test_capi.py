@@ -27,11 +27,12 @@ def test_library_exports_every_declared_symbol():
 def test_abi_version_and_struct_layout():
     lib = _lib.load()
     assert lib.dwba_abi_version() == 1
-    sizes = (ctypes.c_int64 * 9)()
-    assert lib.dwba_struct_sizes(sizes, 9) == 0
+    sizes = (ctypes.c_int64 * 11)()
+    assert lib.dwba_struct_sizes(sizes, 11) == 0
     assert tuple(sizes) == (_lib.NODESET_DTYPE.itemsize, _lib.FOLD_DTYPE.itemsize, _lib.FORM_DTYPE.itemsize,
                             _lib.TAIL_DTYPE.itemsize, _lib.FORM_GRAD_DTYPE.itemsize, _lib.FOLD_ADJ_DTYPE.itemsize,
-                            _lib.FOLD_MULTI_DTYPE.itemsize, _lib.POTENTIAL_DTYPE.itemsize, _lib.DOT_DTYPE.itemsize)
+                            _lib.FOLD_MULTI_DTYPE.itemsize, _lib.POTENTIAL_DTYPE.itemsize, _lib.DOT_DTYPE.itemsize,
+                            _lib.CUPY_SET_DTYPE.itemsize, _lib.CUPY_FORM_DTYPE.itemsize)
 
 
 def test_status_strings():

@@ -46,9 +46,11 @@ def _PT(j, t, c, n):
 
 def fold_pair(grid, V_core, U_i, bound_i, bound_f, cont_i, cont_f, L_max, use_oscillatory_quadrature=True,
               oscillatory_method="advanced", CC_nodes=5, phase_increment=1.5708, min_grid_fraction=0.10,
-              k_threshold=0.5, U_f_array=None):
+              k_threshold=0.5, U_f_array=None, interp_op=None):
     """Folded operands of one (cont_i, cont_f) pair: returns a dict with n1, a_dir, b_dir,
-    a_ex, b_ex (length N), corr_dir, corr_ex (L=0 scalars) and tail[L] (added to direct)."""
+    a_ex, b_ex (length N), corr_dir, corr_ex (L=0 scalars) and tail[L] (added to direct).
+    ``interp_op``: (j, t) of the interpolation onto the CC nodes, by default the reference's
+    arithmetic (``_interp_op``); a test passes another tap arithmetic to separate its effect."""
     r = np.asarray(grid.r, dtype=float)
     w = np.asarray(grid.w_simpson, dtype=float)
     N = len(r)
@@ -73,13 +75,14 @@ def fold_pair(grid, V_core, U_i, bound_i, bound_f, cont_i, cont_f, L_max, use_os
                 nodes = (X, W)
     if osc and n1 >= 2 and nodes is not None:
         X, W = nodes
-        j1, t1 = _interp_op(X, r[:n1])
+        iop = interp_op or _interp_op
+        j1, t1 = iop(X, r[:n1])
         a_dir = np.zeros(N)
         a_dir[:n1] = _PT(j1, t1, W * _P(j1, t1, (chi_f * chi_i)[:n1]), n1)
         a_ex = np.zeros(N)
         a_ex[:n1] = _PT(j1, t1, W * _P(j1, t1, (u_f * chi_i)[:n1]), n1)
         b_dir = w * u_f * u_i
-        j2, t2 = _interp_op(X, r)
+        j2, t2 = iop(X, r)
         cex = W * _P(j2, t2, chi_f * u_i)
         iR = np.clip(np.searchsorted(r, X), 1, N - 1)
         iL = iR - 1

@@ -132,3 +132,27 @@ def levin_condition(w, r_m, r_max):
             xs = 0.5 * (b - a) * (x[::-1] + 1) + a
             worst = max(worst, np.linalg.cond(D * (2 / (xs[-1] - xs[0])) + np.diag(1j * d1(xs))))
     return worst
+
+
+def fullsize_batch_inputs():
+    """Kernel-batch inputs at full size: N = 15000 on [1e-5, 400], the benchmark's four bound pairs
+    and 16 continuum pairs over l = 0..63, k = 0.5..8 (the extremes included), seeded."""
+    import bench
+    g = bench.make_grid(15000, 1e-5, 400.0)
+    r = g.r
+    _, zeros, bounds, _ = bench.make_workload(15000, n_cont=1)
+    rng = np.random.default_rng(101)
+    picks = [((0, 0.5), (63, 8.0)), ((63, 0.5), (0, 8.0)), ((63, 8.0), (63, 8.0)), ((0, 0.5), (0, 0.5)),
+             ((1, 8.0), (62, 0.5)), ((31, 4.0), (32, 4.25)), ((0, 8.0), (0, 8.0)), ((63, 0.5), (63, 0.5))]
+    while len(picks) < 16:
+        picks.append(((int(rng.integers(0, 64)), float(rng.uniform(0.5, 8.0))),
+                      (int(rng.integers(0, 64)), float(rng.uniform(0.5, 8.0)))))
+    pairs = []
+    for pi in picks:
+        w = []
+        for l, k in pi:
+            d = float(rng.uniform(0.0, np.pi))
+            chi = np.sin(k * r - 0.5 * l * np.pi + d) * (1.0 - np.exp(-(r / ((l + 1) / k)) ** (l + 1)))
+            w.append(bench._Wave(l, k, d, chi))
+        pairs.append(tuple(w))
+    return g, zeros, bounds, pairs

@@ -59,6 +59,14 @@ def interp_taps(r, n, log_grid, x):
     return j, t
 
 
+def engine_interp_op(X, x):
+    """(j, t) of the interpolation onto the nodes ``X`` with the kernel's tap arithmetic, in the
+    form of the oracle's ``_interp_op`` (log taps where the grid passes the log-spacing test)."""
+    from oracle.quadrature import is_log_spaced_grid
+    x = np.asarray(x, dtype=float)
+    return interp_taps(x, len(x), is_log_spaced_grid(x), np.asarray(X, dtype=float))
+
+
 def bands(r, n1, n_breaks, breaks, n_cc, log1, log2):
     """(ta, bx) banded operators of one node set, as nodes.cu:bands_kernel."""
     N = len(r)

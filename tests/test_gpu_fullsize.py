@@ -10,6 +10,14 @@ restatement at these sizes in ``tests/test_oracle_fullsize.py``), with the same 
 plus, on the direct integrals with outer tails, the round-off of the tails (Levin segments agree
 only to round-off times the condition number of their collocation systems).
 
+The checker interpolates onto the CC nodes with the kernel's tap arithmetic (kernel_model.py):
+on log grids the kernel forms log x - log r_j from the series of log(1 + (x - r_j)/r_j), where the
+reference subtracts two rounded logarithms, an error of about eps |log x| / (log r_{j+1} - log r_j)
+per tap (1e-12 at N = 15000 on [1e-5, 400]) that moves direct integrals there by up to 3e-14 S_L.
+tests/test_oracle_fullsize.py shows that the two tap arithmetics differ by no more than the
+first-order bound of that rounding; here the engines are held to the gate above against the same
+taps.
+
 Workloads and sizes (seeded synthetic inputs with the shapes of each study):
 * kernel batch: N = 15000 on [1e-5, 400], L = 0..8, the four bound pairs of the benchmark and
   16 continuum pairs spanning l = 0..63, k = 0.5..8 (the extremes included);
@@ -23,7 +31,8 @@ import numpy as np
 import pytest
 
 import bench
-from golden_cases import levin_condition
+from golden_cases import fullsize_batch_inputs, levin_condition
+from kernel_model import engine_interp_op
 from oracle.folded import fold_pair, semiseparable_eval
 
 pytestmark = pytest.mark.gpu
@@ -35,7 +44,7 @@ TC_SCALE = 5e-6  # split-BF16 exchange forms: FP32 accumulation, checked against
 
 def _oracle(grid, V, Ui, bi, bf, ci, cf, L_max, Uf):
     """(direct, exchange, S_direct, S_exchange, tail tolerance, folded operands) of one (transition, pair)."""
-    fp = fold_pair(grid, V, Ui, bi, bf, ci, cf, L_max, U_f_array=Uf)
+    fp = fold_pair(grid, V, Ui, bi, bf, ci, cf, L_max, U_f_array=Uf, interp_op=engine_interp_op)
     r = np.asarray(grid.r)
 
     def ev(a, b):
@@ -71,30 +80,9 @@ def _check(gd, ge, ref, abs_scale, what, tc=False):
 
 
 # ----------------------------------------------------------------------------- kernel batch
-def _batch_inputs():
-    g = bench.make_grid(15000, 1e-5, 400.0)
-    r = g.r
-    _, zeros, bounds, _ = bench.make_workload(15000, n_cont=1)
-    rng = np.random.default_rng(101)
-    picks = [((0, 0.5), (63, 8.0)), ((63, 0.5), (0, 8.0)), ((63, 8.0), (63, 8.0)), ((0, 0.5), (0, 0.5)),
-             ((1, 8.0), (62, 0.5)), ((31, 4.0), (32, 4.25)), ((0, 8.0), (0, 8.0)), ((63, 0.5), (63, 0.5))]
-    while len(picks) < 16:
-        picks.append(((int(rng.integers(0, 64)), float(rng.uniform(0.5, 8.0))),
-                      (int(rng.integers(0, 64)), float(rng.uniform(0.5, 8.0)))))
-    pairs = []
-    for pi in picks:
-        w = []
-        for l, k in pi:
-            d = float(rng.uniform(0.0, np.pi))
-            chi = np.sin(k * r - 0.5 * l * np.pi + d) * (1.0 - np.exp(-(r / ((l + 1) / k)) ** (l + 1)))
-            w.append(bench._Wave(l, k, d, chi))
-        pairs.append(tuple(w))
-    return g, zeros, bounds, pairs
-
-
 @pytest.fixture(scope="module")
 def batch_case():
-    g, zeros, bounds, pairs = _batch_inputs()
+    g, zeros, bounds, pairs = fullsize_batch_inputs()
     refs = [[_oracle(g, zeros, zeros, bi, bf, ci, cf, 8, zeros) for ci, cf in pairs] for bi, bf in bounds]
     return g, zeros, bounds, pairs, refs
 

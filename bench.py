@@ -202,6 +202,10 @@ def ragged_sweep(engine, L_max=6, replays=5, n_energy=64, points=None, split=Tru
     outs = mp.collect()
     finite = all(np.isfinite(d).all() and np.isfinite(e).all() for d, e in outs)
     n_int = sum(2 * p.T * p.P * p.nl for p in parts)
+    routed = None
+    if mp.tc_groups:  # exchange forms the accuracy guard recomputed in FP64 (dominant forms)
+        routed = {"forms": int(sum(g["guard"].n_routed() for g in mp.tc_groups)),
+                  "of": int(sum(g["n"] for g in mp.tc_groups))}
     n_energy = len(points) // 2
     Ns = [len(pt["grid"].r) for pt in points]
     n_tail = int(sum(p.n_tail for p in parts))
@@ -215,7 +219,7 @@ def ragged_sweep(engine, L_max=6, replays=5, n_energy=64, points=None, split=Tru
             "integrals": n_int, "ms_per_sweep": ms, "ms_per_energy": ms / n_energy,
             "integrals_per_s": n_int / (ms * 1e-3), "graph": True, "replays": replays,
             "split_ms": stages, "split_algorithmic_gbs": gbs, "tail_records": n_tail,
-            "results_finite": bool(finite)}, outs
+            "tc_guard_routed": routed, "results_finite": bool(finite)}, outs
 
 
 def sweep_tcs_errors(points, ref, test, L_max=6):
@@ -937,6 +941,7 @@ def main():
                 "split_bf16_vs_plain_fp64_speedup": r_dense["ms_per_sweep"] / r_x3["ms_per_sweep"],
                 "semisep_fp64_vs_plain_fp64_speedup": r_dense["ms_per_sweep"] / ragged["ms_per_sweep"],
                 "tc_bf16x3_tcs_rel_err_max": worst, "tc_bf16x3_tcs_rel_err_median": med,
+                "tc_bf16x3_guard_routed": r_x3.get("tc_guard_routed"),
                 "dense_fp64_tcs_rel_err_max": worst_d,
                 "note": "TCS of every (energy, transition) point from each engine's integrals against the exact "
                         "FP64 semiseparable engine's (which agrees with the oracle to 1e-12 per integral)"}

@@ -125,28 +125,24 @@ __device__ __forceinline__ double ipow(double b, int e) {
   return r;
 }
 
-// envelopes f_L(x) = m_L / x^(L+1) for L = L0 .. L0+nl-1 (zero where |m_L| <= 1e-12 or x <= 1e-6)
-__device__ __forceinline__ void envelopes(const double* m, int L0, int nl, double x, double* f) {
-  if (!(x > 1e-6)) {
-#pragma unroll
-    for (int q = 0; q < LC; ++q) f[q] = 0.0;
-    return;
+// x^-(L0+1) for the envelopes f_L(x) = m_L x^-(L+1) of a chunk (0 where x <= 1e-6): the envelope of
+// multipole L0 + q is m[q] p with p advanced by 1/x per multipole
+struct EnvPow {
+  double p0, inv;
+  __device__ __forceinline__ EnvPow(double x, int L0) {
+    const bool in = x > 1e-6;
+    inv = in ? 1.0 / x : 0.0;
+    p0 = in ? ipow(inv, L0 + 1) : 0.0;
   }
-  const double inv = 1.0 / x;
-  double p = ipow(inv, L0 + 1);
-#pragma unroll
-  for (int q = 0; q < LC; ++q) {
-    f[q] = q < nl ? m[q] * p : 0.0;
-    p *= inv;
-  }
-}
+};
 
 // Re of the Filon integral over one segment (nn equally spaced nodes, nn odd) for every multipole
-// of the chunk: _filon_segment_complex with the node phases and the panel weights shared by all L
+// of the chunk: _filon_segment_complex with the node phases and the panel weights shared by all L.
+// Envelope values are formed inside the multipole loops from one running power per node, so no
+// per-node arrays of envelopes are kept.
 __device__ __forceinline__ void filon_segment_all(const double* m, int L0, int nl, double a, double b, int nn, double omega,
                                   double off, KSum* acc) {
   if (!(b - a >= 1e-15)) return;
-  double f0[LC], f1[LC], f2[LC];
   if (fabs(omega * (b - a)) < 1e-3) {  // scipy simpson with possibly unequal spacing, times the mid phase
     const double ce = cexpi(omega * (a + b) / 2 + off).re;
     double part[LC];
@@ -156,12 +152,16 @@ __device__ __forceinline__ void filon_segment_all(const double* m, int L0, int n
       const double x0 = lin(a, b, nn, i), x1 = lin(a, b, nn, i + 1), x2 = lin(a, b, nn, i + 2);
       const double h0 = x1 - x0, h1 = x2 - x1;
       const double hs = h0 + h1, hp = h0 * h1, qq = h0 / h1;
-      envelopes(m, L0, nl, x0, f0);
-      envelopes(m, L0, nl, x1, f1);
-      envelopes(m, L0, nl, x2, f2);
+      const EnvPow e0(x0, L0), e1(x1, L0), e2(x2, L0);
+      double p0 = e0.p0, p1 = e1.p0, p2 = e2.p0;
 #pragma unroll
-      for (int q = 0; q < LC; ++q)
-        part[q] += hs / 6.0 * (f0[q] * (2.0 - 1.0 / qq) + f1[q] * (hs * (hs / hp)) + f2[q] * (2.0 - qq));
+      for (int q = 0; q < LC; ++q) {
+        const double mq = q < nl ? m[q] : 0.0;
+        part[q] += hs / 6.0 * ((mq * p0) * (2.0 - 1.0 / qq) + (mq * p1) * (hs * (hs / hp)) + (mq * p2) * (2.0 - qq));
+        p0 *= e0.inv;
+        p1 *= e1.inv;
+        p2 *= e2.inv;
+      }
     }
 #pragma unroll
     for (int q = 0; q < LC; ++q) acc[q].add(part[q] * ce);
@@ -172,21 +172,21 @@ __device__ __forceinline__ void filon_segment_all(const double* m, int L0, int n
   for (int q = 0; q < LC; ++q) seg[q] = 0.0;
   double x0 = a;
   cplx e0 = cexpi(omega * x0 + off);
-  envelopes(m, L0, nl, x0, f0);
+  EnvPow v0(x0, L0);
   for (int i = 0; i + 2 < nn; i += 2) {
     const double x1 = lin(a, b, nn, i + 1), x2 = lin(a, b, nn, i + 2);
     const double h = x2 - x0;
     const cplx e1 = cexpi(omega * x1 + off), e2 = cexpi(omega * x2 + off);
-    envelopes(m, L0, nl, x1, f1);
-    envelopes(m, L0, nl, x2, f2);
+    const EnvPow v1(x1, L0), v2(x2, L0);
     if (h >= 1e-15) {
+      double w0, w1, w2;
       if (fabs(omega * h) < 1e-3) {  // the 3-node panel itself is non-oscillatory: Simpson times the mid phase
         const double h0 = x1 - x0, h1 = x2 - x1;
         const double hs = h0 + h1, hp = h0 * h1, qq = h0 / h1;
         const double ce = cexpi(omega * (x0 + x2) / 2 + off).re;
-#pragma unroll
-        for (int q = 0; q < LC; ++q)
-          seg[q] += ce * (hs / 6.0 * (f0[q] * (2.0 - 1.0 / qq) + f1[q] * (hs * (hs / hp)) + f2[q] * (2.0 - qq)));
+        w0 = ce * (hs / 6.0) * (2.0 - 1.0 / qq);
+        w1 = ce * (hs / 6.0) * (hs * (hs / hp));
+        w2 = ce * (hs / 6.0) * (2.0 - qq);
       } else {
         const double th = omega * h / 2;
         double st, ct;
@@ -209,84 +209,113 @@ __device__ __forceinline__ void filon_segment_all(const double* m, int L0, int n
         // as weights of f0, f1, f2 that every multipole shares
         const cplx mi = {0.0, -1.0 / omega};
         const cplx am = cscale(al, mi);
-        const double w0 = (h / 2) * cmul(csub(cplx{be, 0.0}, am), e0).re;
-        const double w1 = (h / 2) * (ga * e1.re);
-        const double w2 = (h / 2) * cmul(cadd(cplx{be, 0.0}, am), e2).re;
+        w0 = (h / 2) * cmul(csub(cplx{be, 0.0}, am), e0).re;
+        w1 = (h / 2) * (ga * e1.re);
+        w2 = (h / 2) * cmul(cadd(cplx{be, 0.0}, am), e2).re;
+      }
+      double p0 = v0.p0, p1 = v1.p0, p2 = v2.p0;
 #pragma unroll
-        for (int q = 0; q < LC; ++q) seg[q] += w0 * f0[q] + w1 * f1[q] + w2 * f2[q];
+      for (int q = 0; q < LC; ++q) {
+        const double mq = q < nl ? m[q] : 0.0;
+        seg[q] += w0 * (mq * p0) + w1 * (mq * p1) + w2 * (mq * p2);
+        p0 *= v0.inv;
+        p1 *= v1.inv;
+        p2 *= v2.inv;
       }
     }
     x0 = x2;
     e0 = e2;
-#pragma unroll
-    for (int q = 0; q < LC; ++q) f0[q] = f2[q];
+    v0 = v2;
   }
 #pragma unroll
   for (int q = 0; q < LC; ++q) acc[q].add(seg[q]);
 }
 
-// Levin collocation on one segment (8 nodes) for every multipole of the chunk: the system matrix
-// does not depend on L, so it is factorised once and solved for each envelope
-// res[q]: the segment's contribution to multipole L0 + q (zero where there is none); a separate
-// result array keeps the caller's accumulators out of local memory
-__device__ __noinline__ void levin_segment_all(const double* m, int L0, int nl, const PhaseD& ph, double a, double b,
-                                  double* res) {
-  for (int q = 0; q < LC; ++q) res[q] = 0.0;
+// Levin collocation on one segment (8 nodes) for every multipole of the chunk, solved by a group
+// of 8 lanes: lane `row` of the group holds row `row` of the 8x8 complex collocation system in
+// registers (compile-time column indices only, so nothing goes to local memory). The system does
+// not depend on L: it is factorised once by Gaussian elimination with partial pivoting (largest
+// |re| + |im| of the column among the rows not yet used; the pivot order is kept instead of
+// swapping rows, and the pivot row is broadcast by shuffles) and solved for each envelope.
+// All 32 lanes call it together (shuffles over groups of 8); `valid` = the group has a segment.
+// res[q]: the segment's contribution to multipole L0 + q, the same on every lane of the group
+// (zero for an invalid group or a singular system).
+__device__ __noinline__ void levin_segment_group(const double* m, int L0, int nl, const PhaseD& ph, double a, double b,
+                                                 bool valid, double* res) {
+  const int row = threadIdx.x & 7;
   const LevinD& lv = s_lv;
-  cplx A[8][8];
-  double x[8];
-  int perm[8];
-  for (int k = 0; k < 8; ++k) x[k] = 0.5 * (b - a) * (lv.xr[k] + 1) + a;
-  const double h = x[7] - x[0];
-  if (h < 1e-15) return;
-  const double sc = 2.0 / h;
-  for (int i = 0; i < 8; ++i) {
-    for (int j = 0; j < 8; ++j) A[i][j] = {lv.D[i][j] * sc, 0.0};
-    A[i][i].im += ph.d1(x[i]);
-    perm[i] = i;
+  const double hw = 0.5 * (b - a);
+  const double xi = hw * (lv.xr[row] + 1) + a;
+  const double x0 = hw * (lv.xr[0] + 1) + a, x7 = hw * (lv.xr[7] + 1) + a;
+  const double h = x7 - x0;
+  bool ok = valid && !(h < 1e-15);
+  const double sc = ok ? 2.0 / h : 0.0;
+  const double d1 = ph.d1(xi);
+  cplx A[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) A[j] = {lv.D[row][j] * sc, j == row ? d1 : 0.0};
+  int step_of = 8;  // elimination step at which this row became the pivot
+  int pv[8];        // pivot row of each step
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    double mag = step_of < 8 ? -1.0 : fabs(A[k].re) + fabs(A[k].im);
+    int who = row;
+#pragma unroll
+    for (int off = 4; off > 0; off >>= 1) {  // group argmax, ties to the lower row
+      const double om = __shfl_xor_sync(0xffffffffu, mag, off, 8);
+      const int ow = __shfl_xor_sync(0xffffffffu, who, off, 8);
+      if (om > mag || (om == mag && ow < who)) {
+        mag = om;
+        who = ow;
+      }
+    }
+    pv[k] = who;
+    if (!(mag > 0.0)) ok = false;  // singular (or an invalid group): the result is dropped
+    cplx P[8];
+#pragma unroll
+    for (int j = k; j < 8; ++j) {
+      P[j].re = __shfl_sync(0xffffffffu, A[j].re, who, 8);
+      P[j].im = __shfl_sync(0xffffffffu, A[j].im, who, 8);
+    }
+    if (row == who) {
+      step_of = k;
+    } else if (step_of == 8) {
+      const cplx inv = cdiv({1.0, 0.0}, P[k]);
+      const cplx l = cmul(A[k], inv);
+      A[k] = l;
+#pragma unroll
+      for (int j = k + 1; j < 8; ++j) A[j] = csub(A[j], cmul(l, P[j]));
+    }
   }
+  const cplx e7 = cexpi(ph.phi(x7)), e0 = cexpi(ph.phi(x0));
+  const double inv_x = xi > 1e-6 ? 1.0 / xi : 0.0;
+  double pw = xi > 1e-6 ? ipow(inv_x, L0 + 1) : 0.0;
 #pragma unroll 1
-  for (int k = 0; k < 8; ++k) {  // partial pivoting by |re| + |im|, multipliers kept in A
-    int piv = k;
-    double best = -1.0;
-    for (int i = k; i < 8; ++i) {
-      const double mm = fabs(A[i][k].re) + fabs(A[i][k].im);
-      if (mm > best) { best = mm; piv = i; }
+  for (int q = 0; q < LC; ++q) {
+    res[q] = 0.0;
+    if (q >= nl) continue;  // warp-uniform
+    cplx u = {m[q] * pw, 0.0};
+    pw *= inv_x;
+    // forward: rows that became pivots after step k take their multiplier of step k
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      cplx y;
+      y.re = __shfl_sync(0xffffffffu, u.re, pv[k], 8);
+      y.im = __shfl_sync(0xffffffffu, u.im, pv[k], 8);
+      if (step_of > k) u = csub(u, cmul(A[k], y));
     }
-    if (best == 0.0) return;
-    if (piv != k) {
-      for (int j = 0; j < 8; ++j) { cplx t = A[k][j]; A[k][j] = A[piv][j]; A[piv][j] = t; }
-      const int t = perm[k]; perm[k] = perm[piv]; perm[piv] = t;
+    // backward: the pivot row of step k gives unknown k (node k); every lane keeps all unknowns
+    cplx z[8];
+#pragma unroll
+    for (int k = 7; k >= 0; --k) {
+      cplx t = u;
+#pragma unroll
+      for (int j = k + 1; j < 8; ++j) t = csub(t, cmul(A[j], z[j]));
+      const cplx zk = cdiv(t, A[k]);
+      z[k].re = __shfl_sync(0xffffffffu, zk.re, pv[k], 8);
+      z[k].im = __shfl_sync(0xffffffffu, zk.im, pv[k], 8);
     }
-    const cplx inv = cdiv({1.0, 0.0}, A[k][k]);
-    for (int i = k + 1; i < 8; ++i) {
-      const cplx l = cmul(A[i][k], inv);
-      A[i][k] = l;
-      for (int j = k + 1; j < 8; ++j) A[i][j] = csub(A[i][j], cmul(l, A[k][j]));
-    }
-  }
-  const cplx e7 = cexpi(ph.phi(x[7])), e0 = cexpi(ph.phi(x[0]));
-  double inv[8], pw[8];  // 1 / x and x^-(L+1) at the permuted nodes, advanced by one power per multipole
-  for (int i = 0; i < 8; ++i) {
-    const double xi = x[perm[i]];
-    inv[i] = xi > 1e-6 ? 1.0 / xi : 0.0;
-    pw[i] = xi > 1e-6 ? ipow(inv[i], L0 + 1) : 0.0;
-  }
-#pragma unroll 1
-  for (int q = 0; q < nl; ++q) {
-    cplx u[8];
-    for (int i = 0; i < 8; ++i) {
-      u[i] = {m[q] * pw[i], 0.0};
-      pw[i] *= inv[i];
-    }
-    for (int k = 0; k < 8; ++k)
-      for (int i = k + 1; i < 8; ++i) u[i] = csub(u[i], cmul(A[i][k], u[k]));
-    for (int i = 7; i >= 0; --i) {
-      cplx sum = u[i];
-      for (int j = i + 1; j < 8; ++j) sum = csub(sum, cmul(A[i][j], u[j]));
-      u[i] = cdiv(sum, A[i][i]);
-    }
-    res[q] = csub(cmul(u[7], e7), cmul(u[0], e0)).re;
+    res[q] = ok ? csub(cmul(z[7], e7), cmul(z[0], e0)).re : 0.0;
   }
 }
 
@@ -315,14 +344,21 @@ __device__ __noinline__ void outer_branch_all(const double* m, int L0, int nl, c
       filon_segment_all(m, L0, nl, a, b, nn, om, off, acc);
     }
   } else {
+    // four segments per warp pass, one per group of 8 lanes; lane 0 of a group accumulates it
     const int nseg = (int)max(1.0, ceil((rmax - rm) / h));
-    for (int s = lane; s < nseg; s += 32) {
-      const double a = lin(rm, rmax, nseg + 1, s), b = lin(rm, rmax, nseg + 1, s + 1);
+    const int grp = lane >> 3;
+    for (int s0 = 0; s0 < nseg; s0 += 4) {  // warp-uniform
+      const int s = s0 + grp;
+      const bool valid = s < nseg;
+      const double a = valid ? lin(rm, rmax, nseg + 1, s) : rm;
+      const double b = valid ? lin(rm, rmax, nseg + 1, s + 1) : rm;
       double res[LC];
-      levin_segment_all(m, L0, nl, ph, a, b, res);
+      levin_segment_group(m, L0, nl, ph, a, b, valid, res);
+      if (valid && (lane & 7) == 0) {
 #pragma unroll
-      for (int q = 0; q < LC; ++q)
-        if (q < nl) acc[q].add(res[q]);
+        for (int q = 0; q < LC; ++q)
+          if (q < nl) acc[q].add(res[q]);
+      }
     }
   }
 #pragma unroll
@@ -352,7 +388,10 @@ __device__ double analytical_tail(double r_m, const WaveD& wi, const WaveD& wf, 
 
 // one warp per (record, chunk of up to LC multipoles): the Filon / Levin segments of both phase
 // branches over the lanes, every node's phase factor and every panel's weights shared by the chunk
-__global__ void __launch_bounds__(128, 4) tails_kernel(const dwba_tail_t* __restrict__ recs, int n, int L_max, int max_seg, double max_dphi,
+#ifndef DWBA_TAILS_MIN_BLOCKS
+#define DWBA_TAILS_MIN_BLOCKS 3  // 168 registers: the Filon and Levin paths run without spills
+#endif
+__global__ void __launch_bounds__(128, DWBA_TAILS_MIN_BLOCKS) tails_kernel(const dwba_tail_t* __restrict__ recs, int n, int L_max, int max_seg, double max_dphi,
                              LevinD lv) {
   for (int i = threadIdx.x; i < 72; i += blockDim.x)
     (&s_lv.D[0][0])[i] = i < 64 ? lv.D[i / 8][i % 8] : lv.xr[i - 64];

@@ -26,44 +26,55 @@ ENGINES = ("dense", "semisep", "tc_bf16x3", "tc_bf16x6")
 TC_TERMS = {"tc_bf16x3": 2, "tc_bf16x6": 3}
 
 
-def tc_route_ratio() -> float:
-    """Cancellation bound of the split-BF16 engines: an exchange form whose scale S_L = |a|^T K_L |b|
-    exceeds this multiple of |I_L| at any L is recomputed in FP64 (DWBA_B200_TC_ROUTE; <= 0 disables)."""
+def tc_route_fraction() -> float:
+    """Routing bound of the split-BF16 engines: an exchange form whose |I_L| exceeds this fraction of
+    the largest |I_L| of its transition at any L is recomputed in FP64 (DWBA_B200_TC_ROUTE; <= 0
+    disables the guard)."""
     import os
     try:
-        return float(os.environ.get("DWBA_B200_TC_ROUTE", "8"))
+        return float(os.environ.get("DWBA_B200_TC_ROUTE", "0.1"))
     except ValueError:
-        return 8.0
+        return 0.1
 
 
 class TCGuard:
-    """Accuracy guard of the split-BF16 exchange forms of one launch (FP32 accumulation of K_L b).
+    """Accuracy guard of the split-BF16 exchange forms of one launch.
 
-    After the tensor-core pass: the exact scale S_L of every form (semiseparable pass on |a|, |b|),
-    a flag for the forms with S_L > R |I_L| at some L (their FP32 rounding, about 1e-7 S_L, is then
-    not small against I_L), the flagged forms recomputed by the exact FP64 form (the others masked to
-    empty forms, which cost nothing) and merged into the result. Device-side only, no host sync, so
-    it is captured in CUDA graphs with the rest of the launch sequence."""
+    The tensor-core forms carry an error of about 1e-6 of their scale |a|^T K_L |b| (FP32 values of
+    K_L and FP32 accumulation), independent of the bf16 split. A transition's cross section is
+    dominated by its largest integrals, so the guard recomputes in FP64 the forms whose |I_L| (from
+    the tensor-core pass) exceeds ``theta`` times the largest |I_L| of their transition (``groups``:
+    the transition of each form) at some L -- typically a few percent of the forms -- and keeps the
+    tensor-core values of the rest, whose errors are small against the dominant integrals. The
+    flagged forms are evaluated by the exact semiseparable form (the others masked to empty forms,
+    which cost nothing) and merged into the result. Device-side only, no host sync, so it is
+    captured in CUDA graphs with the rest of the launch sequence."""
 
-    def __init__(self, forms_host: np.ndarray, forms_d: torch.Tensor, n: int, nl: int, dev, ratio: float):
-        self.n, self.ratio = n, ratio
+    def __init__(self, forms_d: torch.Tensor, n: int, nl: int, dev, groups: np.ndarray, theta: float):
+        self.n, self.theta, self.nl = n, theta, nl
         self.forms_d = forms_d
+        g = np.ascontiguousarray(groups, dtype=np.int64)
+        self.n_groups = int(g.max()) + 1 if len(g) else 0
+        self.gidx = _dev(g, dev)
+        self.gidx2 = self.gidx[:, None].expand(n, nl)
         self.desc32 = forms_d.view(torch.int32).view(n, _lib.FORM_DTYPE.itemsize // 4)
         self.masked = torch.empty_like(forms_d)
         self.masked32 = self.masked.view(torch.int32).view(n, _lib.FORM_DTYPE.itemsize // 4)
-        self.scale = torch.empty((n, nl), dtype=torch.float64, device=dev)
+        self.mag = torch.empty((n, nl), dtype=torch.float64, device=dev)
+        self.gmax = torch.empty((max(1, self.n_groups), nl), dtype=torch.float64, device=dev)
         self.exact = torch.empty((n, nl), dtype=torch.float64, device=dev)
         self.over = torch.empty((n, nl), dtype=torch.bool, device=dev)
         self.flag = torch.zeros(n, dtype=torch.bool, device=dev)
         self.rows = _lib.FORM_DTYPE.fields["n_rows"][1] // 4  # int32 column of n_rows (n_cols follows)
 
     def launch(self, lib, L_max: int, ds: np.ndarray, r_min: float, r_max: float, out: torch.Tensor) -> None:
-        if self.ratio <= 0 or self.n == 0:
+        if self.theta <= 0 or self.n == 0:
             return
         st = _stream()
-        _lib.check(lib.dwba_bilinear_semisep_abs_fp64(_ptr(self.forms_d), self.n, L_max, ds.ctypes.data, r_min, r_max,
-                                                      _ptr(self.scale), st), "dwba_bilinear_semisep_abs_fp64")
-        torch.gt(self.scale, self.ratio * out.abs(), out=self.over)
+        torch.abs(out, out=self.mag)
+        self.gmax.zero_()
+        self.gmax.scatter_reduce_(0, self.gidx2, self.mag, reduce="amax", include_self=True)
+        torch.gt(self.mag, self.theta * self.gmax.index_select(0, self.gidx), out=self.over)
         torch.any(self.over, dim=1, out=self.flag)
         self.masked.copy_(self.forms_d)
         keep = self.flag.to(torch.int32)
@@ -74,7 +85,7 @@ class TCGuard:
         out.copy_(torch.where(self.flag[:, None], self.exact, out))
 
     def n_routed(self) -> int:
-        return int(self.flag.sum().item()) if self.ratio > 0 else 0
+        return int(self.flag.sum().item()) if self.theta > 0 else 0
 
 
 def _ptr(t: Optional[torch.Tensor]) -> int:
@@ -924,7 +935,7 @@ class PreparedJob:
             self.forms_ex_d = _dev(np.ascontiguousarray(forms[1::2]).view(np.uint8), dev)
             self.out_dir = torch.empty((T * P, nl), dtype=torch.float64, device=dev)
             self.out_ex = torch.empty((T * P, nl), dtype=torch.float64, device=dev)
-            self.tc_guard = TCGuard(forms[1::2], self.forms_ex_d, T * P, nl, dev, tc_route_ratio())
+            self.tc_guard = TCGuard(self.forms_ex_d, T * P, nl, dev, np.repeat(np.arange(T), P), tc_route_fraction())
             dp = self.direct_plan
             self.form_launch = FormLaunch([(forms, dp, N, _ptr(dg.r), dp.dot_fo // 2, dp.ss_fo // 2)], self.out_dir,
                                           nl, dev)
@@ -1200,7 +1211,10 @@ class MultiPrepared:
                        "status": torch.zeros(1, dtype=torch.int32, device=dev),
                        "out": torch.empty((len(fe), self.nl), dtype=torch.float64, device=dev),
                        "r_lo": float(parts[ks[0]].job.grid.r[0]), "r_hi": float(parts[ks[0]].job.grid.r[-1])}
-                grp["guard"] = TCGuard(fe, grp["forms"], len(fe), self.nl, dev, tc_route_ratio())
+                # transition of each form across the group's jobs (the jobs' forms are transition-major)
+                gids = np.concatenate([g0 + np.repeat(np.arange(parts[k].T), parts[k].P)
+                                       for g0, k in zip(np.cumsum([0] + [parts[k].T for k in ks])[:-1], ks)])
+                grp["guard"] = TCGuard(grp["forms"], len(fe), self.nl, dev, gids, tc_route_fraction())
                 off = 0
                 for k in ks:
                     p = parts[k]

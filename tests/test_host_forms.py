@@ -159,9 +159,9 @@ class _EmulatedLib:
         return self._run(forms, n, L_max, out, False)
 
 
-def test_tensor_core_guard_routes_cancelling_forms(monkeypatch):
-    """The guard recomputes exactly the exchange forms whose scale S_L exceeds R |I_L| at some L and
-    leaves the others as the tensor cores gave them."""
+def test_tensor_core_guard_routes_the_dominant_forms(monkeypatch):
+    """The guard recomputes exactly the exchange forms whose |I_L| exceeds theta times the largest
+    |I_L| of their transition at some L, and leaves the others as the tensor cores gave them."""
     from dwba_b200 import engine
     monkeypatch.setattr(engine, "_stream", lambda: 0)  # no CUDA stream on the CPU
     pj, r = _job("tc_bf16x3")
@@ -175,11 +175,16 @@ def test_tensor_core_guard_routes_cancelling_forms(monkeypatch):
     lib.dwba_bilinear_semisep_fp64(g.forms_d.data_ptr(), n, pj.job.L_max, None, 0, 0, exact.data_ptr(), None)
     out = exact * (1.0 + 1e-3)
     before = out.clone()
-    scale = torch.zeros((n, nl), dtype=torch.float64)
-    lib.dwba_bilinear_semisep_abs_fp64(g.forms_d.data_ptr(), n, pj.job.L_max, None, 0, 0, scale.data_ptr(), None)
-    g.ratio = float(torch.median((scale / before.abs()).max(1).values))  # about half the forms cancel more
+    g.theta = 0.3
     g.launch(lib, pj.job.L_max, pj.ds, float(r[0]), float(r[-1]), out)
-    want = (scale > g.ratio * before.abs()).any(1)
+    t_of = torch.from_numpy(np.repeat(np.arange(pj.T), pj.P))
+    gmax = torch.stack([before[t_of == t].abs().max(0).values for t in range(pj.T)])
+    want = (before.abs() > 0.3 * gmax[t_of]).any(1)
     assert torch.equal(g.flag, want) and 0 < int(want.sum()) < n
     assert torch.equal(out[want], exact[want]) and torch.equal(out[~want], before[~want])
     assert torch.equal(g.forms_d, pj.forms_ex_d)  # the descriptors themselves are untouched
+    # every transition keeps its largest form at each L exactly
+    for t in range(pj.T):
+        rows = torch.nonzero(t_of == t).ravel()
+        top = rows[before[rows].abs().argmax(0)]
+        assert bool(g.flag[top].all())

@@ -769,12 +769,25 @@ def main():
             p.launch_forms_exchange()
         ev_tc[1].record(st)
     else:
+        form_marks = []
         for p in preps:
-            p.launch_forms()
+            if args.engine == "semisep":
+                p.form_launch.launch(p.lib, p.job.L_max, p.ds, float(p.job.grid.r[0]), float(p.job.grid.r[-1]),
+                                     marks=form_marks)
+            else:
+                p.launch_forms()
     ev[3].record(st)
     barrier()
     split = {"nodesets_ms": ev[0].elapsed_time(ev[1]), "folds_ms": ev[1].elapsed_time(ev[2]),
              "forms_ms": ev[2].elapsed_time(ev[3])}
+    sub_ms = {}
+    if not tc and args.engine == "semisep":
+        # the forms stage per launch: potentials, dot forms, semiseparable forms (events between them)
+        prev = ev[2]
+        for name, e in form_marks:
+            sub_ms[name] = sub_ms.get(name, 0.0) + prev.elapsed_time(e)
+            prev = e
+        split.update({f"{k}_ms": v for k, v in sub_ms.items()})
     if tc:
         split["forms_exchange_tensor_ms"] = ev_tc[0].elapsed_time(ev_tc[1])
     # timed region
@@ -812,7 +825,7 @@ def main():
     # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu capture of
     # the default workload (profiles/launches_semisep_synthetic_batch_N15000.md); other sizes: null
     default_size = args.n_cont == N_CONT
-    traffic = {"nodeset_rows_kernel": 1.929e9, "fold_kernel": 4.654e9, "semisep_kernel": 3.214e9}
+    traffic = {"nodeset_rows_kernel": 1.929e9, "fold_kernel": 4.654e9}
 
     def hbm_roof(kernel, nbytes, t_ms, note):
         ach = nbytes / (t_ms * 1e-3) / 1e9
@@ -840,8 +853,17 @@ def main():
                 "note": "achieved = executed bf16 MMA flops (2*M*N*K per product, 3 or 6 products of the split) / "
                         "kernel time; useful = dense-equivalent 2*n_rows*n_cols per exchange integral"}
     elif args.engine == "semisep":
-        roof = hbm_roof("semisep_kernel", fb, forms_ms,
-                        "algorithmic bytes = 8*(n_rows + n_cols + n_grid) per form (a, b, r read once)")
+        sb = {}
+        for p in preps:
+            for k, v in p.form_launch.stage_bytes().items():
+                sb[k] = sb.get(k, 0.0) + v
+        kernels.append(hbm_roof("potential_kernel", sb["potentials"], sub_ms["potentials"],
+                                "algorithmic bytes = b and r read, (L_max+1) potential rows written, per transition"))
+        kernels.append(hbm_roof("dot_kernel", sb["dots"], sub_ms["dots"],
+                                "algorithmic bytes = each pair's folded density a read once per transition, each "
+                                "potential tile once per run of 16 pairs"))
+        roof = hbm_roof("semisep_kernel", sb["semisep"], sub_ms["semisep"],
+                        "algorithmic bytes = 8*(n_rows + n_cols + n_grid) per exchange form (a, b, r read once)")
     else:
         ach = flops / (forms_ms * 1e-3) / 1e12
         roof = {"bound": "fp64", "achieved": ach, "peak": None, "unit": "TFLOP/s (dense-equivalent 2 n1 n2 per L)",

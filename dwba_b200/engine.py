@@ -717,17 +717,45 @@ class FormLaunch:
             self.out_ss = torch.empty((self.n_ss, nl), dtype=torch.float64, device=dev)
         self.pots_host, self.dots_host = pots, dots
 
-    def launch(self, lib, L_max: int, ds: np.ndarray, r_min: float, r_max: float) -> None:
+    def launch(self, lib, L_max: int, ds: np.ndarray, r_min: float, r_max: float, marks: Optional[list] = None) -> None:
+        """Enqueue the potentials, the dot forms and the semiseparable forms. With ``marks`` (a list),
+        a CUDA event is recorded after each of the three and appended as (name, event)."""
         st = _stream()
+
+        def mark(name):
+            if marks is not None:
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record(torch.cuda.current_stream())
+                marks.append((name, ev))
         if self.n_pots:
             _lib.check(lib.dwba_multipole_potentials(_ptr(self.pots_d), self.n_pots, L_max, ds.ctypes.data, r_min, r_max,
                                                      st), "dwba_multipole_potentials")
+        mark("potentials")
         if self.n_dots:
             _lib.check(lib.dwba_dot_forms(_ptr(self.dots_d), self.n_dots, L_max, st), "dwba_dot_forms")
+        mark("dots")
         if self.n_ss:
             _lib.check(lib.dwba_bilinear_semisep_fp64(_ptr(self.ss_forms_d), self.n_ss, L_max, ds.ctypes.data, r_min,
                                                       r_max, _ptr(self.out_ss), st), "dwba_bilinear_semisep_fp64")
             self.out.index_copy_(0, self.ss_rows_d, self.out_ss)
+        mark("semisep")
+
+    def stage_bytes(self) -> Dict[str, float]:
+        """Algorithmic bytes of each of the three launches (see ``algorithmic_bytes``)."""
+        out = {"potentials": 0.0, "dots": 0.0, "semisep": 0.0}
+        if self.n_pots:
+            p = self.pots_host
+            out["potentials"] = float(np.sum(8.0 * (2.0 * p["n_cols"] + self.nl * p["n_rows"].astype(np.float64))))
+        if self.n_dots:
+            d = self.dots_host
+            runs = d[::_lib.DOT_RUN]
+            out["dots"] = float(np.sum(8.0 * d["n_rows"].astype(np.float64))) + \
+                float(np.sum(8.0 * self.nl * runs["stride"].astype(np.float64)))
+        if self.n_ss:
+            f = self.ss_forms_host
+            m = np.maximum(f["n_rows"], f["n_cols"]).astype(np.float64)
+            out["semisep"] = float(np.sum(8.0 * (f["n_rows"].astype(np.float64) + f["n_cols"] + m)))
+        return out
 
     def algorithmic_bytes(self) -> float:
         """Operand bytes: each potential reads b and r and writes (L_max+1) rows; each dot form reads a

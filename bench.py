@@ -203,9 +203,8 @@ def ragged_sweep(engine, L_max=6, replays=5, n_energy=64, points=None, split=Tru
     finite = all(np.isfinite(d).all() and np.isfinite(e).all() for d, e in outs)
     n_int = sum(2 * p.T * p.P * p.nl for p in parts)
     routed = None
-    if mp.tc_groups:  # exchange forms the accuracy guard recomputed in FP64 (dominant forms)
-        routed = {"forms": int(sum(g["guard"].n_routed() for g in mp.tc_groups)),
-                  "of": int(sum(g["n"] for g in mp.tc_groups))}
+    if mp.tc is not None:  # exchange forms the accuracy guard recomputed in FP64 (dominant forms)
+        routed = {"forms": int(mp.tc["guard"].n_routed()), "of": int(mp.tc["n"])}
     n_energy = len(points) // 2
     Ns = [len(pt["grid"].r) for pt in points]
     n_tail = int(sum(p.n_tail for p in parts))

@@ -44,6 +44,8 @@ CUPY_SET_DTYPE = np.dtype([("r", "<u8"), ("logr", "<u8"), ("ops", "<u8"), ("n1",
                            ("L_max", "<i4"), ("pad", "<i4")])
 CUPY_FORM_DTYPE = np.dtype([("r", "<u8"), ("a", "<u8"), ("f", "<u8"), ("g", "<u8"), ("ops", "<u8"), ("out", "<u8"),
                             ("n1", "<i4"), ("L_max", "<i4")])
+TC_SEGMENT_DTYPE = np.dtype([("forms", "<u8"), ("r", "<u8"), ("out", "<u8"), ("n_forms", "<i4"), ("n_grid", "<i4")])
+TC_TILE_DTYPE = np.dtype([("bn", "<i4"), ("stages", "<i4"), ("order", "<i4"), ("pad", "<i4")])
 TAIL_DTYPE = np.dtype([("wave", "<f8", (10,)), ("r_m", "<f8"), ("r_max", "<f8"), ("moments", "<u8"), ("out", "<u8"),
                        ("mode", "<i4"), ("pad", "<i4")])
 
@@ -94,6 +96,8 @@ def _declare(lib):
         "dwba_dot_forms": (c_int, [c_vp, c_int, c_int, c_vp]),
         "dwba_cupy_exchange_ops": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_int, c_vp]),
         "dwba_cupy_exchange_forms": (c_int, [c_vp, c_int, c_int, c_dbl, c_dbl, c_vp]),
+        "dwba_tc_ragged_workspace_bytes": (c_i64, [c_vp, c_int, c_int, c_int, c_vp]),
+        "dwba_bilinear_tc_bf16_ragged": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -113,11 +117,12 @@ def load():
     lib = _declare(ctypes.CDLL(LIB_PATH))
     if lib.dwba_abi_version() != 1:
         raise ImportError("libdwba_b200.so ABI version mismatch")
-    sizes = (ctypes.c_int64 * 11)()
-    lib.dwba_struct_sizes(sizes, 11)
+    sizes = (ctypes.c_int64 * 13)()
+    lib.dwba_struct_sizes(sizes, 13)
     want = (NODESET_DTYPE.itemsize, FOLD_DTYPE.itemsize, FORM_DTYPE.itemsize, TAIL_DTYPE.itemsize,
             FORM_GRAD_DTYPE.itemsize, FOLD_ADJ_DTYPE.itemsize, FOLD_MULTI_DTYPE.itemsize,
-            POTENTIAL_DTYPE.itemsize, DOT_DTYPE.itemsize, CUPY_SET_DTYPE.itemsize, CUPY_FORM_DTYPE.itemsize)
+            POTENTIAL_DTYPE.itemsize, DOT_DTYPE.itemsize, CUPY_SET_DTYPE.itemsize, CUPY_FORM_DTYPE.itemsize,
+            TC_SEGMENT_DTYPE.itemsize, TC_TILE_DTYPE.itemsize)
     if tuple(sizes) != want:
         raise ImportError(f"struct layout mismatch: library {tuple(sizes)} vs binding {want}")
     _lib = lib

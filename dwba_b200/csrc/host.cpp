@@ -464,6 +464,8 @@ extern "C" int dwba_struct_sizes(int64_t* sizes, int n) {
   if (n >= 9) sizes[8] = (int64_t)sizeof(dwba_dot_t);
   if (n >= 10) sizes[9] = (int64_t)sizeof(dwba_cupy_set_t);
   if (n >= 11) sizes[10] = (int64_t)sizeof(dwba_cupy_form_t);
+  if (n >= 12) sizes[11] = (int64_t)sizeof(dwba_tc_segment_t);
+  if (n >= 13) sizes[12] = (int64_t)sizeof(dwba_tc_tile_t);
   return DWBA_OK;
 }
 

@@ -25,7 +25,10 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <atomic>
+#include <mutex>
+#include <vector>
 
 #include "common.cuh"
 
@@ -58,6 +61,29 @@ struct GemmParams {
   long long wait_cycles;       // bound of every pipeline wait (SM clocks)
   int n_grid, n_pad, f_pad, n_iblk, L_max, n_forms, n_kb, n_Ltot;
   double diag[DWBA_MAX_L + 1];
+};
+
+// One grid of a (ragged) launch: its operands, workspace tables and layout. The B terms of every
+// segment are rows of one bf16 matrix (one tensor map): segment rows row0 .. row0 + NT f_pad - 1.
+struct TcSeg {
+  const double* r;             // grid (n_grid)
+  const double* lg;            // log2(r) (n_grid)
+  const dwba_form_t* forms;    // a_f (rows) for the epilogue
+  double* partial;             // [n_L][n_iblk][f_pad]
+  const int* bexp;             // per form: b was scaled by 2^-bexp before the split
+  const float* vt;             // [2][n_L][n_pad]
+  const float* st;             // [n_L][n_iblk][n_kb]
+  double* gpart;               // gradient mode: [n_L][f_pad][n_pad]
+  int n_grid, n_pad, f_pad, n_iblk, n_forms, n_kb, row0, n_fblk;
+};
+constexpr int TC_MAX_SEGS = 96;
+// The segments of one launch, passed by value (kernel parameter space). CTAs are numbered
+// segment by segment (cta0 ascending); within a segment, order 0 runs the row blocks fastest,
+// then the form blocks, then the multipoles; order 1 runs the form blocks fastest.
+struct TcSegs {
+  int n, order;
+  int cta0[TC_MAX_SEGS + 1];
+  TcSeg s[TC_MAX_SEGS];
 };
 
 // ---- PTX wrappers --------------------------------------------------------------------
@@ -208,13 +234,15 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 //   above the diagonal: K = r_i^L / r_j^(L+1) = [(r_i/c_hi)^L] [c_hi^L / c_b^(L+1)] [(r_j/c_b)^-(L+1)]
 // GRAD = false: I_f,L = sum_i a_f[i] Z_L[i, f] (partials per row block). GRAD = true (backward):
 // the epilogue writes g_f,L Z_L[i, f] for every row i instead, summed over L afterwards.
-template <int NT, int BN, bool GRAD>
+template <int NT, int BN, bool GRAD, int SN = tc_stages(NT)>
 __global__ void __launch_bounds__(THREADS, 1)
-tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P) {
+tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const __grid_constant__ GemmParams P,
+                   const __grid_constant__ TcSegs SG) {
   constexpr int B_BYTES = BN * BK * 2;            // one term
   constexpr int STAGE = NT * B_BYTES;             // shared memory per stage
   constexpr int NPROD = NT == 2 ? 3 : 6;
-  constexpr int S = tc_stages(NT);
+  constexpr int S = SN;
+  static_assert(S >= 2 && S * STAGE + 1024 <= 227 * 1024, "shared memory");
   constexpr int A_COLS = BK / 2;                  // tensor-memory columns of one K_L term
   static_assert(BN + S * NT * A_COLS <= TMEM_COLS, "tensor memory");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -227,9 +255,29 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
   __shared__ volatile int s_abort;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int iblk = blockIdx.x, fblk = blockIdx.y, L = blockIdx.z;
+  // this CTA's segment (binary search over the ascending cta0) and its (row block, form block, L)
+  const int cta = blockIdx.x;
+  int sg_lo = 0, sg_hi = SG.n - 1;
+  while (sg_lo < sg_hi) {
+    const int mid = (sg_lo + sg_hi + 1) >> 1;
+    if (SG.cta0[mid] <= cta) sg_lo = mid; else sg_hi = mid - 1;
+  }
+  const TcSeg& G = SG.s[sg_lo];  // parameter space (grid constant): no local copy
+  const int local = cta - SG.cta0[sg_lo];
+  int iblk, fblk, L;
+  if (SG.order == 0) {
+    iblk = local % G.n_iblk;
+    const int q = local / G.n_iblk;
+    fblk = q % G.n_fblk;
+    L = q / G.n_fblk;
+  } else {
+    fblk = local % G.n_fblk;
+    const int q = local / G.n_fblk;
+    iblk = q % G.n_iblk;
+    L = q / G.n_iblk;
+  }
   const int i0 = iblk * BM, f0 = fblk * BN;
-  const int n_kb = P.n_kb;
+  const int n_kb = G.n_kb;
 
   if (tid == 0) {
     // a CTA that starts after another one timed out skips the work (the decision is shared
@@ -251,13 +299,13 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
   }
   // row factors: U_i below the diagonal (c_lo^L / r_i^(L+1)) and above ((r_i/c_hi)^L), as exp2 of
   // FP64 differences of log2 r
-  const double lg_lo = P.lg[i0];
-  const double lg_hi = P.lg[min(i0 + BM, P.n_grid) - 1];
+  const double lg_lo = G.lg[i0];
+  const double lg_hi = G.lg[min(i0 + BM, G.n_grid) - 1];
   const double Lp1 = (double)(L + 1), Ld = (double)L;
   for (int m = tid; m < BM; m += THREADS) {
-    const bool in = i0 + m < P.n_grid;
-    const double ri = in ? P.r[i0 + m] : 0.0;
-    const double li = in ? P.lg[i0 + m] : 0.0;
+    const bool in = i0 + m < G.n_grid;
+    const double ri = in ? G.r[i0 + m] : 0.0;
+    const double li = in ? G.lg[i0 + m] : 0.0;
     sRi[m] = ri;
     sUb[m] = in ? (float)exp2(-Lp1 * (li - lg_lo) - lg_lo) : 0.0f;
     sUa[m] = in ? (float)exp2(Ld * (li - lg_hi)) : 0.0f;
@@ -291,7 +339,7 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
         mbar_expect_tx(&bar_b[st_idx], NT * B_BYTES);
 #pragma unroll
         for (int t = 0; t < NT; ++t)
-          tma_load_2d(b_dst + t * B_BYTES, &bmap, &bar_b[st_idx], kb_t * BK, t * P.f_pad + f0);
+          tma_load_2d(b_dst + t * B_BYTES, &bmap, &bar_b[st_idx], kb_t * BK, G.row0 + t * G.f_pad + f0);
         b_step[st_idx] = step_t;
         b_pending[st_idx] = true;
       };
@@ -347,9 +395,9 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
     const int kh = ((warp - 1) >> 2) * 16;     // first of this warp's 16 columns of the block
     const int i = i0 + row;
     const uint32_t lane_off = (uint32_t)(32 * quarter) << 16;
-    const float* vt_b = P.vt + (int64_t)L * P.n_pad;                  // below the diagonal
-    const float* vt_a = P.vt + (int64_t)(P.L_max + 1 + L) * P.n_pad;  // above
-    const float* st = P.st + ((int64_t)L * P.n_iblk + iblk) * n_kb;
+    const float* vt_b = G.vt + (int64_t)L * G.n_pad;                  // below the diagonal
+    const float* vt_a = G.vt + (int64_t)(P.L_max + 1 + L) * G.n_pad;  // above
+    const float* st = G.st + ((int64_t)L * G.n_iblk + iblk) * n_kb;
     // column factors and block scale of a j block (rank-one blocks only), 16 columns per thread
     auto load_factors = [&](int kb_t, float4* v, float& sc) {
       const int kind = kind_of(kb_t);
@@ -389,11 +437,11 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
         for (int e = 0; e < 16; ++e) {
           const int j = j0 + kh + e;
           double kv = 0.0;
-          if (i < P.n_grid && j < P.n_grid) {
+          if (i < G.n_grid && j < G.n_grid) {
             if (i == j) {
               kv = P.diag[L] / ri;
             } else {
-              const double rj = P.r[j];
+              const double rj = G.r[j];
               const double rl = fmin(ri, rj), rg = fmax(ri, rj);
               const double inv = 1.0 / rg;
               double ratio = rl * inv, pw = 1.0;
@@ -451,9 +499,9 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
 #pragma unroll
       for (int c = 0; c < 32; ++c) {
         const int f = f0 + c0 + c;
-        if (f < P.n_forms && i < P.n_grid)
-          P.gpart[((int64_t)L * P.f_pad + f) * P.n_pad + i] =
-              ldexp((double)z[c], P.bexp[f]) * P.gw[(int64_t)f * P.n_Ltot + L];
+        if (f < G.n_forms && i < G.n_grid)
+          G.gpart[((int64_t)L * G.f_pad + f) * G.n_pad + i] =
+              ldexp((double)z[c], G.bexp[f]) * P.gw[(int64_t)f * P.n_Ltot + L];
       }
     }
   }
@@ -471,9 +519,9 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
         // a_f[i] of column f: the lanes of a warp read 32 consecutive rows of one form
         const int f = f0 + c0 + c;
         double av = 0.0;
-        if (f < P.n_forms) {
-          const dwba_form_t F = P.forms[f];
-          if (i < F.n_rows) av = ldexp(F.a_dev[i], P.bexp[f]);
+        if (f < G.n_forms) {
+          const dwba_form_t F = G.forms[f];
+          if (i < F.n_rows) av = ldexp(F.a_dev[i], G.bexp[f]);
         }
         double v = av * (double)z[c];
 #pragma unroll
@@ -487,7 +535,7 @@ tc_exchange_kernel(const __grid_constant__ CUtensorMap bmap, const GemmParams P)
   if (!GRAD && ok) {
     for (int c = tid; c < BN; c += THREADS) {
       const double v = sRed[0][c] + sRed[1][c] + sRed[2][c] + sRed[3][c];
-      P.partial[((int64_t)L * P.n_iblk + iblk) * P.f_pad + f0 + c] = v;
+      G.partial[((int64_t)L * G.n_iblk + iblk) * G.f_pad + f0 + c] = v;
     }
   }
   if (warp == 0) {
@@ -518,9 +566,10 @@ __global__ void tc_scale_kernel(const dwba_form_t* __restrict__ forms, int n_for
 
 // b_f -> NT bf16 terms in [NT][f_pad][n_pad] (zero padded): t_0 = bf16(b'), t_1 = bf16(b' - t_0), ...,
 // b' = 2^-e_f b_f
+// (ld: row stride of bterms, >= n_pad; columns n_pad .. ld-1 are not touched)
 template <int NT>
 __global__ void tc_prepare_kernel(const dwba_form_t* __restrict__ forms, int n_forms, int n_pad, int f_pad,
-                                  const int* __restrict__ bexp, __nv_bfloat16* __restrict__ bterms) {
+                                  const int* __restrict__ bexp, __nv_bfloat16* __restrict__ bterms, int64_t ld) {
   const int64_t total = (int64_t)f_pad * n_pad;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
     const int f = (int)(idx / n_pad), j = (int)(idx - (int64_t)f * n_pad);
@@ -534,7 +583,7 @@ __global__ void tc_prepare_kernel(const dwba_form_t* __restrict__ forms, int n_f
     for (int t = 0; t < NT; ++t) {
       const __nv_bfloat16 q = __float2bfloat16_rn(rem);
       rem -= __bfloat162float(q);
-      bterms[((int64_t)t * f_pad + f) * n_pad + j] = q;
+      bterms[((int64_t)t * f_pad + f) * ld + j] = q;
     }
   }
 }
@@ -624,6 +673,8 @@ __global__ void tc_grad_reduce_kernel(const double* __restrict__ gpart, const dw
 
 // bound of the pipeline waits of the next launches (process-wide; 0 = WAIT_CYCLES)
 std::atomic<long long> g_wait_cycles{0};
+// serialises the host-side assembly of the (large) segment tables of the launches
+std::mutex g_launch_mutex;
 
 long long wait_cycles() {
   const long long c = g_wait_cycles.load();
@@ -642,27 +693,66 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   return fn;
 }
 
-template <int NT, int BN, bool GRAD = false>
-int launch_tc(const GemmParams& P, const __nv_bfloat16* bterms, int n_L, cudaStream_t st) {
+// One launch over the segments of SG: B terms of every segment in one bf16 matrix of `ld` columns
+// and `rows` rows (one tensor map), `n_ctas` CTAs in total.
+template <int NT, int BN, bool GRAD = false, int SN = tc_stages(NT)>
+int launch_tc_segs(const GemmParams& P, const TcSegs& SG, const __nv_bfloat16* bterms, int64_t ld, int64_t rows,
+                   int64_t n_ctas, cudaStream_t st) {
+  if (n_ctas <= 0) return DWBA_OK;
+  if (n_ctas > 0x7fffffffLL) return DWBA_ERR_INVALID_ARG;
   auto encode = get_encode();
   if (!encode) return DWBA_ERR_CUDA;
   CUtensorMap map;
-  cuuint64_t dims[2] = {(cuuint64_t)P.n_pad, (cuuint64_t)NT * (cuuint64_t)P.f_pad};
-  cuuint64_t strides[1] = {(cuuint64_t)P.n_pad * 2};
+  cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
   cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BN};
   cuuint32_t estr[2] = {1, 1};
   CUresult cr = encode(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)bterms, dims, strides, box, estr,
                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) return DWBA_ERR_CUDA;
-  const int smem = tc_stages(NT) * NT * (BN * BK * 2) + 1024;
-  if (cudaFuncSetAttribute(tc_exchange_kernel<NT, BN, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+  const int smem = SN * NT * (BN * BK * 2) + 1024;
+  if (cudaFuncSetAttribute(tc_exchange_kernel<NT, BN, GRAD, SN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
       cudaSuccess)
     return DWBA_ERR_CUDA;
-  dim3 grid(P.n_iblk, P.f_pad / BN, n_L);
-  tc_exchange_kernel<NT, BN, GRAD><<<grid, THREADS, smem, st>>>(map, P);
+  tc_exchange_kernel<NT, BN, GRAD, SN><<<(unsigned)n_ctas, THREADS, smem, st>>>(map, P, SG);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;
+}
+
+// the one segment of a single-grid launch, from its parameters
+void single_segment(const GemmParams& P, int bn, int n_L, TcSegs& SG) {
+  SG.n = 1;
+  SG.order = 0;
+  TcSeg& g = SG.s[0];
+  g.r = P.r;
+  g.lg = P.lg;
+  g.forms = P.forms;
+  g.partial = P.partial;
+  g.bexp = P.bexp;
+  g.vt = P.vt;
+  g.st = P.st;
+  g.gpart = P.gpart;
+  g.n_grid = P.n_grid;
+  g.n_pad = P.n_pad;
+  g.f_pad = P.f_pad;
+  g.n_iblk = P.n_iblk;
+  g.n_forms = P.n_forms;
+  g.n_kb = P.n_kb;
+  g.row0 = 0;
+  g.n_fblk = P.f_pad / bn;
+  SG.cta0[0] = 0;
+  SG.cta0[1] = (int)((int64_t)P.n_iblk * g.n_fblk * n_L);
+}
+
+template <int NT, int BN, bool GRAD = false>
+int launch_tc(const GemmParams& P, const __nv_bfloat16* bterms, int n_L, cudaStream_t st) {
+  static TcSegs SG;  // ~10 KB: kept off the host stack (guarded by the launch mutex)
+  std::lock_guard<std::mutex> lock(g_launch_mutex);
+  const int64_t n_ctas = (int64_t)P.n_iblk * (P.f_pad / BN) * n_L;
+  if (n_ctas > 0x7fffffffLL) return DWBA_ERR_INVALID_ARG;
+  single_segment(P, BN, n_L, SG);
+  return launch_tc_segs<NT, BN, GRAD>(P, SG, bterms, P.n_pad, (int64_t)NT * P.f_pad, n_ctas, st);
 }
 
 }  // namespace
@@ -739,10 +829,10 @@ extern "C" int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, 
   }
   if (n_terms == 2)
     tc_prepare_kernel<2><<<dwba_grid_1d(total, 256, 65535), 256, 0, st>>>(forms_dev, n_forms, P.n_pad, P.f_pad,
-                                                                          bexp, bterms);
+                                                                          bexp, bterms, P.n_pad);
   else
     tc_prepare_kernel<3><<<dwba_grid_1d(total, 256, 65535), 256, 0, st>>>(forms_dev, n_forms, P.n_pad, P.f_pad,
-                                                                          bexp, bterms);
+                                                                          bexp, bterms, P.n_pad);
   DWBA_CHECK_LAUNCH();
   const int n_L = L_max + 1;
   int rc = n_terms == 2 ? launch_tc<2, TC_BN2>(P, bterms, n_L, st) : launch_tc<3, TC_BN3>(P, bterms, n_L, st);
@@ -753,10 +843,216 @@ extern "C" int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, 
   return DWBA_OK;
 }
 
-// ---- backward ------------------------------------------------------------------------
+// ---- ragged launch: forms on several grids in one tensor-core launch -----------------------
 namespace {
+
 int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
+
+struct SegLayout {
+  int n_grid, n_pad, f_pad, n_iblk, n_kb, n_forms, row0;
+  int64_t off_partial, off_bexp, off_lg, off_vt, off_st;
+};
+
+// default pipeline depth of a tile: the deepest that fits (tensor memory: bn + S NT 32 columns <= 512;
+// shared memory: S NT bn 128 bytes)
+int default_stages(int nt, int bn) { return nt == 2 ? (bn == 256 ? 3 : 4) : (bn == 256 ? 2 : 3); }
+
+bool valid_tile(int nt, int bn, int stages) {
+  if (bn != 128 && bn != 256) return false;
+  if (nt == 2) return (bn == 256 && stages == 3) || (bn == 128 && (stages == 3 || stages == 4));
+  return (bn == 256 && stages == 2) || (bn == 128 && (stages == 2 || stages == 3));
+}
+
+// the tile of a call (NULL: bn 256, default stages, row blocks fastest); false if invalid
+bool resolve_tile(const dwba_tc_tile_t* tile, int nt, int& bn, int& stages, int& order) {
+  bn = tile && tile->bn ? tile->bn : 256;
+  stages = tile && tile->stages ? tile->stages : default_stages(nt, bn);
+  order = tile ? tile->order : 0;
+  return valid_tile(nt, bn, stages) && (order == 0 || order == 1);
+}
+
+// workspace layout of a ragged call: the B terms of all segments as one [rows][ld] bf16 matrix,
+// then per segment its partials, exponents, log2 r and factor tables; returns the bytes (-1 if invalid)
+int64_t ragged_layout(const dwba_tc_segment_t* segs, int n, int L_max, int nt, int bn, SegLayout* lay,
+                      int64_t* ld_out, int64_t* rows_out) {
+  int64_t ld = BK, rows = 0;
+  for (int s = 0; s < n; ++s) {
+    if (segs[s].n_forms < 0 || segs[s].n_grid < 2 || segs[s].n_grid > (1 << 24)) return -1;
+    const int64_t n_pad = ((int64_t)segs[s].n_grid + BK - 1) / BK * BK;
+    ld = n_pad > ld ? n_pad : ld;
+  }
+  const int64_t nL = L_max + 1;
+  for (int s = 0; s < n; ++s) {
+    SegLayout L{};
+    L.n_grid = segs[s].n_grid;
+    L.n_forms = segs[s].n_forms;
+    L.n_pad = (L.n_grid + BK - 1) / BK * BK;
+    L.f_pad = (int)(((int64_t)L.n_forms + bn - 1) / bn * bn);
+    L.n_iblk = (L.n_grid + BM - 1) / BM;
+    L.n_kb = L.n_pad / BK;
+    L.row0 = (int)rows;
+    rows += (int64_t)nt * L.f_pad;
+    if (lay) lay[s] = L;
+  }
+  int64_t off = align256(rows * ld * 2);
+  for (int s = 0; s < n; ++s) {
+    const int64_t f_pad = ((int64_t)segs[s].n_forms + bn - 1) / bn * bn;
+    const int64_t n_pad = ((int64_t)segs[s].n_grid + BK - 1) / BK * BK;
+    const int64_t n_iblk = ((int64_t)segs[s].n_grid + BM - 1) / BM;
+    if (lay) lay[s].off_partial = off;
+    off += align256(nL * n_iblk * f_pad * 8);
+    if (lay) lay[s].off_bexp = off;
+    off += align256(f_pad * 4);
+    if (lay) lay[s].off_lg = off;
+    off += align256(n_pad * 8);
+    if (lay) lay[s].off_vt = off;
+    off += align256(2 * nL * n_pad * 4);
+    if (lay) lay[s].off_st = off;
+    off += align256(nL * n_iblk * (n_pad / BK) * 4);
+  }
+  if (rows > 0x7fffffffLL) return -1;
+  if (ld_out) *ld_out = ld;
+  if (rows_out) *rows_out = rows;
+  return off;
+}
+
+int launch_variant(int nt, int bn, int stages, const GemmParams& P, const TcSegs& SG, const __nv_bfloat16* bterms,
+                   int64_t ld, int64_t rows, int64_t n_ctas, cudaStream_t st) {
+  if (nt == 2) {
+    if (bn == 256) return launch_tc_segs<2, 256, false, 3>(P, SG, bterms, ld, rows, n_ctas, st);
+    if (stages == 3) return launch_tc_segs<2, 128, false, 3>(P, SG, bterms, ld, rows, n_ctas, st);
+    return launch_tc_segs<2, 128, false, 4>(P, SG, bterms, ld, rows, n_ctas, st);
+  }
+  if (bn == 256) return launch_tc_segs<3, 256, false, 2>(P, SG, bterms, ld, rows, n_ctas, st);
+  if (stages == 2) return launch_tc_segs<3, 128, false, 2>(P, SG, bterms, ld, rows, n_ctas, st);
+  return launch_tc_segs<3, 128, false, 3>(P, SG, bterms, ld, rows, n_ctas, st);
+}
+
 }  // namespace
+
+extern "C" int64_t dwba_tc_ragged_workspace_bytes(const dwba_tc_segment_t* segs_host, int n_segs, int L_max,
+                                                  int n_terms, const dwba_tc_tile_t* tile) {
+  if (!segs_host || n_segs < 0 || L_max < 0 || L_max > DWBA_MAX_L || (n_terms != 2 && n_terms != 3)) return -1;
+  int bn, stages, order;
+  if (!resolve_tile(tile, n_terms, bn, stages, order)) return -1;
+  return ragged_layout(segs_host, n_segs, L_max, n_terms, bn, nullptr, nullptr, nullptr);
+}
+
+extern "C" int dwba_bilinear_tc_bf16_ragged(const dwba_tc_segment_t* segs_host, int n_segs, int L_max, int n_terms,
+                                            const dwba_tc_tile_t* tile, const double* diag_scale_host,
+                                            void* workspace, int64_t workspace_bytes, int* status_dev,
+                                            dwba_stream_t stream) {
+  if (n_segs == 0) return DWBA_OK;
+  if (!segs_host || n_segs < 0 || !diag_scale_host || !workspace || !status_dev || L_max < 0 || L_max > DWBA_MAX_L ||
+      (n_terms != 2 && n_terms != 3))
+    return DWBA_ERR_INVALID_ARG;
+  int bn, stages, order;
+  if (!resolve_tile(tile, n_terms, bn, stages, order)) return DWBA_ERR_INVALID_ARG;
+  for (int s = 0; s < n_segs; ++s)
+    if (segs_host[s].n_forms > 0 && (!segs_host[s].forms_dev || !segs_host[s].r_dev || !segs_host[s].out_dev))
+      return DWBA_ERR_INVALID_ARG;
+  if (((uintptr_t)workspace & 255) != 0) return DWBA_ERR_INVALID_ARG;
+  std::vector<SegLayout> lay(n_segs);
+  int64_t ld = 0, rows = 0;
+  const int64_t need = ragged_layout(segs_host, n_segs, L_max, n_terms, bn, lay.data(), &ld, &rows);
+  if (need < 0) return DWBA_ERR_INVALID_ARG;
+  if (workspace_bytes < need) return DWBA_ERR_WORKSPACE;
+  uint8_t* ws = (uint8_t*)workspace;
+  __nv_bfloat16* bterms = (__nv_bfloat16*)ws;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n_L = L_max + 1;
+  // per segment: exponents, log2 r, factor tables, bf16 terms of b (rows row0 .. of the shared matrix)
+  for (int s = 0; s < n_segs; ++s) {
+    const dwba_tc_segment_t& G = segs_host[s];
+    const SegLayout& L = lay[s];
+    if (G.n_forms == 0) continue;
+    int* bexp = (int*)(ws + L.off_bexp);
+    double* lg = (double*)(ws + L.off_lg);
+    float* vt = (float*)(ws + L.off_vt);
+    float* stab = (float*)(ws + L.off_st);
+    tc_scale_kernel<<<G.n_forms, 256, 0, st>>>(G.forms_dev, G.n_forms, bexp);
+    DWBA_CHECK_LAUNCH();
+    tc_log2_kernel<<<dwba_grid_1d(G.n_grid, 256), 256, 0, st>>>(G.r_dev, G.n_grid, lg);
+    DWBA_CHECK_LAUNCH();
+    const int64_t n_fac = 2LL * n_L * L.n_pad + (int64_t)n_L * L.n_iblk * L.n_kb;
+    tc_factors_kernel<<<dwba_grid_1d(n_fac, 256, 65535), 256, 0, st>>>(lg, G.n_grid, L.n_pad, L.n_kb, L.n_iblk, n_L,
+                                                                       vt, stab);
+    DWBA_CHECK_LAUNCH();
+    const int64_t total = (int64_t)L.f_pad * L.n_pad;
+    __nv_bfloat16* bt = bterms + (int64_t)L.row0 * ld;
+    if (n_terms == 2)
+      tc_prepare_kernel<2><<<dwba_grid_1d(total, 256, 65535), 256, 0, st>>>(G.forms_dev, G.n_forms, L.n_pad, L.f_pad,
+                                                                            bexp, bt, ld);
+    else
+      tc_prepare_kernel<3><<<dwba_grid_1d(total, 256, 65535), 256, 0, st>>>(G.forms_dev, G.n_forms, L.n_pad, L.f_pad,
+                                                                            bexp, bt, ld);
+    DWBA_CHECK_LAUNCH();
+  }
+  // the tensor-core launches: segments by decreasing grid size (the longest CTAs start first), at
+  // most TC_MAX_SEGS per launch
+  std::vector<int> ord;
+  for (int s = 0; s < n_segs; ++s)
+    if (segs_host[s].n_forms > 0) ord.push_back(s);
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return segs_host[a].n_grid > segs_host[b].n_grid; });
+  GemmParams P{};
+  P.status = status_dev;
+  P.gw = nullptr;
+  P.gpart = nullptr;
+  P.wait_cycles = wait_cycles();
+  P.L_max = L_max;
+  P.n_Ltot = n_L;
+  for (int l = 0; l <= DWBA_MAX_L; ++l) P.diag[l] = l <= L_max ? diag_scale_host[l] : 0.0;
+  {
+    static TcSegs SG;  // ~10 KB: kept off the host stack (guarded by the launch mutex)
+    std::lock_guard<std::mutex> lock(g_launch_mutex);
+    for (size_t c0 = 0; c0 < ord.size(); c0 += TC_MAX_SEGS) {
+      const int m = (int)std::min<size_t>(TC_MAX_SEGS, ord.size() - c0);
+      SG.n = m;
+      SG.order = order;
+      int64_t ctas = 0;
+      for (int q = 0; q < m; ++q) {
+        const int s = ord[c0 + q];
+        const dwba_tc_segment_t& G = segs_host[s];
+        const SegLayout& L = lay[s];
+        TcSeg& g = SG.s[q];
+        g.r = G.r_dev;
+        g.lg = (const double*)(ws + L.off_lg);
+        g.forms = G.forms_dev;
+        g.partial = (double*)(ws + L.off_partial);
+        g.bexp = (const int*)(ws + L.off_bexp);
+        g.vt = (const float*)(ws + L.off_vt);
+        g.st = (const float*)(ws + L.off_st);
+        g.gpart = nullptr;
+        g.n_grid = L.n_grid;
+        g.n_pad = L.n_pad;
+        g.f_pad = L.f_pad;
+        g.n_iblk = L.n_iblk;
+        g.n_forms = L.n_forms;
+        g.n_kb = L.n_kb;
+        g.row0 = L.row0;
+        g.n_fblk = L.f_pad / bn;
+        SG.cta0[q] = (int)ctas;
+        ctas += (int64_t)L.n_iblk * g.n_fblk * n_L;
+        if (ctas > 0x7fffffffLL) return DWBA_ERR_INVALID_ARG;
+      }
+      SG.cta0[m] = (int)ctas;
+      const int rc = launch_variant(n_terms, bn, stages, P, SG, bterms, ld, rows, ctas, st);
+      if (rc != DWBA_OK) return rc;
+    }
+  }
+  // per segment: the partials summed in fixed order into the segment's results
+  for (int s = 0; s < n_segs; ++s) {
+    const dwba_tc_segment_t& G = segs_host[s];
+    const SegLayout& L = lay[s];
+    if (G.n_forms == 0) continue;
+    tc_reduce_kernel<<<dwba_grid_1d((int64_t)G.n_forms * n_L, 256), 256, 0, st>>>(
+        (const double*)(ws + L.off_partial), G.n_forms, L.f_pad, L.n_iblk, n_L, G.out_dev);
+    DWBA_CHECK_LAUNCH();
+  }
+  return DWBA_OK;
+}
+
+// ---- backward ------------------------------------------------------------------------
 
 extern "C" int64_t dwba_tc_backward_workspace_bytes(int n_forms, int n_grid, int L_max, int n_terms) {
   if (n_forms < 0 || n_grid < 2 || L_max < 0 || L_max > DWBA_MAX_L || (n_terms != 2 && n_terms != 3)) return -1;
@@ -838,10 +1134,10 @@ extern "C" int dwba_bilinear_tc_bf16_backward(const dwba_form_grad_t* forms_dev,
     DWBA_CHECK_LAUNCH();
     if (n_terms == 2)
       tc_prepare_kernel<2><<<dwba_grid_1d(total, 256, 65535), 256, 0, st>>>(fs, n_forms, P.n_pad, P.f_pad, bexp,
-                                                                            bterms);
+                                                                            bterms, P.n_pad);
     else
       tc_prepare_kernel<3><<<dwba_grid_1d(total, 256, 65535), 256, 0, st>>>(fs, n_forms, P.n_pad, P.f_pad, bexp,
-                                                                            bterms);
+                                                                            bterms, P.n_pad);
     DWBA_CHECK_LAUNCH();
     int rc = n_terms == 2 ? launch_tc<2, TC_BN2, true>(P, bterms, n_L, st)
                           : launch_tc<3, TC_BN3, true>(P, bterms, n_L, st);

@@ -349,7 +349,7 @@ def radial_ME_all_L_batch(grid, V_core_array, U_i_array, bound_i, bound_f,
 
 @_no_gc
 def radial_ME_all_L_sweep(points: Sequence[dict], L_max: int, engine: Optional[str] = None, graph: bool = False,
-                          replays: int = 0, **options):
+                          replays: int = 0, tile: Union[None, str, dict] = None, **options):
     """Many energy points in shared launches (new entry point; the reference loops over energies).
 
     ``points``: one dict per energy point with the arguments of ``radial_ME_all_L_batch``:
@@ -357,7 +357,10 @@ def radial_ME_all_L_sweep(points: Sequence[dict], L_max: int, engine: Optional[s
     sequences), ``pairs`` and optionally ``U_f_array``. Every point keeps its own grid (LOCAL
     adaptive grids of any size); all node sets, operand folds and bilinear forms of all points
     are evaluated in one launch each. With ``graph=True`` the launch sequence is captured once
-    in a CUDA graph and replayed (``replays`` extra replays, e.g. for timing).
+    in a CUDA graph and replayed (``replays`` extra replays, e.g. for timing). With a split-BF16
+    engine the exchange forms of all points go in one ragged tensor-core launch; ``tile`` chooses
+    its tile: None (the default), a dict(bn=, stages=, order=) or "auto" (timed per shape class by
+    ``tune.TILE_TUNER``, which records its choices).
     Returns, per point, what ``radial_ME_all_L_batch`` returns for it.
     """
     if not HAS_CUPY:
@@ -389,6 +392,12 @@ def radial_ME_all_L_sweep(points: Sequence[dict], L_max: int, engine: Optional[s
         _, mp = tune.TUNER.select(key, cands, build, lambda m: m.launch())
     else:
         mp = build(eng)
+    if mp.tc is not None and tile is not None:
+        if tile == "auto":
+            n_ex = int(mp.tc["n"])
+            tune.TILE_TUNER.select(tune.TILE_TUNER.key(mp.tc["nt"], mp.max_grid, n_ex, L_max), mp)
+        else:
+            mp.set_tile(tile)
     if graph:
         mp.capture()
         for _ in range(max(0, int(replays)) + 1):

@@ -438,17 +438,28 @@ class WaveMatrix:
                 groups.setdefault(id(rb[0]), [rb[0], [], []])
                 groups[id(rb[0])][1].append(i)
                 groups[id(rb[0])][2].append(rb[1])
+        big = []
         for base, idx, rows in groups.values():
             if len(idx) < 2 or 2 * len(set(rows)) < base.shape[0]:
                 continue  # a small share of a large matrix: per-row copies below
-            # the (small, synchronous) index copies first, so that the host does not wait for the
-            # large asynchronous copy of the matrix behind them
-            sel = torch.as_tensor(np.asarray(rows, dtype=np.int64), device=device)
-            dst = torch.as_tensor(np.asarray(idx, dtype=np.int64), device=device)
+            big.append((base, idx, rows))
+            done[idx] = True
+        # every small (synchronous) copy first -- the rows outside the grouped matrices and the
+        # index arrays of the gathers -- so that none of them waits behind a large asynchronous
+        # copy in the stream; the grouped matrices (asynchronous from pinned memory) last
+        self._copy_rows(out, done, N, n)
+        gathers = [(torch.as_tensor(np.asarray(rows, dtype=np.int64), device=device),
+                    torch.as_tensor(np.asarray(idx, dtype=np.int64), device=device), base) for base, idx, rows in big]
+        for sel, dst, base in gathers:
             src = torch.from_numpy(base)
             dev_base = src.to(device, non_blocking=src.is_pinned())
-            out[dst] = dev_base.index_select(0, sel)[:, :N]
-            done[idx] = True
+            out.index_copy_(0, dst, dev_base.index_select(0, sel)[:, :N])
+        self._uploaded[str(device)] = (n, out)
+        return out
+
+    def _copy_rows(self, out: torch.Tensor, done: np.ndarray, N: int, n: int) -> None:
+        """Rows not taken from a grouped matrix: consecutive ones in memory as one block, the others
+        one by one."""
         i = 0
         while i < n:
             if done[i]:
@@ -472,8 +483,6 @@ class WaveMatrix:
                 src = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).reshape(1, N)
             out[i:j].copy_(src, non_blocking=src.is_pinned())
             i = j
-        self._uploaded[str(device)] = (n, out)
-        return out
 
 
 @dataclass
@@ -1136,8 +1145,8 @@ class MultiPrepared:
     with shared launches: one node-set launch, one fold launch and one bilinear-form launch for
     all of them (every descriptor carries its own grid pointer and sizes). The launch sequence
     does no host synchronisation and no allocation, so it can be captured in a CUDA graph and
-    replayed (``capture()`` / ``replay()``). Tensor-core engines need one grid per launch and
-    launch their exchange forms per job."""
+    replayed (``capture()`` / ``replay()``). With the tensor-core engines the exchange forms of all
+    jobs go in one ragged tensor-core launch (one segment per grid)."""
 
     def __init__(self, parts: List[PreparedJob]):
         if not parts:
@@ -1201,15 +1210,15 @@ class MultiPrepared:
                     self.offsets[k] + p.direct_plan.ss_fo) for k, p in enumerate(parts)]
             self.form_launch = FormLaunch(ent, self.out, self.nl, dev)
         # tensor-core engines: the direct forms of every job in one exact launch sequence (each
-        # descriptor names its own grid); the exchange forms of all jobs on equal grids (e.g. the
-        # transitions of one energy) in one tensor-core launch, so that their forms share the
-        # 256-wide form tiles; those launches and the jobs' tails go round-robin (largest grid
-        # first) over side streams, so that the small grids of low-energy points run side by side
-        # instead of each leaving most SMs idle in its last wave. The jobs' result buffers become
-        # views of the shared ones (jobs of a MultiPrepared are launched through it only).
+        # descriptor names its own grid); the exchange forms of all jobs in ONE ragged tensor-core
+        # launch (one segment per distinct grid, so the transitions of an energy share the form
+        # tiles), then one accuracy guard over all of them; the jobs' tails go round-robin (largest
+        # grid first) over side streams forked from and joined back into the launching stream.
+        # The jobs' own direct / exchange output rows become views of the shared ones (jobs of a
+        # MultiPrepared are launched through it only).
         self.side_streams = []
         self.tc_order = []
-        self.tc_groups = []
+        self.tc = None
         if self.engine in TC_TERMS:
             nt = TC_TERMS[self.engine]
             self.side_streams = [torch.cuda.Stream(device=dev) for _ in range(min(4, len(parts)))]
@@ -1220,38 +1229,75 @@ class MultiPrepared:
             ent = [(p.forms_host, p.direct_plan, p.job.grid.N, _ptr(p.dg.r), d_off[k] + p.direct_plan.dot_fo // 2,
                     d_off[k] + p.direct_plan.ss_fo // 2) for k, p in enumerate(parts)]
             self.form_launch = FormLaunch(ent, self.tc_out_dir, self.nl, dev)
-            by_grid: Dict[tuple, List[int]] = {}
             off = 0
             for k, p in enumerate(parts):
                 n = p.T * p.P
                 p.out_dir = self.tc_out_dir[off:off + n]
                 off += n
+            by_grid: Dict[tuple, List[int]] = {}
+            for k, p in enumerate(parts):
                 r = np.ascontiguousarray(p.job.grid.r, dtype=np.float64)
                 by_grid.setdefault((len(r), hashlib.sha1(r.tobytes()).hexdigest()), []).append(k)
-            for ks in sorted(by_grid.values(), key=lambda v: -parts[v[0]].job.grid.N):
-                fe = np.concatenate([np.ascontiguousarray(parts[k].forms_host[1::2]) for k in ks])
-                N = parts[ks[0]].job.grid.N
-                ws = int(self.lib.dwba_tc_workspace_bytes(len(fe), N, self.L_max, nt))
-                if ws < 0:
-                    raise ValueError("invalid tensor-core form sizes")
-                grp = {"forms": _dev(fe.view(np.uint8), dev), "n": len(fe), "N": N, "r": parts[ks[0]].dg.r,
-                       "ws": torch.empty(max(ws, 256), dtype=torch.uint8, device=dev),
+            groups = sorted(by_grid.values(), key=lambda v: -parts[v[0]].job.grid.N)
+            order = [k for ks in groups for k in ks]  # the jobs' exchange forms, grouped by grid
+            fe = np.concatenate([np.ascontiguousarray(parts[k].forms_host[1::2]) for k in order])
+            n_ex = len(fe)
+            self.tc = {"forms": _dev(fe.view(np.uint8), dev), "n": n_ex, "nt": nt,
                        "status": torch.zeros(1, dtype=torch.int32, device=dev),
-                       "out": torch.empty((len(fe), self.nl), dtype=torch.float64, device=dev),
-                       "r_lo": float(parts[ks[0]].job.grid.r[0]), "r_hi": float(parts[ks[0]].job.grid.r[-1])}
-                # transition of each form across the group's jobs (the jobs' forms are transition-major)
-                gids = np.concatenate([g0 + np.repeat(np.arange(parts[k].T), parts[k].P)
-                                       for g0, k in zip(np.cumsum([0] + [parts[k].T for k in ks])[:-1], ks)])
-                grp["guard"] = TCGuard(grp["forms"], len(fe), self.nl, dev, gids, tc_route_fraction())
-                off = 0
-                for k in ks:
-                    p = parts[k]
-                    n = p.T * p.P
-                    p.out_ex = grp["out"][off:off + n]
-                    p.tc_status = grp["status"]
-                    p.tc_ws = None  # the group's workspace serves it
-                    off += n
-                self.tc_groups.append(grp)
+                       "out": torch.empty((n_ex, self.nl), dtype=torch.float64, device=dev)}
+            fbase, obase = _ptr(self.tc["forms"]), _ptr(self.tc["out"])
+            segs = np.zeros(len(groups), dtype=_lib.TC_SEGMENT_DTYPE)
+            f0 = 0
+            for q, ks in enumerate(groups):
+                n = int(sum(parts[k].T * parts[k].P for k in ks))
+                segs[q] = (fbase + f0 * _lib.FORM_DTYPE.itemsize, _ptr(parts[ks[0]].dg.r),
+                           obase + f0 * 8 * self.nl, n, parts[ks[0]].job.grid.N)
+                f0 += n
+            self.tc["segs"] = segs
+            self.set_tile(None)
+            off = 0
+            gids, g0 = [], 0
+            for k in order:
+                p = parts[k]
+                n = p.T * p.P
+                p.out_ex = self.tc["out"][off:off + n]
+                p.tc_status = self.tc["status"]
+                p.tc_ws = None  # the shared workspace serves it
+                off += n
+                gids.append(g0 + np.repeat(np.arange(p.T), p.P))  # transition of each form
+                g0 += p.T
+            self.tc["guard"] = TCGuard(self.tc["forms"], n_ex, self.nl, dev, np.concatenate(gids),
+                                       tc_route_fraction())
+            self.r_lo_tc = min(float(p.job.grid.r[0]) for p in parts)
+            self.r_hi_tc = max(float(p.job.grid.r[-1]) for p in parts)
+
+    def launch_tensor(self) -> None:
+        """The ragged tensor-core launch alone, on the current stream (for timing its tiles)."""
+        tc = self.tc
+        segs = tc["segs"]
+        _lib.check(self.lib.dwba_bilinear_tc_bf16_ragged(segs.ctypes.data, len(segs), self.L_max, tc["nt"],
+                                                         tc["tile"].ctypes.data, self.ds.ctypes.data, _ptr(tc["ws"]),
+                                                         tc["ws"].numel(), _ptr(tc["status"]), _stream()),
+                   "dwba_bilinear_tc_bf16_ragged")
+
+    def set_tile(self, tile: Optional[dict]) -> None:
+        """Tile of the ragged tensor-core launch: dict(bn=128|256, stages=..., order=0|1) or None for the
+        default; (re)sizes the shared workspace. Capture the graph again after a change."""
+        if self.tc is None:
+            return
+        t = np.zeros(1, dtype=_lib.TC_TILE_DTYPE)
+        if tile:
+            t["bn"], t["stages"], t["order"] = tile.get("bn", 0), tile.get("stages", 0), tile.get("order", 0)
+        segs = self.tc["segs"]
+        ws = int(self.lib.dwba_tc_ragged_workspace_bytes(segs.ctypes.data, len(segs), self.L_max, self.tc["nt"],
+                                                          t.ctypes.data))
+        if ws < 0:
+            raise ValueError(f"invalid tensor-core tile or form sizes: {tile}")
+        old = self.tc.get("ws")
+        if old is None or old.numel() < ws:
+            self.tc["ws"] = torch.empty(max(ws, 256), dtype=torch.uint8, device=self.parts[0].dg.device)
+        self.tc["tile"] = t
+        self.tile = dict(tile) if tile else None
 
     def launch(self, marks: Optional[list] = None) -> None:
         """The launch sequence. With ``marks`` (a list), a CUDA event is recorded on the stream after
@@ -1295,16 +1341,19 @@ class MultiPrepared:
                 for sd in self.side_streams:
                     sd.wait_stream(main)
                 if stage == "forms":
-                    # direct forms on the main stream, beside the tensor-core groups
+                    # direct forms on the main stream, beside the one ragged tensor-core launch (and
+                    # its guard) on a side stream
                     self.form_launch.launch(lib, self.L_max, self.ds, self.r_min, self.r_max)
-                    for q, g in enumerate(self.tc_groups):
-                        sd = self.side_streams[q % len(self.side_streams)]
-                        _lib.check(lib.dwba_bilinear_tc_bf16(_ptr(g["forms"]), g["n"], _ptr(g["r"]), g["N"], self.L_max,
-                                                             nt, self.ds.ctypes.data, _ptr(g["ws"]), g["ws"].numel(),
-                                                             _ptr(g["status"]), _ptr(g["out"]), int(sd.cuda_stream)),
-                                   "dwba_bilinear_tc_bf16")
-                        with torch.cuda.stream(sd):
-                            g["guard"].launch(lib, self.L_max, self.ds, g["r_lo"], g["r_hi"], g["out"])
+                    tc = self.tc
+                    sd = self.side_streams[0]
+                    segs = tc["segs"]
+                    _lib.check(lib.dwba_bilinear_tc_bf16_ragged(segs.ctypes.data, len(segs), self.L_max, nt,
+                                                                tc["tile"].ctypes.data, self.ds.ctypes.data,
+                                                                _ptr(tc["ws"]), tc["ws"].numel(), _ptr(tc["status"]),
+                                                                int(sd.cuda_stream)),
+                               "dwba_bilinear_tc_bf16_ragged")
+                    with torch.cuda.stream(sd):
+                        tc["guard"].launch(lib, self.L_max, self.ds, self.r_lo_tc, self.r_hi_tc, tc["out"])
                 else:
                     for q, k in enumerate(self.tc_order):
                         with torch.cuda.stream(self.side_streams[q % len(self.side_streams)]):

@@ -273,6 +273,38 @@ int dwba_bilinear_tc_bf16(const dwba_form_t* forms_dev, int n_forms, const doubl
                           int n_terms, const double* diag_scale_host, void* workspace, int64_t workspace_bytes,
                           int* status_dev, double* out_dev, dwba_stream_t stream);
 
+/* The split-BF16 form over forms on several grids in one tensor-core launch (energy points of a
+ * sweep, each with its own grid; the per-energy loop of driver.py:907-1029 as one launch). Each
+ * segment: its forms (all on its r_dev, n_grid points) and its result array out_dev
+ * ((n_forms, L_max+1) doubles). The results of a segment are bit-identical to
+ * dwba_bilinear_tc_bf16 on that segment alone, for every tile. tile (NULL: the default):
+ *   bn     forms per CTA, 128 or 256 (0: 256);
+ *   stages pipeline depth (0: the deepest that fits): n_terms 2: bn 256 -> 3, bn 128 -> 3 or 4;
+ *          n_terms 3: bn 256 -> 2, bn 128 -> 2 or 3;
+ *   order  0: the CTAs of a segment run its row blocks fastest, 1: its form blocks fastest.
+ * Segments run largest grid first. workspace: dwba_tc_ragged_workspace_bytes(...) bytes,
+ * 256-byte aligned. status_dev as for dwba_bilinear_tc_bf16. */
+typedef struct {
+  const dwba_form_t* forms_dev;
+  const double* r_dev;
+  double* out_dev;
+  int32_t n_forms;
+  int32_t n_grid;
+} dwba_tc_segment_t;
+
+typedef struct {
+  int32_t bn;
+  int32_t stages;
+  int32_t order;
+  int32_t pad;
+} dwba_tc_tile_t;
+
+int64_t dwba_tc_ragged_workspace_bytes(const dwba_tc_segment_t* segs_host, int n_segs, int L_max, int n_terms,
+                                       const dwba_tc_tile_t* tile);
+int dwba_bilinear_tc_bf16_ragged(const dwba_tc_segment_t* segs_host, int n_segs, int L_max, int n_terms,
+                                 const dwba_tc_tile_t* tile, const double* diag_scale_host, void* workspace,
+                                 int64_t workspace_bytes, int* status_dev, dwba_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Host helpers (no GPU work)
  * ------------------------------------------------------------------------- */
@@ -326,7 +358,8 @@ int dwba_bilinear_tc_bf16_backward(const dwba_form_grad_t* forms_dev, int n_form
                                    int L_max, int n_terms, const double* diag_scale_host, const double* grad_dev,
                                    void* workspace, int64_t workspace_bytes, int* status_dev, dwba_stream_t stream);
 
-/* Bound of every pipeline wait of the tensor-core kernels (dwba_bilinear_tc_bf16 and its backward)
+/* Bound of every pipeline wait of the tensor-core kernels (dwba_bilinear_tc_bf16, its ragged form
+ * and its backward)
  * launched after this call, in SM clock cycles; 0 restores the default (about one second). No
  * reference counterpart: it lets a test make a wait run out on a normal input. A wait that runs
  * out sets the call's status word to 2; its CTA then waits, with the default bound, for its own
@@ -382,8 +415,8 @@ const char* dwba_status_string(int status);
 int dwba_device_probe(int* n_devices, int* cc_major, int* cc_minor);
 /* sizeof(dwba_nodeset_t), sizeof(dwba_fold_t), sizeof(dwba_form_t), sizeof(dwba_tail_t),
  * sizeof(dwba_form_grad_t), sizeof(dwba_fold_adj_t), sizeof(dwba_fold_multi_t),
- * sizeof(dwba_potential_t), sizeof(dwba_dot_t), sizeof(dwba_cupy_set_t), sizeof(dwba_cupy_form_t) into
- * sizes[0..10] (the first n of them). */
+ * sizeof(dwba_potential_t), sizeof(dwba_dot_t), sizeof(dwba_cupy_set_t), sizeof(dwba_cupy_form_t),
+ * sizeof(dwba_tc_segment_t), sizeof(dwba_tc_tile_t) into sizes[0..12] (the first n of them). */
 int dwba_struct_sizes(int64_t* sizes, int n);
 
 #ifdef __cplusplus

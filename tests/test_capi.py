@@ -27,12 +27,13 @@ def test_library_exports_every_declared_symbol():
 def test_abi_version_and_struct_layout():
     lib = _lib.load()
     assert lib.dwba_abi_version() == 1
-    sizes = (ctypes.c_int64 * 11)()
-    assert lib.dwba_struct_sizes(sizes, 11) == 0
+    sizes = (ctypes.c_int64 * 13)()
+    assert lib.dwba_struct_sizes(sizes, 13) == 0
     assert tuple(sizes) == (_lib.NODESET_DTYPE.itemsize, _lib.FOLD_DTYPE.itemsize, _lib.FORM_DTYPE.itemsize,
                             _lib.TAIL_DTYPE.itemsize, _lib.FORM_GRAD_DTYPE.itemsize, _lib.FOLD_ADJ_DTYPE.itemsize,
                             _lib.FOLD_MULTI_DTYPE.itemsize, _lib.POTENTIAL_DTYPE.itemsize, _lib.DOT_DTYPE.itemsize,
-                            _lib.CUPY_SET_DTYPE.itemsize, _lib.CUPY_FORM_DTYPE.itemsize)
+                            _lib.CUPY_SET_DTYPE.itemsize, _lib.CUPY_FORM_DTYPE.itemsize,
+                            _lib.TC_SEGMENT_DTYPE.itemsize, _lib.TC_TILE_DTYPE.itemsize)
 
 
 def test_status_strings():
@@ -74,3 +75,36 @@ def test_tensor_core_backward_host_checks():
                                               None) == _lib.DWBA_ERR_INVALID_ARG
     assert lib.dwba_bilinear_tc_bf16_backward(None, 0, None, 3001, 6, 2, ds.ctypes.data, None, None, 0, None,
                                               None) == _lib.DWBA_OK  # nothing to do
+
+
+def test_ragged_tensor_core_host_checks():
+    """Workspace of the ragged split-BF16 launch: the segments' B terms share one matrix as wide as
+    the largest grid, then each segment's tables; invalid tiles and sizes are rejected on the host."""
+    lib = _lib.load()
+    segs = np.zeros(3, dtype=_lib.TC_SEGMENT_DTYPE)
+    segs["n_forms"] = [300, 0, 1000]
+    segs["n_grid"] = [2000, 5000, 15000]
+    tile = np.zeros(1, dtype=_lib.TC_TILE_DTYPE)
+
+    def ws(bn=0, stages=0, order=0, nt=2, L=6, s=segs):
+        tile["bn"], tile["stages"], tile["order"] = bn, stages, order
+        return lib.dwba_tc_ragged_workspace_bytes(s.ctypes.data, len(s), L, nt, tile.ctypes.data)
+    base = ws()
+    assert base > 0 and base % 256 == 0
+    # the B terms alone: 2 terms x (300 + 1000 forms padded to 256) rows x 15040 columns of bf16
+    assert base >= 2 * (512 + 1024) * 15040 * 2
+    assert lib.dwba_tc_ragged_workspace_bytes(segs.ctypes.data, 3, 6, 2, None) == base  # NULL tile = default
+    assert ws(bn=128) < base  # less padding of the form blocks
+    assert ws(bn=128, stages=4) == ws(bn=128, stages=3)  # the depth does not change the workspace
+    for bad in (dict(bn=64), dict(bn=256, stages=4), dict(bn=256, stages=2), dict(order=2),
+                dict(nt=3, bn=256, stages=3), dict(nt=4)):
+        assert ws(**bad) == -1, bad
+    assert ws(nt=3, bn=256, stages=2) > 0 and ws(nt=3, bn=128, stages=3) > 0
+    short = segs.copy()
+    short["n_grid"][0] = 1
+    assert ws(s=short) == -1
+    ds = np.ones(7)
+    assert lib.dwba_bilinear_tc_bf16_ragged(segs.ctypes.data, 3, 6, 2, None, ds.ctypes.data, None, 0, None,
+                                            None) == _lib.DWBA_ERR_INVALID_ARG
+    assert lib.dwba_bilinear_tc_bf16_ragged(segs.ctypes.data, 0, 6, 2, None, ds.ctypes.data, None, 0, None,
+                                            None) == _lib.DWBA_OK  # nothing to do

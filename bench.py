@@ -175,6 +175,13 @@ def ragged_sweep(engine, L_max=6, replays=5, n_energy=64, points=None, split=Tru
                         L_max, pt["U_f_array"], kw, cache)
         parts.append(PreparedJob(job, cache.dg, engine, rebuild_nodesets=True))
     mp = MultiPrepared(parts)
+    tile = None
+    if mp.tc is not None:
+        # the ragged tensor-core launch's tile, chosen by the tuner (median of repeated launches)
+        from dwba_b200 import tune
+        key = tune.TILE_TUNER.key(mp.tc["nt"], mp.max_grid, int(mp.tc["n"]), L_max)
+        tile = {"choice": tune._tile_name(tune.TILE_TUNER.select(key, mp)),
+                "timings_ms": tune.TILE_TUNER.timings_ms[key]}
     mp.capture()
     mp.replay()
     torch.cuda.synchronize()
@@ -218,7 +225,7 @@ def ragged_sweep(engine, L_max=6, replays=5, n_energy=64, points=None, split=Tru
             "integrals": n_int, "ms_per_sweep": ms, "ms_per_energy": ms / n_energy,
             "integrals_per_s": n_int / (ms * 1e-3), "graph": True, "replays": replays,
             "split_ms": stages, "split_algorithmic_gbs": gbs, "tail_records": n_tail,
-            "tc_guard_routed": routed, "results_finite": bool(finite)}, outs
+            "tc_guard_routed": routed, "tc_tile": tile, "results_finite": bool(finite)}, outs
 
 
 def sweep_tcs_errors(points, ref, test, L_max=6):
@@ -824,7 +831,7 @@ def main():
     # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu capture of
     # the default workload (profiles/launches_semisep_synthetic_batch_N15000.md); other sizes: null
     default_size = args.n_cont == N_CONT
-    traffic = {"nodeset_rows_kernel": 1.929e9, "fold_kernel": 4.654e9}
+    traffic: dict = {}
 
     def hbm_roof(kernel, nbytes, t_ms, note):
         ach = nbytes / (t_ms * 1e-3) / 1e9
@@ -833,9 +840,10 @@ def main():
                 "algorithmic_bytes": nbytes, "peak_source": peak_src, "note": note}
     kernels = [
         hbm_roof("nodeset_rows_kernel", sum(p.nodesets.algorithmic_bytes() for p in preps), split["nodesets_ms"],
-                 "algorithmic bytes = 8*(3*n1 + 5*N) operator doubles written + 8*2*N grid doubles read per "
-                 "node set; the kernel is issue/latency bound (per-row loops over the CC nodes, FP64 log "
-                 "per node visit)"),
+                 "algorithmic bytes = per node set 8*2*N grid doubles read, plus 8*(3*n1 + 5*N) operator "
+                 "doubles written when stored, or (sets serving one pair, applied at once to its folds) each "
+                 "folded function read once and every fold output written; the kernel is issue/latency bound "
+                 "(per-row loops over the CC nodes)"),
         hbm_roof("fold_kernel", sum(p.fold_bytes() for p in preps), split["folds_ms"],
                  "algorithmic bytes = every distinct operand array (band operators, continuum waves, bound "
                  "states) read once over its longest use + every output written"),
@@ -962,7 +970,7 @@ def main():
                 "split_bf16_vs_plain_fp64_speedup": r_dense["ms_per_sweep"] / r_x3["ms_per_sweep"],
                 "semisep_fp64_vs_plain_fp64_speedup": r_dense["ms_per_sweep"] / ragged["ms_per_sweep"],
                 "tc_bf16x3_tcs_rel_err_max": worst, "tc_bf16x3_tcs_rel_err_median": med,
-                "tc_bf16x3_guard_routed": r_x3.get("tc_guard_routed"),
+                "tc_bf16x3_guard_routed": r_x3.get("tc_guard_routed"), "tc_bf16x3_tile": r_x3.get("tc_tile"),
                 "dense_fp64_tcs_rel_err_max": worst_d,
                 "note": "TCS of every (energy, transition) point from each engine's integrals against the exact "
                         "FP64 semiseparable engine's (which agrees with the oracle to 1e-12 per integral)"}
@@ -985,7 +993,8 @@ def main():
             pass
     if rank == 0:
         per_forms = {"dense": 2, "semisep": 1, "tc_bf16x3": 5, "tc_bf16x6": 5}[args.engine]
-        n_launch = sum((1 if p.nodesets.n else 0) + (p.n_folds + 65534) // 65535 + (p.n_multi + 65534) // 65535 +
+        n_launch = sum((1 if p.nodesets.n else 0) + (1 if p.nodesets.n_fused else 0) + (p.n_folds + 65534) // 65535 +
+                       (p.n_multi + 65534) // 65535 +
                        per_forms for p in preps)
         line = {"metric": METRIC, "value": value, "unit": "integrals/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",

@@ -69,6 +69,7 @@ def _declare(lib):
         "dwba_device_probe": (c_int, [ctypes.POINTER(c_int)] * 3),
         "dwba_struct_sizes": (c_int, [ctypes.POINTER(c_i64), c_int]),
         "dwba_build_nodesets": (c_int, [c_vp, c_int, c_int, c_vp, c_vp, c_int, c_vp, c_vp]),
+        "dwba_build_nodesets_folded": (c_int, [c_vp, c_vp, c_int, c_int, c_vp, c_vp, c_int, c_vp, c_vp]),
         "dwba_fold": (c_int, [c_vp, c_int, c_int, c_vp]),
         "dwba_dense_chunk_prefix": (c_i64, [c_vp, c_int, c_vp]),
         "dwba_bilinear_dense_fp64": (c_int, [c_vp, c_int, c_int, c_vp, c_vp, c_i64, c_vp, c_i64, c_vp, c_vp]),

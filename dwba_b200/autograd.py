@@ -192,7 +192,8 @@ class RadialIntegrals:
         job.tails_per_unit_moment = True
         plans = plan_job(job)
         state = _State()
-        state.prepared = PreparedJob(job, self.cache.dg, self.engine, plans=plans)
+        # the backward applies the transposed node-set operators, so they must be stored (not fused)
+        state.prepared = PreparedJob(job, self.cache.dg, self.engine, plans=plans, fuse_folds=False)
         state.backward = self.backward
         I = _BilinearFn.apply(chi_i, chi_f, u_i, u_f, state)
         dev = chi_i.device

@@ -70,11 +70,44 @@ constexpr int OWN_ROWS = 30;
 #ifndef DWBA_NODESET_MIN_BLOCKS
 #define DWBA_NODESET_MIN_BLOCKS 24
 #endif
-template <int NCC>  // CC nodes per interval known at compile time (0: n_cc at run time)
+// FOLD = true: the operators are not stored; each row applies them at once to the two multi-folds
+// of its set (folds[2 set] with the tridiagonal T, folds[2 set + 1] with the band B), with the
+// arithmetic of fold_multi_kernel, and writes the folded operands instead.
+template <int H>
+__device__ __forceinline__ void fold_row_from_taps(const dwba_fold_multi_t* __restrict__ m, int i, const double* tap) {
+  if (i >= m->n_clear) return;
+  const int n_f = m->n_f, n_src = m->n_src;
+  if (i >= m->n_out) {
+    for (int t = 0; t < n_f; ++t) m->out_dev[t][i] = 0.0;
+    return;
+  }
+  const double* __restrict__ g = m->g_dev;
+  double tp[2 * H + 1], gv[2 * H + 1];
+#pragma unroll
+  for (int d = -H; d <= H; ++d) {
+    const int k = i + d;
+    const bool in = k >= 0 && k < n_src;
+    tp[d + H] = in ? tap[d + H] : 0.0;
+    gv[d + H] = in ? g[k] : 0.0;
+  }
+  for (int t = 0; t < n_f; ++t) {
+    const double* __restrict__ f = m->f_dev[t];
+    double acc = 0.0;
+#pragma unroll
+    for (int d = -H; d <= H; ++d) {
+      const int k = i + d;
+      if (k >= 0 && k < n_src) acc += tp[d + H] * (f[k] * gv[d + H]);
+    }
+    m->out_dev[t][i] = acc;
+  }
+}
+
+template <int NCC, bool FOLD>  // NCC: CC nodes per interval known at compile time (0: n_cc at run time)
 __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets,
                                                               const double* __restrict__ ccx_g,
                                                               const double* __restrict__ ccw_g, int n_cc_rt,
-                                                              int* status) {
+                                                              int* status,
+                                                              const dwba_fold_multi_t* __restrict__ folds) {
   __shared__ double ccw[MAX_CC], ccx1[MAX_CC];
   const int n_cc = NCC > 0 ? NCC : n_cc_rt;
   if (threadIdx.x < n_cc) {
@@ -243,17 +276,31 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
     const double q_b1 = __shfl_up_sync(0xffffffffu, x_b1, 1), q_b2 = __shfl_up_sync(0xffffffffu, x_b2, 1);
     const double q_b3 = __shfl_up_sync(0xffffffffu, x_b3, 1);
     if (lane >= 2 && g < N) {
-      if (g < n1) {
-        d.ta_dev[3 * g + 0] = p_lo + q_lo;  // from nodes below r_g only
-        d.ta_dev[3 * g + 1] = (p_di + q_di) + o_di;
-        d.ta_dev[3 * g + 2] = q_up + o_up;
+      const double t0 = p_lo + q_lo;  // from nodes below r_g only
+      const double t1 = (p_di + q_di) + o_di;
+      const double t2 = q_up + o_up;
+      const double b1 = q_b1, b2 = q_b2 + o_b2, b3 = q_b3 + o_b3, b4 = o_b4;
+      if (FOLD) {
+        const dwba_fold_multi_t* mt = folds + 2 * (int64_t)blockIdx.y;
+        if (g < n1) {
+          const double tt[3] = {t0, t1, t2};
+          fold_row_from_taps<1>(mt, g, tt);
+        }
+        const double bb[5] = {0.0, b1, b2, b3, b4};
+        fold_row_from_taps<2>(mt + 1, g, bb);
+      } else {
+        if (g < n1) {
+          d.ta_dev[3 * g + 0] = t0;
+          d.ta_dev[3 * g + 1] = t1;
+          d.ta_dev[3 * g + 2] = t2;
+        }
+        double* bx = d.bx_dev + 5 * (int64_t)g;
+        bx[0] = 0.0;
+        bx[1] = b1;
+        bx[2] = b2;
+        bx[3] = b3;
+        bx[4] = b4;
       }
-      double* bx = d.bx_dev + 5 * (int64_t)g;
-      bx[0] = 0.0;
-      bx[1] = q_b1;
-      bx[2] = q_b2 + o_b2;
-      bx[3] = q_b3 + o_b3;
-      bx[4] = o_b4;
     }
     if (bad) atomicExch(status, 1);
   }
@@ -273,9 +320,31 @@ extern "C" int dwba_build_nodesets(const dwba_nodeset_t* sets_dev, int n_sets, i
   const int fill = (int)(((int64_t)148 * 24 * DWBA_NODESET_FILL + n_sets - 1) / n_sets);
   dim3 grid(need < fill ? need : fill, n_sets);
   if (n_cc == 5)
-    nodeset_rows_kernel<5><<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc, status_dev);
+    nodeset_rows_kernel<5, false><<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc,
+                                                                         status_dev, nullptr);
   else
-    nodeset_rows_kernel<0><<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc, status_dev);
+    nodeset_rows_kernel<0, false><<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc,
+                                                                         status_dev, nullptr);
+  DWBA_CHECK_LAUNCH();
+  return DWBA_OK;
+}
+
+extern "C" int dwba_build_nodesets_folded(const dwba_nodeset_t* sets_dev, const dwba_fold_multi_t* folds_dev,
+                                          int n_sets, int max_grid, const double* cc_x_dev, const double* cc_w_dev,
+                                          int n_cc, int* status_dev, dwba_stream_t stream) {
+  if (n_sets <= 0) return DWBA_OK;
+  if (!sets_dev || !folds_dev || !cc_x_dev || !cc_w_dev || !status_dev || n_cc < 2 || n_cc > MAX_CC ||
+      max_grid < 2 || n_sets > 65535)
+    return DWBA_ERR_INVALID_ARG;
+  const int need = (max_grid + OWN_ROWS - 1) / OWN_ROWS;
+  const int fill = (int)(((int64_t)148 * 24 * DWBA_NODESET_FILL + n_sets - 1) / n_sets);
+  dim3 grid(need < fill ? need : fill, n_sets);
+  if (n_cc == 5)
+    nodeset_rows_kernel<5, true><<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc,
+                                                                        status_dev, folds_dev);
+  else
+    nodeset_rows_kernel<0, true><<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc,
+                                                                        status_dev, folds_dev);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;
 }

@@ -151,23 +151,57 @@ class CCTables:
 
 
 class NodeSetBatch:
-    """Descriptors of the node sets a job uses; ``launch()`` (re)builds their banded operators."""
+    """Descriptors of the node sets a job uses; ``launch()`` (re)builds their banded operators.
 
-    def __init__(self, dg: DeviceGrid, plans: Sequence[NodeSetPlan], n_cc: int, rebuild: bool = False):
+    ``fused`` (a mask over ``plans``): sets whose operators are applied at once to their pair's
+    multi-folds (``dwba_build_nodesets_folded``) instead of being stored: they get no operator
+    memory, are not cached, and launch with the fold descriptors given by ``set_fused_folds``."""
+
+    def __init__(self, dg: DeviceGrid, plans: Sequence[NodeSetPlan], n_cc: int, rebuild: bool = False,
+                 fused: Optional[np.ndarray] = None):
         self.dg, self.n_cc = dg, n_cc
         dev = dg.device
         N = dg.info.N
         cache = dg.nodesets
         plans = list(plans)
+        fused = np.zeros(len(plans), dtype=bool) if fused is None else np.asarray(fused, dtype=bool)
+        self.fused_idx = np.nonzero(fused)[0]
+        self.n_fused = len(self.fused_idx)
+        self.fused_recs = None
+        self.fused_folds_d = None
+        if self.n_fused:
+            fp = [plans[i] for i in self.fused_idx]
+            fr = np.zeros(self.n_fused, dtype=_lib.NODESET_DTYPE)
+            fr["r"], fr["logr"] = _ptr(dg.r), _ptr(dg.logr)
+            fr["n_grid"], fr["n1"] = N, [p.key.n1 for p in fp]
+            fr["n_breaks"] = [p.n_breaks for p in fp]
+            fr["log1"] = [int(p.log1) for p in fp]
+            fr["log2"] = [int(p.log2) for p in fp]
+            self._fused_breaks = [p.breaks for p in fp]
+            if any(b is not None for b in self._fused_breaks):
+                br_len = np.array([0 if b is None else len(b) for b in self._fused_breaks], dtype=np.int64)
+                self._fused_br = _dev(np.concatenate([np.asarray(b, dtype=np.float64) for b in self._fused_breaks
+                                                      if b is not None]), dev)
+                off = np.concatenate([[0], np.cumsum(br_len)[:-1]])
+                has = br_len > 0
+                fr["breaks"][has] = np.uint64(_ptr(self._fused_br)) + np.uint64(8) * off[has].astype(np.uint64)
+            self.fused_recs = fr
+            self.fused_recs_d = _dev(fr.view(np.uint8), dev)
+            self.fccx, self.fccw = CCTables.get(n_cc, dev)
+            self.fused_status = torch.zeros(1, dtype=torch.int32, device=dev)
+        plans = [p for i, p in enumerate(plans) if not fused[i]]
+        keep = np.nonzero(~fused)[0]
         cached = [cache.get(p.key) for p in plans]
         todo = plans if rebuild else [p for p, c in zip(plans, cached) if c is None]
         self.n = len(todo)
-        # operator addresses of every planned set, in the plans' order (and a 0 for "no set")
-        self.ta_all = np.zeros(len(plans) + 1, dtype=np.uint64)
-        self.bx_all = np.zeros(len(plans) + 1, dtype=np.uint64)
+        # operator addresses of every planned set, in the plans' order (and a 0 for "no set"); the
+        # fused sets have none
+        self.ta_all = np.zeros(len(fused) + 1, dtype=np.uint64)
+        self.bx_all = np.zeros(len(fused) + 1, dtype=np.uint64)
+        self._keep = keep
         if not todo:
-            self.ta_all[:-1] = [c.ta_ptr for c in cached]
-            self.bx_all[:-1] = [c.bx_ptr for c in cached]
+            self.ta_all[keep] = [c.ta_ptr for c in cached]
+            self.bx_all[keep] = [c.bx_ptr for c in cached]
             return
         self.ccx, self.ccw = CCTables.get(n_cc, dev)
         n = len(todo)
@@ -204,12 +238,13 @@ class NodeSetBatch:
             ta_p[old] = [cached[i].ta_ptr for i in old]
             bx_p[old] = [cached[i].bx_ptr for i in old]
         if rebuild:
-            self.ta_all[:-1], self.bx_all[:-1] = ta_p, bx_p
+            self.ta_all[keep], self.bx_all[keep] = ta_p, bx_p
         else:
             done = {id(p): i for i, p in enumerate(todo)}
             for j, (p, c) in enumerate(zip(plans, cached)):
                 k = done.get(id(p))
-                self.ta_all[j], self.bx_all[j] = (ta_p[k], bx_p[k]) if k is not None else (c.ta_ptr, c.bx_ptr)
+                self.ta_all[keep[j]], self.bx_all[keep[j]] = (ta_p[k], bx_p[k]) if k is not None else \
+                    (c.ta_ptr, c.bx_ptr)
         recs = np.zeros(n, dtype=_lib.NODESET_DTYPE)
         recs["r"], recs["logr"] = _ptr(dg.r), _ptr(dg.logr)
         recs["breaks"], recs["ta"], recs["bx"] = br_p, ta_p, bx_p
@@ -221,17 +256,25 @@ class NodeSetBatch:
         self.recs_d = _dev(recs.view(np.uint8), dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
 
+    def set_fused_folds(self, folds: np.ndarray) -> None:
+        """The two multi-folds (T, then B) of every fused set, in the order of ``fused_idx``."""
+        assert len(folds) == 2 * self.n_fused
+        self.fused_folds = folds
+        self.fused_folds_d = _dev(folds.view(np.uint8), self.dg.device) if len(folds) else None
+
     def algorithmic_bytes(self) -> float:
         """Bytes a build must move: the operators written (3 n1 + 5 N doubles per set) and the grid
-        read (r and log r, 2 N doubles per set)."""
-        if self.n == 0:
-            return 0.0
+        read (r and log r, 2 N doubles per set); a fused set writes no operators but reads its
+        folds' functions and writes their outputs (``fold_bytes`` of its multi-folds)."""
         N = float(self.dg.info.N)
-        return float(np.sum(8.0 * (3.0 * self.recs["n1"].astype(np.float64) + 7.0 * N)))
+        b = 0.0
+        if self.n:
+            b += float(np.sum(8.0 * (3.0 * self.recs["n1"].astype(np.float64) + 7.0 * N)))
+        if self.n_fused:
+            b += self.n_fused * 8.0 * 2.0 * N + fused_fold_bytes(self.fused_folds)
+        return b
 
     def launch(self) -> None:
-        if self.n == 0:
-            return
         lib = _lib.load()
         N = self.dg.info.N
         for s0 in range(0, self.n, 65535):
@@ -239,10 +282,35 @@ class NodeSetBatch:
             _lib.check(lib.dwba_build_nodesets(_ptr(self.recs_d) + s0 * _lib.NODESET_DTYPE.itemsize, n, N,
                                                _ptr(self.ccx), _ptr(self.ccw), self.n_cc, _ptr(self.status),
                                                _stream()), "dwba_build_nodesets")
+        for s0 in range(0, self.n_fused, 65535):
+            n = min(65535, self.n_fused - s0)
+            _lib.check(lib.dwba_build_nodesets_folded(_ptr(self.fused_recs_d) + s0 * _lib.NODESET_DTYPE.itemsize,
+                                                      _ptr(self.fused_folds_d) + 2 * s0 * _lib.FOLD_MULTI_DTYPE.itemsize,
+                                                      n, N, _ptr(self.fccx), _ptr(self.fccw), self.n_cc,
+                                                      _ptr(self.fused_status), _stream()),
+                       "dwba_build_nodesets_folded")
 
     def check(self) -> None:
         if self.n and int(self.status.item()) != 0:
             raise _lib.DWBAError(_lib.DWBA_ERR_RANGE, "dwba_build_nodesets")
+        if self.n_fused and int(self.fused_status.item()) != 0:
+            raise _lib.DWBAError(_lib.DWBA_ERR_RANGE, "dwba_build_nodesets_folded")
+
+
+def fused_fold_bytes(folds: np.ndarray) -> float:
+    """Bytes the multi-folds of fused node sets move: each distinct function read once over its
+    longest use and every output written."""
+    if folds is None or not len(folds):
+        return 0.0
+    reads: Dict[int, float] = {}
+    writes = 0.0
+    for m in folds:
+        n_src = float(m["n_src"])
+        for p_ in [int(m["g"])] + [int(x) for x in m["f"][:m["n_f"]]]:
+            if p_ and n_src > reads.get(p_, 0.0):
+                reads[p_] = n_src
+        writes += float(m["n_clear"]) * int(m["n_f"])
+    return 8.0 * (sum(reads.values()) + writes)
 
 
 @dataclass
@@ -785,6 +853,33 @@ class FormLaunch:
         return b
 
 
+FUSE_MIN_SETS = 64  # fuse node sets with their folds when a job has at least this many single-pair sets
+
+
+def fusable_sets(plans: "JobPlan", T: int) -> Optional[np.ndarray]:
+    """Mask over ``plans.nodesets``: the sets whose every use is one pair's phase-split entries with at
+    most FOLD_MULTI - 1 transitions (one multi-fold group per operator), or None if a set has other
+    uses. Such a set is applied to its pair's folds at once instead of being stored -- worthwhile when
+    many distinct sets each serve one pair (e.g. a batch of pairs at different energies); a set that
+    serves several pairs (all pairs of one energy) is built once and stored."""
+    n_sets = len(plans.nodesets)
+    if n_sets == 0:
+        return None
+    use = (plans.ns_index >= 0) & plans.osc[None, :]
+    t_i, p_i = np.nonzero(use)
+    k = plans.ns_index[t_i, p_i]
+    ok = np.zeros(n_sets, dtype=bool)
+    if not len(k):
+        return ok
+    first_p = np.full(n_sets, -1, dtype=np.int64)
+    first_p[k[::-1]] = p_i[::-1]  # some pair of each set
+    single = np.ones(n_sets, dtype=bool)
+    single[np.unique(k[p_i != first_p[k]])] = False  # another pair uses it
+    n_t = np.bincount(k, minlength=n_sets)
+    ok = single & (n_t >= 1) & (n_t <= _lib.FOLD_MULTI - 1)
+    return ok
+
+
 class PreparedJob:
     """A job planned on the host with its inputs and descriptors resident on the device.
 
@@ -795,7 +890,7 @@ class PreparedJob:
     """
 
     def __init__(self, job: Job, dg: DeviceGrid, engine: str = "dense", plans=None,
-                 rebuild_nodesets: bool = False):
+                 rebuild_nodesets: bool = False, fuse_folds: Optional[bool] = None):
         if engine not in ENGINES:
             raise ValueError(f"unknown engine {engine!r}; choose from {ENGINES}")
         if job.L_max < 0:
@@ -811,8 +906,12 @@ class PreparedJob:
         self.plans = plans = plan_job(job) if plans is None else plans
         T, P = len(job.transitions), len(job.pairs)
         self.T, self.P = T, P
-        # 1. node sets (operators cached per grid and key; rebuilt every launch when rebuild_nodesets)
-        self.nodesets = NodeSetBatch(dg, plans.nodesets, job.CC_nodes, rebuild=rebuild_nodesets)
+        # 1. node sets (operators cached per grid and key; rebuilt every launch when rebuild_nodesets);
+        # sets that serve a single pair are applied to its folds at once when fusing (see fusable_sets)
+        fused = fusable_sets(plans, T) if fuse_folds is not False else None
+        if fuse_folds is None and fused is not None and int(fused.sum()) < FUSE_MIN_SETS:
+            fused = None
+        self.nodesets = NodeSetBatch(dg, plans.nodesets, job.CC_nodes, rebuild=rebuild_nodesets, fused=fused)
         # 2. functions on the device: continuum waves (planner order) + bound functions
         waves = getattr(job, "_waves", None) or WaveMatrix(N)
         wi_idx, wf_idx = getattr(job, "_wave_idx", (None, None))
@@ -934,6 +1033,22 @@ class PreparedJob:
             # wave both read (chi_f) is still in L2 for the second
             multi = np.empty(2 * G, dtype=_lib.FOLD_MULTI_DTYPE)
             multi[0::2], multi[1::2] = mT, mB
+            ns = self.nodesets
+            if ns.n_fused:
+                # the groups of fused sets (one per set) go with the node-set launch, in its order
+                pos = np.full(len(ns.ta_all), -1, dtype=np.int64)
+                pos[ns.fused_idx] = np.arange(ns.n_fused)
+                q = pos[kf]
+                fg = q >= 0
+                if int(np.count_nonzero(fg)) != ns.n_fused or len(np.unique(q[fg])) != ns.n_fused:
+                    raise RuntimeError("fused node sets must serve exactly one multi-fold group each")
+                ff = np.empty(2 * ns.n_fused, dtype=_lib.FOLD_MULTI_DTYPE)
+                ff[2 * q[fg]], ff[2 * q[fg] + 1] = mT[fg], mB[fg]
+                ns.set_fused_folds(ff)
+                keep_g = np.repeat(~fg, 2)
+                multi = multi[keep_g]
+        elif self.nodesets.n_fused:
+            raise RuntimeError("fused node sets without multi-folds")
         self.multi_host = multi
         self.n_multi = len(multi)
         self.multi_d = _dev(multi.view(np.uint8), dev) if len(multi) else None
@@ -1161,18 +1276,25 @@ class MultiPrepared:
         if any(p.job.L_max != self.L_max for p in parts):
             raise ValueError("all jobs of a batch share L_max")
         self.nl = self.L_max + 1
-        # node sets of every part (each record names its own grid)
+        # node sets of every part (each record names its own grid); fused sets with their folds
         recs = [p.nodesets.recs for p in parts if p.nodesets.n]
         self.n_sets = int(sum(len(r) for r in recs))
+        frecs = [p.nodesets.fused_recs for p in parts if p.nodesets.n_fused]
+        self.n_fused = int(sum(len(r) for r in frecs))
         self.max_grid = max(p.job.grid.N for p in parts)
-        if self.n_sets:
-            self.recs_d = _dev(np.concatenate(recs).view(np.uint8), dev)
-            cc = {p.nodesets.n_cc for p in parts if p.nodesets.n}
+        if self.n_sets or self.n_fused:
+            cc = {p.nodesets.n_cc for p in parts if p.nodesets.n or p.nodesets.n_fused}
             if len(cc) != 1:
                 raise ValueError("all jobs of a batch share CC_nodes")
             self.n_cc = cc.pop()
             self.ccx, self.ccw = CCTables.get(self.n_cc, dev)
             self.ns_status = torch.zeros(1, dtype=torch.int32, device=dev)
+        if self.n_sets:
+            self.recs_d = _dev(np.concatenate(recs).view(np.uint8), dev)
+        if self.n_fused:
+            self.frecs_d = _dev(np.concatenate(frecs).view(np.uint8), dev)
+            self.ffolds_d = _dev(np.concatenate([p.nodesets.fused_folds for p in parts if p.nodesets.n_fused])
+                                 .view(np.uint8), dev)
         folds = np.concatenate([p.folds_host for p in parts])
         self.n_folds = len(folds)
         self.folds_d = _dev(folds.view(np.uint8), dev)
@@ -1317,6 +1439,12 @@ class MultiPrepared:
                 _lib.check(lib.dwba_build_nodesets(_ptr(self.recs_d) + s0 * _lib.NODESET_DTYPE.itemsize, n,
                                                    self.max_grid, _ptr(self.ccx), _ptr(self.ccw), self.n_cc,
                                                    _ptr(self.ns_status), st), "dwba_build_nodesets")
+        for s0 in range(0, self.n_fused, 65535):
+            n = min(65535, self.n_fused - s0)
+            _lib.check(lib.dwba_build_nodesets_folded(_ptr(self.frecs_d) + s0 * _lib.NODESET_DTYPE.itemsize,
+                                                      _ptr(self.ffolds_d) + 2 * s0 * _lib.FOLD_MULTI_DTYPE.itemsize,
+                                                      n, self.max_grid, _ptr(self.ccx), _ptr(self.ccw), self.n_cc,
+                                                      _ptr(self.ns_status), st), "dwba_build_nodesets_folded")
         mark("nodesets")
         for s0 in range(0, self.n_folds, 65535):
             n = min(65535, self.n_folds - s0)
@@ -1388,7 +1516,7 @@ class MultiPrepared:
         if self.engine in TC_TERMS:
             return [p.collect() for p in self.parts]
         res = self.out.cpu().numpy()
-        if self.n_sets and int(self.ns_status.item()) != 0:
+        if (self.n_sets or self.n_fused) and int(self.ns_status.item()) != 0:
             raise _lib.DWBAError(_lib.DWBA_ERR_RANGE, "dwba_build_nodesets")
         outs = []
         for k, p in enumerate(self.parts):

@@ -120,6 +120,16 @@ typedef struct {
 
 int dwba_fold_multi(const dwba_fold_multi_t* folds_dev, int n_folds, int max_rows, dwba_stream_t stream);
 
+/* Node sets applied at once: builds the operators of each set as dwba_build_nodesets does, but
+ * instead of storing them (ta_dev / bx_dev are not used) applies them row by row to the two
+ * multi-folds of the set, folds_dev[2k] (half_band 1, the set's T) and folds_dev[2k + 1]
+ * (half_band 2, its B), whose op_dev fields are ignored, and writes the folds' outputs with
+ * dwba_fold_multi's arithmetic (the results are bit-identical to building the set, then folding).
+ * For node sets that serve a single pair: the operators never reach memory. */
+int dwba_build_nodesets_folded(const dwba_nodeset_t* sets_dev, const dwba_fold_multi_t* folds_dev, int n_sets,
+                               int max_grid, const double* cc_x_dev, const double* cc_w_dev, int n_cc,
+                               int* status_dev, dwba_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Bilinear forms in FP64: for each form f and L = 0..L_max,
  *   out[f*(L_max+1) + L] = sum_{i<n_rows} sum_{j<n_cols} a_i K_L(r_i, r_j) b_j.

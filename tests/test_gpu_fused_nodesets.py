@@ -1,0 +1,63 @@
+"""Node sets applied at once to their pair's folds (dwba_build_nodesets_folded).
+
+When every node set of a batch serves one pair (pairs at different energies), the engine builds
+each set's banded operators in registers and applies them to that pair's multi-folds in the same
+kernel, instead of storing the operators and folding in a second launch. The arithmetic is the
+fold kernel's, so the integrals must be bit-identical to the stored path: plane-wave-like pairs
+with n1 = N, and Coulomb-like pairs (breakpoint lists, eta != 0) with n1 < N.
+"""
+import numpy as np
+import pytest
+
+import bench
+
+pytestmark = pytest.mark.gpu
+
+
+def _job(kind):
+    from dwba_b200.dwba_matrix_elements import GPUCache, _make_job
+    if kind == "log":
+        g, z, bounds, pairs = bench.make_workload(N=3001, n_cont=96, n_bound=4, seed_shift=21)
+        V = U = z
+    else:
+        # Coulomb-like waves (eta = -1/k, matching index inside the grid: n1 < N) at a different
+        # energy per pair, on a log grid to r = 200, hydrogenic bound states
+        rng = np.random.default_rng(8)
+        g = bench.make_grid(2500, 1e-5, 200.0)
+        r = g.r
+        im = int(np.searchsorted(r, 120.0))
+        pairs = []
+        for _ in range(70):
+            w = []
+            k0 = float(rng.uniform(1.5, 6.0))
+            for l, k in ((int(rng.integers(0, 30)), k0), (int(rng.integers(0, 30)), k0 * 0.9)):
+                eta, d, sig = -1.0 / k, float(rng.uniform(0, np.pi)), float(rng.uniform(-1, 1))
+                chi = np.sin(k * r - 0.5 * l * np.pi + eta * np.log(2 * k * r) + sig + d) * \
+                    (1.0 - np.exp(-(r / ((l + 1) / k)) ** (l + 1)))
+                wv = bench._Wave(l, k, d, chi)
+                wv.eta, wv.sigma_l, wv.idx_match = eta, sig, im
+                w.append(wv)
+            pairs.append(tuple(w))
+        Z = 2.0
+        u1s = 2.0 * Z ** 1.5 * r * np.exp(-Z * r)
+        u2p = (Z / 2) ** 2.5 / np.sqrt(6.0) * r * r * np.exp(-Z * r / 2)
+        bounds = [(bench._Bound(0, u1s), bench._Bound(1, u2p))]
+        V = U = -Z / r
+    cache = GPUCache.from_grid(g)
+    job = _make_job(g, V, U, [b[0] for b in bounds], [b[1] for b in bounds], pairs, 6, U, {}, cache)
+    return job, cache
+
+
+@pytest.mark.parametrize("kind", ["log", "coulomb"])
+def test_fused_node_sets_match_stored_operators(kind):
+    from dwba_b200.engine import PreparedJob
+    job, cache = _job(kind)
+    fu = PreparedJob(job, cache.dg, "semisep", rebuild_nodesets=True, fuse_folds=True)
+    un = PreparedJob(job, cache.dg, "semisep", plans=fu.plans, rebuild_nodesets=True, fuse_folds=False)
+    assert fu.nodesets.n_fused > 0 and len(fu.multi_host) < len(un.multi_host)
+    fu.launch()
+    d1, e1 = fu.collect()
+    un.launch()
+    d2, e2 = un.collect()
+    assert np.array_equal(d1, d2) and np.array_equal(e1, e2)
+    assert np.isfinite(d1).all() and np.abs(e1).max() > 0

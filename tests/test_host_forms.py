@@ -188,3 +188,47 @@ def test_tensor_core_guard_routes_the_dominant_forms(monkeypatch):
         rows = torch.nonzero(t_of == t).ravel()
         top = rows[before[rows].abs().argmax(0)]
         assert bool(g.flag[top].all())
+
+
+def test_fused_node_sets_carry_their_pairs_folds():
+    """A batch whose pairs each have their own node set (different energies): with fusing, every set
+    is applied to its pair's multi-folds in the node-set launch and no multi-fold is left for the fold
+    launch; the fused fold descriptors are those the unfused job launches (same functions, outputs,
+    bands and sizes), in the order of the fused sets, and the sets get no operator memory."""
+    from dwba_b200.dwba_matrix_elements import _make_job
+    from dwba_b200.engine import FUSE_MIN_SETS, DeviceGrid, PreparedJob
+    from dwba_b200.plan import GridInfo
+    g, z, bounds, pairs = bench.make_workload(N=1201, n_cont=FUSE_MIN_SETS + 6, n_bound=3, seed_shift=9)
+
+    class Cache:
+        info = GridInfo(g.r, g.w_simpson, g.w_trapz)
+        dg = DeviceGrid(info, torch.device("cpu"))
+    job = _make_job(g, z, z, [b[0] for b in bounds], [b[1] for b in bounds], pairs, 4, z, {}, Cache)
+    fu = PreparedJob(job, Cache.dg, "semisep", rebuild_nodesets=True)
+    un = PreparedJob(job, Cache.dg, "semisep", plans=fu.plans, rebuild_nodesets=True, fuse_folds=False)
+    ns = fu.nodesets
+    assert ns.n_fused == len(fu.plans.nodesets) >= FUSE_MIN_SETS and ns.n == 0
+    assert len(fu.multi_host) == 0 and len(un.multi_host) == 2 * ns.n_fused
+    assert un.nodesets.n_fused == 0 and un.nodesets.n == ns.n_fused
+
+    def rel(m, job_):  # pointers as offsets into the job's function and operand matrices
+        F, O = job_.F.data_ptr(), job_.ops.data_ptr()
+        key = []
+        for fld in ("g",):
+            key.append(int(m[fld]) - F)
+        key += [int(x) - F for x in m["f"][:m["n_f"]]]
+        key += [int(x) - O for x in m["out"][:m["n_f"]]]
+        return tuple(key) + tuple(int(m[k]) for k in ("n_f", "half_band", "n_out", "n_src", "n_clear"))
+    want = {}
+    for q in range(len(un.multi_host) // 2):
+        mT, mB = un.multi_host[2 * q], un.multi_host[2 * q + 1]
+        k = int(np.nonzero(un.nodesets.ta_all == mT["op"])[0][0])
+        assert un.nodesets.bx_all[k] == mB["op"]
+        want[k] = (rel(mT, un), rel(mB, un))
+    got = {int(k): (rel(ns.fused_folds[2 * q], fu), rel(ns.fused_folds[2 * q + 1], fu))
+           for q, k in enumerate(ns.fused_idx)}
+    assert got == want
+    assert np.all(ns.ta_all == 0) and np.all(ns.bx_all == 0)
+    # a job with fewer single-pair sets than the threshold stores its operators
+    small = _make_job(g, z, z, [b[0] for b in bounds], [b[1] for b in bounds], pairs[:8], 4, z, {}, Cache)
+    assert PreparedJob(small, Cache.dg, "semisep", rebuild_nodesets=True).nodesets.n_fused == 0

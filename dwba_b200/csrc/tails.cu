@@ -136,12 +136,45 @@ struct EnvPow {
   }
 };
 
+// Filon constants shared by every panel of one phase branch: the segments are equal (linspace) and
+// so are their panels, so alpha, beta, gamma of the panel angle theta = omega h / 2 and the phase
+// step between nodes, E = exp(i omega h / 2), are evaluated once per branch instead of per panel.
+struct FilonConst {
+  double al, be, ga;
+  cplx E;
+};
+
+__device__ __forceinline__ FilonConst filon_const(double omega, double seg_w, int nn) {
+  FilonConst c;
+  const double h = 2.0 * seg_w / (nn - 1);  // panel width (two node spacings)
+  const double th = omega * h / 2;
+  double st, ct;
+  sincos(th, &st, &ct);
+  c.E = {ct, st};
+  if (fabs(th) < 0.3) {
+    const double t2 = th * th, t3 = t2 * th, t6 = t2 * t2 * t2;
+    c.al = 2 * t3 / 45 * (1 - t2 / 7 + (t2 * t2) / 189);
+    c.be = 2.0 / 3 + 2 * t2 / 15 - 4 * (t2 * t2) / 105 + 2 * t6 / 567;
+    c.ga = 4.0 / 3 - 2 * t2 / 15 + 1 * (t2 * t2) / 210 - t6 / 11340;
+  } else {
+    const double t2 = th * th, t3 = t2 * th;
+    double s2, c2;
+    sincos(2 * th, &s2, &c2);
+    c.al = (t2 + th * s2 / 2 - 2 * (st * st)) / t3;
+    c.be = 2 * (th * (1 + c2) - s2) / t3;
+    c.ga = 4 * (st - th * ct) / t3;
+  }
+  return c;
+}
+
 // Re of the Filon integral over one segment (nn equally spaced nodes, nn odd) for every multipole
 // of the chunk: _filon_segment_complex with the node phases and the panel weights shared by all L.
+// The first node's phase factor is evaluated directly, the next ones by the recurrence
+// e_{j+1} = e_j E (nn - 1 <= 14 steps: a few ulps), and the panels use the branch's FilonConst.
 // Envelope values are formed inside the multipole loops from one running power per node, so no
 // per-node arrays of envelopes are kept.
 __device__ __forceinline__ void filon_segment_all(const double* m, int L0, int nl, double a, double b, int nn, double omega,
-                                  double off, KSum* acc) {
+                                  double off, const FilonConst& fc, KSum* acc) {
   if (!(b - a >= 1e-15)) return;
   if (fabs(omega * (b - a)) < 1e-3) {  // scipy simpson with possibly unequal spacing, times the mid phase
     const double ce = cexpi(omega * (a + b) / 2 + off).re;
@@ -173,10 +206,13 @@ __device__ __forceinline__ void filon_segment_all(const double* m, int L0, int n
   double x0 = a;
   cplx e0 = cexpi(omega * x0 + off);
   EnvPow v0(x0, L0);
+  const cplx mi = {0.0, -1.0 / omega};
+  const cplx am = cscale(fc.al, mi);
+  const cplx wl = csub(cplx{fc.be, 0.0}, am), wr = cadd(cplx{fc.be, 0.0}, am);
   for (int i = 0; i + 2 < nn; i += 2) {
     const double x1 = lin(a, b, nn, i + 1), x2 = lin(a, b, nn, i + 2);
     const double h = x2 - x0;
-    const cplx e1 = cexpi(omega * x1 + off), e2 = cexpi(omega * x2 + off);
+    const cplx e1 = cmul(e0, fc.E), e2 = cmul(e1, fc.E);
     const EnvPow v1(x1, L0), v2(x2, L0);
     if (h >= 1e-15) {
       double w0, w1, w2;
@@ -188,30 +224,11 @@ __device__ __forceinline__ void filon_segment_all(const double* m, int L0, int n
         w1 = ce * (hs / 6.0) * (hs * (hs / hp));
         w2 = ce * (hs / 6.0) * (2.0 - qq);
       } else {
-        const double th = omega * h / 2;
-        double st, ct;
-        sincos(th, &st, &ct);
-        double al, be, ga;
-        if (fabs(th) < 0.3) {
-          const double t2 = th * th, t3 = t2 * th, t6 = t2 * t2 * t2;
-          al = 2 * t3 / 45 * (1 - t2 / 7 + (t2 * t2) / 189);
-          be = 2.0 / 3 + 2 * t2 / 15 - 4 * (t2 * t2) / 105 + 2 * t6 / 567;
-          ga = 4.0 / 3 - 2 * t2 / 15 + 1 * (t2 * t2) / 210 - t6 / 11340;
-        } else {
-          const double t2 = th * th, t3 = t2 * th;
-          double s2, c2;
-          sincos(2 * th, &s2, &c2);
-          al = (t2 + th * s2 / 2 - 2 * (st * st)) / t3;
-          be = 2 * (th * (1 + c2) - s2) / t3;
-          ga = 4 * (st - th * ct) / t3;
-        }
         // (h/2) [alpha (-i/omega) (f2 e2 - f0 e0) + beta (f0 e0 + f2 e2) + gamma f1 e1], real part,
         // as weights of f0, f1, f2 that every multipole shares
-        const cplx mi = {0.0, -1.0 / omega};
-        const cplx am = cscale(al, mi);
-        w0 = (h / 2) * cmul(csub(cplx{be, 0.0}, am), e0).re;
-        w1 = (h / 2) * (ga * e1.re);
-        w2 = (h / 2) * cmul(cadd(cplx{be, 0.0}, am), e2).re;
+        w0 = (h / 2) * cmul(wl, e0).re;
+        w1 = (h / 2) * (fc.ga * e1.re);
+        w2 = (h / 2) * cmul(wr, e2).re;
       }
       double p0 = v0.p0, p1 = v1.p0, p2 = v2.p0;
 #pragma unroll
@@ -339,9 +356,10 @@ __device__ __noinline__ void outer_branch_all(const double* m, int L0, int nl, c
       const int scl = (int)ceil(eff / max_dphi);
       nn = min(15, max(5, 5 + 2 * (scl - 1)));
     }
+    const FilonConst fc = filon_const(om, (rmax - rm) / nseg, nn);
     for (int s = lane; s < nseg; s += 32) {
       const double a = lin(rm, rmax, nseg + 1, s), b = lin(rm, rmax, nseg + 1, s + 1);
-      filon_segment_all(m, L0, nl, a, b, nn, om, off, acc);
+      filon_segment_all(m, L0, nl, a, b, nn, om, off, fc, acc);
     }
   } else {
     // four segments per warp pass, one per group of 8 lanes; lane 0 of a group accumulates it

@@ -586,6 +586,10 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # wait (up to 3 s) for the first sample, so that a short timed region is sampled too
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
@@ -831,7 +835,8 @@ def main():
     # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu capture of
     # the default workload (profiles/launches_semisep_synthetic_batch_N15000.md); other sizes: null
     default_size = args.n_cont == N_CONT
-    traffic: dict = {}
+    traffic = {"nodeset_rows_kernel": 0.497e9 + 2.184e9, "fold_kernel": 1.09e6, "potential_kernel": 0.66e6,
+               "dot_kernel": 0.498e9 + 0.004e9, "semisep_kernel": 2.191e9 + 0.004e9} if args.engine == "semisep" else {}
 
     def hbm_roof(kernel, nbytes, t_ms, note):
         ach = nbytes / (t_ms * 1e-3) / 1e9

@@ -28,7 +28,29 @@ def sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
+def build_hostpack(verbose: bool = False, force: bool = False) -> str:
+    """The CPython extension ``_hostpack`` (csrc/hostpack.c: packing of a batch's waves on the host),
+    built with the C compiler against this interpreter's headers, next to this file."""
+    import sysconfig
+    src = os.path.join(CSRC, "hostpack.c")
+    out = os.path.join(HERE, "_hostpack" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
+    if not force and os.path.exists(out) and os.path.getmtime(src) <= os.path.getmtime(out):
+        return out
+    cc = os.environ.get("CC") or shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        raise RuntimeError("a C compiler is required to build dwba_b200._hostpack")
+    cmd = [cc, "-O2", "-shared", "-fPIC", "-I", sysconfig.get_paths()["include"], src, "-o", out + ".tmp"]
+    if verbose:
+        print(" ".join(cmd))
+    res = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    if res.returncode != 0:
+        raise RuntimeError("hostpack build failed:\n" + res.stdout.decode(errors="replace"))
+    os.replace(out + ".tmp", out)
+    return out
+
+
 def build(verbose: bool = False, force: bool = False) -> str:
+    build_hostpack(verbose, force)
     srcs = sources()
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     deps.append(os.path.join(HERE, "..", "include", "dwba_b200.h"))

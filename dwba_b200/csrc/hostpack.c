@@ -1,0 +1,179 @@
+/* Host-side packing of a batch's continuum waves (CPython extension, no GPU code).
+ *
+ * One pass over the (cont_i, cont_f) pairs of a call reads each wave's scalar attributes -- the
+ * fields the reference's ContinuumWave carries (k_au, l, idx_match, eta, phase_shift, sigma_l;
+ * dwba_matrix_elements.py reads them per pair in radial_ME_all_L) -- and checks and numbers its
+ * chi_of_r array, so that the engine's planner gets them as arrays instead of walking thousands of
+ * Python objects several times per call:
+ *
+ *   pack_pairs(pairs, N, ndarray_type) ->
+ *       (scalars: bytes of P x 12 doubles (k, l, idx_match, eta, phase_shift, sigma_l of cont_i,
+ *                 then of cont_f),
+ *        rows_i, rows_f: bytes of P int64 (row of each pair's chi in the batch's function matrix:
+ *                 distinct chi objects numbered in order of first appearance, all cont_i first),
+ *        arrays: list of the distinct chi objects in row order)
+ *   or None when some wave does not qualify (its chi_of_r not exactly an ndarray of N float64
+ *   values in C order, or l / k_au missing): the caller then takes its general path.
+ */
+#define PY_SSIZE_T_CLEAN
+#include <Python.h>
+#include <stdint.h>
+#include <string.h>
+
+static int get_double(PyObject* o, const char* name, double dflt, int required, double* out) {
+  PyObject* v = PyObject_GetAttrString(o, name);
+  if (!v) {
+    if (!PyErr_ExceptionMatches(PyExc_AttributeError)) return -1;
+    PyErr_Clear();
+    if (required) return 1;
+    *out = dflt;
+    return 0;
+  }
+  const double d = PyFloat_AsDouble(v);
+  Py_DECREF(v);
+  if (d == -1.0 && PyErr_Occurred()) return -1;
+  *out = d;
+  return 0;
+}
+
+/* the row of chi (by object identity) in rows_map, numbered on first sight; -1 on error,
+ * -2 when chi does not qualify */
+static Py_ssize_t chi_row(PyObject* chi, Py_ssize_t N, PyTypeObject* nd, PyObject* rows_map, PyObject* arrays) {
+  if (Py_TYPE(chi) != nd) return -2;
+  PyObject* key = PyLong_FromVoidPtr((void*)chi);
+  if (!key) return -1;
+  PyObject* hit = PyDict_GetItemWithError(rows_map, key);
+  if (hit) {
+    const Py_ssize_t r = PyLong_AsSsize_t(hit);
+    Py_DECREF(key);
+    return r;
+  }
+  if (PyErr_Occurred()) {
+    Py_DECREF(key);
+    return -1;
+  }
+  Py_buffer view;
+  if (PyObject_GetBuffer(chi, &view, PyBUF_C_CONTIGUOUS | PyBUF_FORMAT) != 0) {
+    PyErr_Clear();
+    Py_DECREF(key);
+    return -2;
+  }
+  const int ok = view.ndim == 1 && view.itemsize == 8 && view.format && strcmp(view.format, "d") == 0 &&
+                 view.shape && view.shape[0] == N;
+  PyBuffer_Release(&view);
+  if (!ok) {
+    Py_DECREF(key);
+    return -2;
+  }
+  const Py_ssize_t r = PyList_GET_SIZE(arrays);
+  PyObject* rv = PyLong_FromSsize_t(r);
+  if (!rv || PyDict_SetItem(rows_map, key, rv) != 0 || PyList_Append(arrays, chi) != 0) {
+    Py_XDECREF(rv);
+    Py_DECREF(key);
+    return -1;
+  }
+  Py_DECREF(rv);
+  Py_DECREF(key);
+  return r;
+}
+
+/* scalars of one wave into s[0..5]; 0 ok, 1 does not qualify, -1 error */
+static int wave_scalars(PyObject* w, double* s) {
+  int rc;
+  if ((rc = get_double(w, "k_au", 0.0, 1, &s[0])) != 0) return rc;
+  if ((rc = get_double(w, "l", 0.0, 1, &s[1])) != 0) return rc;
+  if ((rc = get_double(w, "idx_match", -1.0, 0, &s[2])) != 0) return rc;
+  if ((rc = get_double(w, "eta", 0.0, 0, &s[3])) != 0) return rc;
+  if ((rc = get_double(w, "phase_shift", 0.0, 0, &s[4])) != 0) return rc;
+  if ((rc = get_double(w, "sigma_l", 0.0, 0, &s[5])) != 0) return rc;
+  s[1] = (double)(long long)s[1];
+  s[2] = (double)(long long)s[2];
+  return 0;
+}
+
+static PyObject* pack_pairs(PyObject* self, PyObject* args) {
+  (void)self;
+  PyObject* pairs;
+  Py_ssize_t N;
+  PyObject* nd_obj;
+  if (!PyArg_ParseTuple(args, "OnO", &pairs, &N, &nd_obj)) return NULL;
+  if (!PyType_Check(nd_obj)) {
+    PyErr_SetString(PyExc_TypeError, "ndarray_type must be a type");
+    return NULL;
+  }
+  PyTypeObject* nd = (PyTypeObject*)nd_obj;
+  PyObject* seq = PySequence_Fast(pairs, "pairs must be a sequence");
+  if (!seq) return NULL;
+  const Py_ssize_t P = PySequence_Fast_GET_SIZE(seq);
+  PyObject* scal = PyBytes_FromStringAndSize(NULL, P * 12 * (Py_ssize_t)sizeof(double));
+  PyObject* ri = PyBytes_FromStringAndSize(NULL, P * (Py_ssize_t)sizeof(int64_t));
+  PyObject* rf = PyBytes_FromStringAndSize(NULL, P * (Py_ssize_t)sizeof(int64_t));
+  PyObject* rows_map = PyDict_New();
+  PyObject* arrays = PyList_New(0);
+  PyObject* result = NULL;
+  if (!scal || !ri || !rf || !rows_map || !arrays) goto done;
+  {
+    double* S = (double*)PyBytes_AS_STRING(scal);
+    int64_t* RI = (int64_t*)PyBytes_AS_STRING(ri);
+    int64_t* RF = (int64_t*)PyBytes_AS_STRING(rf);
+    PyObject** items = PySequence_Fast_ITEMS(seq);
+    /* pass 1: cont_i of every pair (their chi arrays take the first rows); pass 2: cont_f */
+    for (int side = 0; side < 2; ++side) {
+      for (Py_ssize_t p = 0; p < P; ++p) {
+        PyObject* pr = items[p];
+        PyObject* w = NULL;
+        if (PyTuple_Check(pr) && PyTuple_GET_SIZE(pr) == 2) {
+          w = PyTuple_GET_ITEM(pr, side);
+          Py_INCREF(w);
+        } else {
+          w = PySequence_GetItem(pr, side);
+          if (!w) goto done;
+        }
+        const int rc = wave_scalars(w, S + 12 * p + 6 * side);
+        if (rc != 0) {
+          Py_DECREF(w);
+          if (rc < 0) goto done;
+          result = Py_None;
+          Py_INCREF(result);
+          goto done;
+        }
+        PyObject* chi = PyObject_GetAttrString(w, "chi_of_r");
+        Py_DECREF(w);
+        if (!chi) {
+          if (!PyErr_ExceptionMatches(PyExc_AttributeError)) goto done;
+          PyErr_Clear();
+          result = Py_None;
+          Py_INCREF(result);
+          goto done;
+        }
+        const Py_ssize_t r = chi_row(chi, N, nd, rows_map, arrays);
+        Py_DECREF(chi);
+        if (r == -1) goto done;
+        if (r == -2) {
+          result = Py_None;
+          Py_INCREF(result);
+          goto done;
+        }
+        (side == 0 ? RI : RF)[p] = (int64_t)r;
+      }
+    }
+    result = Py_BuildValue("(OOOO)", scal, ri, rf, arrays);
+  }
+done:
+  Py_DECREF(seq);
+  Py_XDECREF(scal);
+  Py_XDECREF(ri);
+  Py_XDECREF(rf);
+  Py_XDECREF(rows_map);
+  Py_XDECREF(arrays);
+  return result;
+}
+
+static PyMethodDef methods[] = {
+    {"pack_pairs", pack_pairs, METH_VARARGS,
+     "pack_pairs(pairs, N, ndarray_type) -> (scalars, rows_i, rows_f, arrays) or None"},
+    {NULL, NULL, 0, NULL}};
+
+static struct PyModuleDef module = {PyModuleDef_HEAD_INIT, "_hostpack", NULL, -1, methods, NULL, NULL, NULL, NULL};
+
+PyMODINIT_FUNC PyInit__hostpack(void) { return PyModule_Create(&module); }

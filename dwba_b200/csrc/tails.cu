@@ -407,9 +407,9 @@ __device__ double analytical_tail(double r_m, const WaveD& wi, const WaveD& wf, 
 // one warp per (record, chunk of up to LC multipoles): the Filon / Levin segments of both phase
 // branches over the lanes, every node's phase factor and every panel's weights shared by the chunk
 #ifndef DWBA_TAILS_MIN_BLOCKS
-// four CTAs per SM (128 registers): measured 9.51 ms on the 64-energy sweep's 106,293 records,
-// against 9.65 ms at three (168 registers, no spills) and 11.7 ms at two
-#define DWBA_TAILS_MIN_BLOCKS 4
+// three CTAs per SM (168 registers): measured 5.87 ms on the 64-energy sweep's 106,293 records,
+// against 6.31 ms at four (128 registers, spills)
+#define DWBA_TAILS_MIN_BLOCKS 3
 #endif
 __global__ void __launch_bounds__(128, DWBA_TAILS_MIN_BLOCKS) tails_kernel(const dwba_tail_t* __restrict__ recs, int n, int L_max, int max_seg, double max_dphi,
                              LevinD lv) {

@@ -32,6 +32,11 @@ import numpy as np
 
 from . import _lib
 
+try:  # host packing of a batch's waves (csrc/hostpack.c); the general Python path works without it
+    from . import _hostpack
+except ImportError:  # pragma: no cover - only when the extension was not built
+    _hostpack = None
+
 OscillatoryMethod = Literal["legacy", "advanced", "full_split"]
 SEMANTICS = ("cpu", "cupy")
 
@@ -156,6 +161,29 @@ class _WaveView:
         self.sigma_l = float(getattr(w, "sigma_l", 0.0))
 
 
+class _Packed:
+    """A batch's waves packed in one pass by the host extension: scalars (P x 12), the rows of each
+    pair's two chi arrays among the distinct ones (``arrays``, cont_i first) and, once they are in a
+    WaveMatrix (``owner``), the row of the first (``first``)."""
+    __slots__ = ("scalars", "rows_i", "rows_f", "arrays", "first", "owner")
+
+    def __init__(self, scalars, rows_i, rows_f, arrays):
+        self.scalars, self.rows_i, self.rows_f, self.arrays = scalars, rows_i, rows_f, arrays
+        self.first, self.owner = None, None
+
+
+def _pack(pairs, N):
+    """_Packed for the pairs, or None when a wave needs the general path (or the extension is absent)."""
+    if _hostpack is None or len(pairs) == 0:
+        return None
+    res = _hostpack.pack_pairs(pairs, int(N), np.ndarray)
+    if res is None:
+        return None
+    scal, ri, rf, arrays = res
+    return _Packed(np.frombuffer(scal, dtype=np.float64).reshape(-1, 12), np.frombuffer(ri, dtype=np.int64),
+                   np.frombuffer(rf, dtype=np.int64), arrays)
+
+
 def _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, cache):
     """Job for one or several transitions: bound_i/bound_f are single objects or equal-length sequences."""
     from .engine import Job, Transition
@@ -183,17 +211,23 @@ def _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f
                   hasattr(w, "l") and hasattr(w, "k_au"))
             v = cache_w[id(w)] = w if ok else _WaveView(w, N, what)
         return v
-    wp = [(view(ci, "cont_i.chi"), view(cf, "cont_f.chi")) for ci, cf in pairs]
+    packed = _pack(pairs, N)
+    if packed is not None:
+        wp = [(ci, cf) for ci, cf in pairs]  # every wave qualifies as it is
+    else:
+        wp = [(view(ci, "cont_i.chi"), view(cf, "cont_f.chi")) for ci, cf in pairs]
     meth = kw.get("oscillatory_method", "advanced")
     if meth not in ("legacy", "advanced", "full_split"):
         meth = "advanced"  # the reference treats any other value as "advanced" (dwba_matrix_elements.py:1183)
-    return Job(grid=cache.info, V_core=V, U_i=Ui, U_f=Uf, transitions=trans, pairs=wp, L_max=int(L_max),
+    job = Job(grid=cache.info, V_core=V, U_i=Ui, U_f=Uf, transitions=trans, pairs=wp, L_max=int(L_max),
                use_oscillatory_quadrature=bool(kw.get("use_oscillatory_quadrature", True)),
                oscillatory_method=meth, CC_nodes=int(kw.get("CC_nodes", 5)),
                phase_increment=float(kw.get("phase_increment", 1.5708)),
                min_grid_fraction=float(kw.get("min_grid_fraction", 0.10)),
                k_threshold=float(kw.get("k_threshold", 0.5)),
                tails_on_device=os.environ.get("DWBA_B200_TAILS", "device").strip().lower() != "host")
+    job._packed = packed
+    return job
 
 
 def _no_gc(fn):
@@ -220,10 +254,14 @@ def _early_upload(job, device):
     find them uploaded."""
     from .engine import WaveMatrix
     waves = WaveMatrix(job.grid.N)
-    for ci, _ in job.pairs:
-        waves.add(ci.chi_of_r)
-    for _, cf in job.pairs:
-        waves.add(cf.chi_of_r)
+    packed = getattr(job, "_packed", None)
+    if packed is not None:
+        packed.first, packed.owner = waves.add_distinct(packed.arrays), waves
+    else:
+        for ci, _ in job.pairs:
+            waves.add(ci.chi_of_r)
+        for _, cf in job.pairs:
+            waves.add(cf.chi_of_r)
     for t in job.transitions:
         waves.add(t.u_i)
         waves.add(t.u_f)

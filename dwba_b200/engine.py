@@ -363,6 +363,16 @@ def _wave_scalars(w):
             float(getattr(w, "phase_shift", 0.0)), float(getattr(w, "sigma_l", 0.0)))
 
 
+def _packed_pair_arrays(scal: np.ndarray):
+    """_pair_arrays from the packed scalars (P x 12: k, l, idx_match, eta, phase_shift, sigma_l of
+    cont_i then cont_f)."""
+    a = scal
+    out = dict(k_i=a[:, 0], l_i=a[:, 1].astype(np.int64), im_i=a[:, 2].astype(np.int64), e_i=a[:, 3], d_i=a[:, 4],
+               s_i=a[:, 5], k_f=a[:, 6], l_f=a[:, 7].astype(np.int64), im_f=a[:, 8].astype(np.int64), e_f=a[:, 9],
+               d_f=a[:, 10], s_f=a[:, 11])
+    return {k: np.ascontiguousarray(v) for k, v in out.items()}
+
+
 def _pair_arrays(pairs):
     """Scalar metadata of every pair's two waves as arrays (each distinct wave read once)."""
     memo: Dict[int, tuple] = {}
@@ -451,6 +461,16 @@ class WaveMatrix:
         self._uploaded: Dict[str, Tuple[int, torch.Tensor]] = {}
         self._by_id: Dict[int, int] = {}
         self._keep: List[object] = []
+
+    def add_distinct(self, arrays: Sequence[np.ndarray]) -> int:
+        """Append arrays known to be distinct objects of N float64 values that are not rows yet (a
+        packed batch's waves), in order; returns the row of the first."""
+        first = len(self.arrays)
+        for i, a in enumerate(arrays):
+            self._by_id[id(a)] = first + i
+        self.arrays.extend(arrays)
+        self._keep.extend(arrays)
+        return first
 
     def add(self, arr: np.ndarray) -> int:
         """Row of ``arr`` (one row per distinct array object; the object is kept alive with it)."""
@@ -594,7 +614,8 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
     g = job.grid
     N, r, w = g.N, g.r, g.w
     P, T = len(job.pairs), len(job.transitions)
-    pa = _pair_arrays(job.pairs)
+    packed = getattr(job, "_packed", None)
+    pa = _packed_pair_arrays(packed.scalars) if packed is not None else _pair_arrays(job.pairs)
     k_total = pa["k_i"] + pa["k_f"]
     eta_total = pa["e_i"] + pa["e_f"]
     osc = np.asarray(job.use_oscillatory_quadrature & (k_total > job.k_threshold), dtype=bool)
@@ -604,8 +625,14 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
     legacy = job.oscillatory_method == "legacy"
     if waves is None:
         waves = WaveMatrix(N)
-    wi_idx = np.array([waves.add(ci.chi_of_r) for ci, _ in job.pairs], dtype=np.int64)
-    wf_idx = np.array([waves.add(cf.chi_of_r) for _, cf in job.pairs], dtype=np.int64)
+    if packed is not None and packed.owner is not waves and not waves.arrays:
+        packed.first, packed.owner = waves.add_distinct(packed.arrays), waves
+    if packed is not None and packed.owner is waves:
+        # rows of the packed waves (added to this matrix in the packed order)
+        wi_idx, wf_idx = packed.rows_i + packed.first, packed.rows_f + packed.first
+    else:
+        wi_idx = np.array([waves.add(ci.chi_of_r) for ci, _ in job.pairs], dtype=np.int64)
+        wf_idx = np.array([waves.add(cf.chi_of_r) for _, cf in job.pairs], dtype=np.int64)
     n1_all = np.zeros((T, P), dtype=np.int64)
     ns_index = np.full((T, P), -1, dtype=np.int64)
     corr_dir = np.zeros((T, P))

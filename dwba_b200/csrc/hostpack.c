@@ -11,7 +11,8 @@
  *                 then of cont_f),
  *        rows_i, rows_f: bytes of P int64 (row of each pair's chi in the batch's function matrix:
  *                 distinct chi objects numbered in order of first appearance, all cont_i first),
- *        arrays: list of the distinct chi objects in row order)
+ *        arrays: list of the distinct chi objects in row order,
+ *        ptrs: list of the data addresses of the distinct arrays, in row order)
  *   or None when some wave does not qualify (its chi_of_r not exactly an ndarray of N float64
  *   values in C order, or l / k_au missing): the caller then takes its general path.
  */
@@ -38,7 +39,8 @@ static int get_double(PyObject* o, const char* name, double dflt, int required, 
 
 /* the row of chi (by object identity) in rows_map, numbered on first sight; -1 on error,
  * -2 when chi does not qualify */
-static Py_ssize_t chi_row(PyObject* chi, Py_ssize_t N, PyTypeObject* nd, PyObject* rows_map, PyObject* arrays) {
+static Py_ssize_t chi_row(PyObject* chi, Py_ssize_t N, PyTypeObject* nd, PyObject* rows_map, PyObject* arrays,
+                          PyObject* ptrs) {
   if (Py_TYPE(chi) != nd) return -2;
   PyObject* key = PyLong_FromVoidPtr((void*)chi);
   if (!key) return -1;
@@ -60,6 +62,7 @@ static Py_ssize_t chi_row(PyObject* chi, Py_ssize_t N, PyTypeObject* nd, PyObjec
   }
   const int ok = view.ndim == 1 && view.itemsize == 8 && view.format && strcmp(view.format, "d") == 0 &&
                  view.shape && view.shape[0] == N;
+  const int64_t addr = (int64_t)(intptr_t)view.buf;
   PyBuffer_Release(&view);
   if (!ok) {
     Py_DECREF(key);
@@ -67,11 +70,15 @@ static Py_ssize_t chi_row(PyObject* chi, Py_ssize_t N, PyTypeObject* nd, PyObjec
   }
   const Py_ssize_t r = PyList_GET_SIZE(arrays);
   PyObject* rv = PyLong_FromSsize_t(r);
-  if (!rv || PyDict_SetItem(rows_map, key, rv) != 0 || PyList_Append(arrays, chi) != 0) {
+  PyObject* pv = PyLong_FromLongLong((long long)addr);
+  if (!rv || !pv || PyDict_SetItem(rows_map, key, rv) != 0 || PyList_Append(arrays, chi) != 0 ||
+      PyList_Append(ptrs, pv) != 0) {
     Py_XDECREF(rv);
+    Py_XDECREF(pv);
     Py_DECREF(key);
     return -1;
   }
+  Py_DECREF(pv);
   Py_DECREF(rv);
   Py_DECREF(key);
   return r;
@@ -110,8 +117,9 @@ static PyObject* pack_pairs(PyObject* self, PyObject* args) {
   PyObject* rf = PyBytes_FromStringAndSize(NULL, P * (Py_ssize_t)sizeof(int64_t));
   PyObject* rows_map = PyDict_New();
   PyObject* arrays = PyList_New(0);
+  PyObject* ptrs = PyList_New(0);
   PyObject* result = NULL;
-  if (!scal || !ri || !rf || !rows_map || !arrays) goto done;
+  if (!scal || !ri || !rf || !rows_map || !arrays || !ptrs) goto done;
   {
     double* S = (double*)PyBytes_AS_STRING(scal);
     int64_t* RI = (int64_t*)PyBytes_AS_STRING(ri);
@@ -146,7 +154,7 @@ static PyObject* pack_pairs(PyObject* self, PyObject* args) {
           Py_INCREF(result);
           goto done;
         }
-        const Py_ssize_t r = chi_row(chi, N, nd, rows_map, arrays);
+        const Py_ssize_t r = chi_row(chi, N, nd, rows_map, arrays, ptrs);
         Py_DECREF(chi);
         if (r == -1) goto done;
         if (r == -2) {
@@ -157,7 +165,7 @@ static PyObject* pack_pairs(PyObject* self, PyObject* args) {
         (side == 0 ? RI : RF)[p] = (int64_t)r;
       }
     }
-    result = Py_BuildValue("(OOOO)", scal, ri, rf, arrays);
+    result = Py_BuildValue("(OOOOO)", scal, ri, rf, arrays, ptrs);
   }
 done:
   Py_DECREF(seq);
@@ -166,12 +174,13 @@ done:
   Py_XDECREF(rf);
   Py_XDECREF(rows_map);
   Py_XDECREF(arrays);
+  Py_XDECREF(ptrs);
   return result;
 }
 
 static PyMethodDef methods[] = {
     {"pack_pairs", pack_pairs, METH_VARARGS,
-     "pack_pairs(pairs, N, ndarray_type) -> (scalars, rows_i, rows_f, arrays) or None"},
+     "pack_pairs(pairs, N, ndarray_type) -> (scalars, rows_i, rows_f, arrays, ptrs) or None"},
     {NULL, NULL, 0, NULL}};
 
 static struct PyModuleDef module = {PyModuleDef_HEAD_INIT, "_hostpack", NULL, -1, methods, NULL, NULL, NULL, NULL};

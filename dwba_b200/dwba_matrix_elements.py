@@ -165,10 +165,11 @@ class _Packed:
     """A batch's waves packed in one pass by the host extension: scalars (P x 12), the rows of each
     pair's two chi arrays among the distinct ones (``arrays``, cont_i first) and, once they are in a
     WaveMatrix (``owner``), the row of the first (``first``)."""
-    __slots__ = ("scalars", "rows_i", "rows_f", "arrays", "first", "owner")
+    __slots__ = ("scalars", "rows_i", "rows_f", "arrays", "ptrs", "first", "owner")
 
-    def __init__(self, scalars, rows_i, rows_f, arrays):
+    def __init__(self, scalars, rows_i, rows_f, arrays, ptrs):
         self.scalars, self.rows_i, self.rows_f, self.arrays = scalars, rows_i, rows_f, arrays
+        self.ptrs = np.asarray(ptrs, dtype=np.int64)
         self.first, self.owner = None, None
 
 
@@ -179,9 +180,9 @@ def _pack(pairs, N):
     res = _hostpack.pack_pairs(pairs, int(N), np.ndarray)
     if res is None:
         return None
-    scal, ri, rf, arrays = res
+    scal, ri, rf, arrays, ptrs = res
     return _Packed(np.frombuffer(scal, dtype=np.float64).reshape(-1, 12), np.frombuffer(ri, dtype=np.int64),
-                   np.frombuffer(rf, dtype=np.int64), arrays)
+                   np.frombuffer(rf, dtype=np.int64), arrays, ptrs)
 
 
 def _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, cache):
@@ -256,7 +257,7 @@ def _early_upload(job, device):
     waves = WaveMatrix(job.grid.N)
     packed = getattr(job, "_packed", None)
     if packed is not None:
-        packed.first, packed.owner = waves.add_distinct(packed.arrays), waves
+        packed.first, packed.owner = waves.add_distinct(packed.arrays, packed.ptrs), waves
     else:
         for ci, _ in job.pairs:
             waves.add(ci.chi_of_r)

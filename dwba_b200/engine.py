@@ -461,15 +461,19 @@ class WaveMatrix:
         self._uploaded: Dict[str, Tuple[int, torch.Tensor]] = {}
         self._by_id: Dict[int, int] = {}
         self._keep: List[object] = []
+        self._ptrs: Dict[int, Tuple[int, np.ndarray]] = {}  # first row -> (count, data addresses)
 
-    def add_distinct(self, arrays: Sequence[np.ndarray]) -> int:
-        """Append arrays known to be distinct objects of N float64 values that are not rows yet (a
-        packed batch's waves), in order; returns the row of the first."""
+    def add_distinct(self, arrays: Sequence[np.ndarray], ptrs: Optional[np.ndarray] = None) -> int:
+        """Append arrays known to be distinct C-contiguous objects of N float64 values that are not
+        rows yet (a packed batch's waves, with their data addresses), in order; returns the row of
+        the first."""
         first = len(self.arrays)
         for i, a in enumerate(arrays):
             self._by_id[id(a)] = first + i
         self.arrays.extend(arrays)
         self._keep.extend(arrays)
+        if ptrs is not None:
+            self._ptrs[first] = (len(arrays), np.asarray(ptrs, dtype=np.int64))
         return first
 
     def add(self, arr: np.ndarray) -> int:
@@ -519,9 +523,28 @@ class WaveMatrix:
         done = np.zeros(n, dtype=bool)
         groups: Dict[int, list] = {}
         base_ptrs: Dict[int, int] = {}
-        ptrs = [a.__array_interface__["data"][0] for a in self.arrays]
+        grouped = np.zeros(n, dtype=bool)
+        # runs of packed rows (addresses known): those lying in the rows of the matrix behind their
+        # first array are grouped with it by address arithmetic, without a pass per array
+        for first, (cnt, addr) in self._ptrs.items():
+            b = self.arrays[first].base
+            if not (isinstance(b, np.ndarray) and b.ndim == 2 and b.dtype == np.float64 and b.flags.c_contiguous
+                    and b.shape[1] >= N):
+                continue
+            bp = b.__array_interface__["data"][0]
+            rb = 8 * b.shape[1]
+            off = addr - bp
+            ok = (off >= 0) & (off % rb == 0) & (off // rb < b.shape[0])
+            idx = first + np.nonzero(ok)[0]
+            if len(idx):
+                grp = groups.setdefault(id(b), [b, [], []])
+                grp[1].extend(idx.tolist())
+                grp[2].extend((off[ok] // rb).tolist())
+                grouped[idx] = True
         for i, a in enumerate(self.arrays):
-            rb = self._row_of(a, N, ptrs[i], base_ptrs)
+            if grouped[i]:
+                continue
+            rb = self._row_of(a, N, a.__array_interface__["data"][0], base_ptrs)
             if rb is not None:
                 groups.setdefault(id(rb[0]), [rb[0], [], []])
                 groups[id(rb[0])][1].append(i)
@@ -626,7 +649,7 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
     if waves is None:
         waves = WaveMatrix(N)
     if packed is not None and packed.owner is not waves and not waves.arrays:
-        packed.first, packed.owner = waves.add_distinct(packed.arrays), waves
+        packed.first, packed.owner = waves.add_distinct(packed.arrays, packed.ptrs), waves
     if packed is not None and packed.owner is waves:
         # rows of the packed waves (added to this matrix in the packed order)
         wi_idx, wf_idx = packed.rows_i + packed.first, packed.rows_f + packed.first

@@ -1,0 +1,63 @@
+"""Host packing of a batch's waves (the C extension dwba_b200._hostpack) against the Python path.
+
+pack_pairs reads every wave's scalars and numbers its chi array in one pass; the planner and the
+upload then use arrays instead of walking the wave objects. The packed scalars and rows must equal
+what the general Python path computes, a wave that does not qualify (chi not exactly N float64
+values in C order, a missing l / k_au) must send the whole call to the general path, and the rows of
+a batch's chi matrix must be grouped into one transfer by address arithmetic.
+"""
+import numpy as np
+import pytest
+import torch
+
+import bench
+from dwba_b200 import _hostpack
+from dwba_b200.dwba_matrix_elements import _pack
+from dwba_b200.engine import WaveMatrix, _pair_arrays
+
+
+def test_packed_scalars_and_rows_match_the_python_path():
+    g, z, bounds, pairs = bench.make_workload(N=501, n_cont=40, n_bound=1, seed_shift=3)
+    pairs = pairs + [pairs[3], (pairs[5][0], pairs[7][1])]  # repeated wave objects share rows
+    pk = _pack(pairs, 501)
+    assert pk is not None
+    pa = _pair_arrays(pairs)
+    for j, k in enumerate(("k_i", "l_i", "im_i", "e_i", "d_i", "s_i", "k_f", "l_f", "im_f", "e_f", "d_f", "s_f")):
+        assert np.array_equal(pk.scalars[:, j], pa[k].astype(np.float64)), k
+    w = WaveMatrix(501)
+    rows_i = [w.add(ci.chi_of_r) for ci, _ in pairs]
+    rows_f = [w.add(cf.chi_of_r) for _, cf in pairs]
+    assert list(pk.rows_i) == rows_i and list(pk.rows_f) == rows_f
+    assert len(pk.arrays) == len(w.arrays) and all(a is b for a, b in zip(pk.arrays, w.arrays))
+    assert list(pk.ptrs) == [a.__array_interface__["data"][0] for a in pk.arrays]
+
+
+@pytest.mark.parametrize("bad", ["float32", "short", "strided", "no_l", "list"])
+def test_waves_that_do_not_qualify_take_the_general_path(bad):
+    g, z, bounds, pairs = bench.make_workload(N=301, n_cont=6, n_bound=1, seed_shift=4)
+    w = pairs[2][1]
+    if bad == "float32":
+        w.chi_of_r = w.chi_of_r.astype(np.float32)
+    elif bad == "short":
+        w.chi_of_r = w.chi_of_r[:300]
+    elif bad == "strided":
+        w.chi_of_r = np.repeat(w.chi_of_r, 2)[::2]
+    elif bad == "no_l":
+        del w.l
+    else:
+        w.chi_of_r = list(w.chi_of_r)
+    assert _hostpack.pack_pairs(pairs, 301, np.ndarray) is None
+
+
+def test_upload_groups_packed_rows_by_address():
+    """The chi matrix behind a batch's waves goes as one gather; the rows match the arrays."""
+    g, z, bounds, pairs = bench.make_workload(N=257, n_cont=30, n_bound=2, seed_shift=6)
+    pk = _pack(pairs, 257)
+    w = WaveMatrix(257)
+    pk.first, pk.owner = w.add_distinct(pk.arrays, pk.ptrs), w
+    for b in bounds:
+        w.add(b[0].u_of_r)
+        w.add(b[1].u_of_r)
+    out = w.upload(torch.device("cpu")).numpy()
+    for i, a in enumerate(w.arrays):
+        assert np.array_equal(out[i], a)

@@ -33,63 +33,42 @@ __global__ void fold_kernel(const dwba_fold_t* __restrict__ folds) {
   }
 }
 
-// Multi-fold: one operator and g, several f (a pair's density products for every transition).
-// The threads of a warp take consecutive rows; each lane forms the products f_t[k] g[k] of its own
-// row once and takes its neighbours' (k = i-H .. i+H) from the neighbouring lanes by shuffles
-// (lanes at a warp edge load the missing ones), so every function value is read once per row
-// instead of 2H+1 times. Same products, operator taps and summation order as a row-by-row fold.
 template <int H>
-__device__ __forceinline__ void fold_multi_rows(const dwba_fold_multi_t* __restrict__ m, int n_f, int n_src, int n_out,
-                                                int n_clear) {
-  const int lane = threadIdx.x & 31;
-  const int stride = gridDim.x * blockDim.x;
-  const double* __restrict__ op = m->op_dev;
+__device__ __forceinline__ void fold_multi_row(const dwba_fold_multi_t* __restrict__ m, int n_f, int n_src, int i) {
+  double tap[2 * H + 1], gv[2 * H + 1];
+  const double* __restrict__ op = m->op_dev + (int64_t)(2 * H + 1) * i;
   const double* __restrict__ g = m->g_dev;
-  // warp-uniform loop: every lane of a warp takes part in the shuffles of each of its rows
-  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n_clear; base += stride) {
-    const int i = base + lane;
-    const bool row_in = i < n_src;
-    const double gi = row_in ? g[i] : 0.0;
-    double tap[2 * H + 1];
+#pragma unroll
+  for (int d = -H; d <= H; ++d) {
+    const int k = i + d;
+    const bool in = k >= 0 && k < n_src;
+    tap[d + H] = in ? op[d + H] : 0.0;
+    gv[d + H] = in ? g[k] : 0.0;
+  }
+  for (int t = 0; t < n_f; ++t) {
+    const double* __restrict__ f = m->f_dev[t];  // descriptor fields read from global memory
+    double acc = 0.0;
 #pragma unroll
     for (int d = -H; d <= H; ++d) {
       const int k = i + d;
-      tap[d + H] = (i < n_out && k >= 0 && k < n_src) ? op[(int64_t)(2 * H + 1) * i + d + H] : 0.0;
+      if (k >= 0 && k < n_src) acc += tap[d + H] * (f[k] * gv[d + H]);
     }
-    for (int t = 0; t < n_f; ++t) {
-      const double* __restrict__ f = m->f_dev[t];
-      const double pi = row_in ? f[i] * gi : 0.0;
-      double pv[2 * H + 1];
-      pv[H] = pi;
-#pragma unroll
-      for (int d = 1; d <= H; ++d) {
-        const double up = __shfl_up_sync(0xffffffffu, pi, d);    // row i - d
-        const double dn = __shfl_down_sync(0xffffffffu, pi, d);  // row i + d
-        const int ku = i - d, kd = i + d;
-        pv[H - d] = lane >= d ? up : ((ku >= 0 && ku < n_src) ? f[ku] * g[ku] : 0.0);
-        pv[H + d] = lane + d < 32 ? dn : ((kd >= 0 && kd < n_src) ? f[kd] * g[kd] : 0.0);
-      }
-      if (i < n_out) {
-        double acc = 0.0;
-#pragma unroll
-        for (int d = -H; d <= H; ++d) {
-          const int k = i + d;
-          if (k >= 0 && k < n_src) acc += tap[d + H] * pv[d + H];
-        }
-        m->out_dev[t][i] = acc;
-      } else if (i < n_clear) {
-        m->out_dev[t][i] = 0.0;
-      }
-    }
+    m->out_dev[t][i] = acc;
   }
 }
 
 __global__ void fold_multi_kernel(const dwba_fold_multi_t* __restrict__ folds) {
   const dwba_fold_multi_t* __restrict__ m = folds + blockIdx.y;
   const int n_f = m->n_f, H = m->half_band, n_out = m->n_out, n_src = m->n_src, n_clear = m->n_clear;
-  if (H == 0) fold_multi_rows<0>(m, n_f, n_src, n_out, n_clear);
-  else if (H == 1) fold_multi_rows<1>(m, n_f, n_src, n_out, n_clear);
-  else fold_multi_rows<2>(m, n_f, n_src, n_out, n_clear);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_clear; i += gridDim.x * blockDim.x) {
+    if (i < n_out) {
+      if (H == 0) fold_multi_row<0>(m, n_f, n_src, i);
+      else if (H == 1) fold_multi_row<1>(m, n_f, n_src, i);
+      else fold_multi_row<2>(m, n_f, n_src, i);
+    } else {
+      for (int t = 0; t < n_f; ++t) m->out_dev[t][i] = 0.0;
+    }
+  }
 }
 
 #ifndef DWBA_FOLD_THREADS

@@ -551,20 +551,24 @@ class WaveMatrix:
                 groups[id(rb[0])][2].append(rb[1])
         big = []
         for base, idx, rows in groups.values():
-            if len(idx) < 2 or 2 * len(set(rows)) < base.shape[0]:
-                continue  # a small share of a large matrix: per-row copies below
-            big.append((base, idx, rows))
+            # the contiguous block of the matrix's rows that the group spans goes as one copy when
+            # the group uses at least half of it (e.g. all pairs of a batch, or one chunk of them)
+            r_arr = np.asarray(rows, dtype=np.int64)
+            lo, hi = int(r_arr.min()), int(r_arr.max()) + 1
+            if len(idx) < 2 or 2 * len(np.unique(r_arr)) < hi - lo:
+                continue  # a small share of its span: per-row copies below
+            big.append((base[lo:hi], idx, r_arr - lo))
             done[idx] = True
         # every small (synchronous) copy first -- the rows outside the grouped matrices and the
         # index arrays of the gathers -- so that none of them waits behind a large asynchronous
-        # copy in the stream; the grouped matrices (asynchronous from pinned memory) last
+        # copy in the stream; the grouped blocks (asynchronous from pinned memory) last
         self._copy_rows(out, done, N, n)
-        gathers = [(torch.as_tensor(np.asarray(rows, dtype=np.int64), device=device),
-                    torch.as_tensor(np.asarray(idx, dtype=np.int64), device=device), base) for base, idx, rows in big]
-        for sel, dst, base in gathers:
-            src = torch.from_numpy(base)
-            dev_base = src.to(device, non_blocking=src.is_pinned())
-            out.index_copy_(0, dst, dev_base.index_select(0, sel)[:, :N])
+        gathers = [(torch.as_tensor(rows, device=device),
+                    torch.as_tensor(np.asarray(idx, dtype=np.int64), device=device), block) for block, idx, rows in big]
+        for sel, dst, block in gathers:
+            src = torch.from_numpy(block)
+            dev_block = src.to(device, non_blocking=src.is_pinned())
+            out.index_copy_(0, dst, dev_block.index_select(0, sel)[:, :N])
         self._uploaded[str(device)] = (n, out)
         return out
 

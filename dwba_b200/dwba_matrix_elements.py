@@ -294,10 +294,6 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
     from . import tune
     cache = _cache_for(grid, gpu_cache)
     eng = _engine_name(engine)
-    if semantics == "cpu" and eng in ("semisep", "dense") and len(pairs) >= 2 * PIPELINE_PAIRS:
-        I_dir, I_exc = _run_pipelined(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw,
-                                      cache, eng)
-        return (I_dir, I_exc) if as_arrays else _results(I_dir, I_exc)
     job = _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, cache)
     with torch.cuda.device(cache.device):
         if semantics == "cupy":
@@ -321,28 +317,6 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
     if as_arrays:
         return I_dir, I_exc
     return _results(I_dir, I_exc)
-
-
-PIPELINE_PAIRS = 512  # pairs per chunk of a pipelined batch
-
-
-def _run_pipelined(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, cache, eng):
-    """A large batch on an exact engine in chunks of PIPELINE_PAIRS pairs: each chunk is planned,
-    prepared and launched while the kernels of the previous ones run, and the results are read once
-    all are launched. Every integral is evaluated exactly as in one call (each form, correction and
-    tail depends on its own pair only), so the results equal the unchunked call's bit for bit."""
-    import torch
-    from .engine import PreparedJob, plan_job
-    parts = []
-    with torch.cuda.device(cache.device):
-        for c0 in range(0, len(pairs), PIPELINE_PAIRS):
-            job = _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs[c0:c0 + PIPELINE_PAIRS], L_max,
-                            U_f_array, kw, cache)
-            pj = PreparedJob(job, cache.dg, eng, plans=plan_job(job, _early_upload(job, cache.device)))
-            pj.launch()
-            parts.append(pj)
-        outs = [pj.collect() for pj in parts]
-    return np.concatenate([o[0] for o in outs], axis=1), np.concatenate([o[1] for o in outs], axis=1)
 
 
 def radial_ME_all_L(grid, V_core_array, U_i_array, bound_i, bound_f, cont_i, cont_f, L_max: int,

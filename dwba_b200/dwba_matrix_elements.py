@@ -270,8 +270,23 @@ def _early_upload(job, device):
     return waves
 
 
-def _results(I_dir: np.ndarray, I_exc: np.ndarray):
-    """(T, P, L_max+1) arrays -> results[t][p] as RadialDWBAIntegrals of Python floats."""
+def _skeleton(T: int, P: int, nl: int):
+    """results[t][p] as RadialDWBAIntegrals whose dicts hold the keys 0..nl-1 and no values yet,
+    with the list of those dicts, made while the device computes (None without the extension)."""
+    if _hostpack is None:
+        return None
+    return _hostpack.make_results(RadialDWBAIntegrals, int(T), int(P), int(nl))
+
+
+def _results(I_dir: np.ndarray, I_exc: np.ndarray, skeleton=None):
+    """(T, P, L_max+1) arrays -> results[t][p] as RadialDWBAIntegrals of Python floats (the values
+    filled into ``skeleton`` from _skeleton when given)."""
+    T, P, nl = I_dir.shape
+    if _hostpack is not None and I_exc.shape == I_dir.shape:
+        res, dicts = skeleton if skeleton is not None else _skeleton(T, P, nl)
+        _hostpack.fill_results(dicts, np.ascontiguousarray(I_dir, dtype=np.float64),
+                               np.ascontiguousarray(I_exc, dtype=np.float64), nl)
+        return res
     d, e = I_dir.tolist(), I_exc.tolist()
     return [[RadialDWBAIntegrals(I_L_direct=dict(enumerate(dp)), I_L_exchange=dict(enumerate(ep)))
              for dp, ep in zip(dt, et)] for dt, et in zip(d, e)]
@@ -309,14 +324,15 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
             _, pj = tune.TUNER.select(key, cands, lambda e: PreparedJob(job, cache.dg, e, plans=plans),
                                       lambda p: p.launch())
             pj.launch()
-            I_dir, I_exc = pj.collect()
         else:
             pj = PreparedJob(job, cache.dg, eng, plans=plans)
             pj.launch()
-            I_dir, I_exc = pj.collect()
+        # the result objects are made while the kernels run; collect() then waits for them
+        skel = None if as_arrays else _skeleton(len(job.transitions), len(job.pairs), job.L_max + 1)
+        I_dir, I_exc = pj.collect()
     if as_arrays:
         return I_dir, I_exc
-    return _results(I_dir, I_exc)
+    return _results(I_dir, I_exc, skel)
 
 
 def radial_ME_all_L(grid, V_core_array, U_i_array, bound_i, bound_f, cont_i, cont_f, L_max: int,

@@ -61,3 +61,28 @@ def test_upload_groups_packed_rows_by_address():
     out = w.upload(torch.device("cpu")).numpy()
     for i, a in enumerate(w.arrays):
         assert np.array_equal(out[i], a)
+
+
+def test_result_objects_match_the_python_path():
+    """make_results + fill_results give the same RadialDWBAIntegrals (frozen, {L: float} dicts in L
+    order) as constructing them in Python, and reject arrays of the wrong size."""
+    import dataclasses
+    from dwba_b200 import dwba_matrix_elements as dme
+    rng = np.random.default_rng(12)
+    for T, P, nl in ((1, 1, 1), (3, 17, 9), (2, 5, 300)):
+        I_d, I_e = rng.standard_normal((T, P, nl)), rng.standard_normal((T, P, nl))
+        fast = dme._results(I_d, I_e, dme._skeleton(T, P, nl))
+        ref = [[dme.RadialDWBAIntegrals(I_L_direct={L: float(I_d[t, p, L]) for L in range(nl)},
+                                        I_L_exchange={L: float(I_e[t, p, L]) for L in range(nl)})
+                for p in range(P)] for t in range(T)]
+        assert fast == ref
+        x = fast[-1][-1]
+        assert type(x) is dme.RadialDWBAIntegrals and list(x.I_L_direct) == list(range(nl))
+        assert all(type(v) is float for v in x.I_L_exchange.values())
+        with pytest.raises(dataclasses.FrozenInstanceError):
+            x.I_L_direct = {}
+    _, dicts = dme._skeleton(2, 3, 4)
+    with pytest.raises(ValueError):
+        _hostpack.fill_results(dicts, np.zeros(2 * 3 * 4 - 1), np.zeros(2 * 3 * 4), 4)
+    with pytest.raises(ValueError):
+        _hostpack.fill_results(dicts, np.zeros(24, dtype=np.float32), np.zeros(24), 4)

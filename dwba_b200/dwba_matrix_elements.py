@@ -266,7 +266,7 @@ def _early_upload(job, device):
     for t in job.transitions:
         waves.add(t.u_i)
         waves.add(t.u_f)
-    waves.upload(device)
+    waves.upload(device, side_stream=True)  # the kernels' launch waits for it (WaveMatrix.wait_ready)
     return waves
 
 

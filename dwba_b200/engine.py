@@ -10,9 +10,13 @@ launch; the L=0 corrections and the outer tails are added in FP64 on the host.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 from dataclasses import dataclass, field
+import functools
 import hashlib
+from itertools import repeat
+import operator
 from typing import Dict, List, NamedTuple, Optional, Sequence, Tuple
 
 import numpy as np
@@ -97,7 +101,14 @@ def _stream() -> int:
 
 
 def _dev(x: np.ndarray, device) -> torch.Tensor:
-    return torch.from_numpy(np.ascontiguousarray(x)).to(device, non_blocking=False)
+    """A host array on the device. To a GPU it goes through pinned staging memory as an
+    asynchronous copy on the current stream, so that the host does not wait while a large transfer
+    occupies the copy engine (the staging block is held by torch's pinned allocator until the copy
+    has run; later changes to ``x`` do not reach the copy)."""
+    t = torch.from_numpy(np.ascontiguousarray(x))
+    if torch.device(device).type != "cuda":
+        return t.to(device)
+    return t.pin_memory().to(device, non_blocking=True)
 
 
 class DeviceGrid:
@@ -150,6 +161,9 @@ class CCTables:
         return v
 
 
+_KEY_N1 = operator.itemgetter(1)  # NodeSetKey.n1
+
+
 class NodeSetBatch:
     """Descriptors of the node sets a job uses; ``launch()`` (re)builds their banded operators.
 
@@ -170,15 +184,14 @@ class NodeSetBatch:
         self.fused_recs = None
         self.fused_folds_d = None
         if self.n_fused:
-            fp = [plans[i] for i in self.fused_idx]
+            fp = list(map(plans.__getitem__, self.fused_idx.tolist()))
+            f_key, f_nb, f_br, f_l1, f_l2 = zip(*fp)  # fields of every fused set, without a Python loop
             fr = np.zeros(self.n_fused, dtype=_lib.NODESET_DTYPE)
             fr["r"], fr["logr"] = _ptr(dg.r), _ptr(dg.logr)
-            fr["n_grid"], fr["n1"] = N, [p.key.n1 for p in fp]
-            fr["n_breaks"] = [p.n_breaks for p in fp]
-            fr["log1"] = [int(p.log1) for p in fp]
-            fr["log2"] = [int(p.log2) for p in fp]
-            self._fused_breaks = [p.breaks for p in fp]
-            if any(b is not None for b in self._fused_breaks):
+            fr["n_grid"], fr["n1"] = N, list(map(_KEY_N1, f_key))
+            fr["n_breaks"], fr["log1"], fr["log2"] = f_nb, f_l1, f_l2
+            self._fused_breaks = f_br
+            if any(map(operator.is_not, f_br, repeat(None))):
                 br_len = np.array([0 if b is None else len(b) for b in self._fused_breaks], dtype=np.int64)
                 self._fused_br = _dev(np.concatenate([np.asarray(b, dtype=np.float64) for b in self._fused_breaks
                                                       if b is not None]), dev)
@@ -189,8 +202,8 @@ class NodeSetBatch:
             self.fused_recs_d = _dev(fr.view(np.uint8), dev)
             self.fccx, self.fccw = CCTables.get(n_cc, dev)
             self.fused_status = torch.zeros(1, dtype=torch.int32, device=dev)
-        plans = [p for i, p in enumerate(plans) if not fused[i]]
         keep = np.nonzero(~fused)[0]
+        plans = list(map(plans.__getitem__, keep.tolist()))
         cached = [cache.get(p.key) for p in plans]
         todo = plans if rebuild else [p for p, c in zip(plans, cached) if c is None]
         self.n = len(todo)
@@ -389,27 +402,38 @@ def _pair_arrays(pairs):
     return {k: np.ascontiguousarray(v) for k, v in out.items()}
 
 
-def _idx_limits(job: Job, pa, t: Transition, cupy: bool = False) -> np.ndarray:
+def _idx_limits(job: Job, pa, t: Transition, cupy: bool = False, memo: Optional[dict] = None) -> np.ndarray:
     """Vectorised ``idx_limit`` (dwba_matrix_elements.py:909-1022) for every pair of one transition.
     ``cupy``: the CuPy path's rule (``:1676-1720``, ``_refine_idx_limit_physics`` :688-777), which counts the
-    final state's extent only for a bound final state."""
+    final state's extent only for a bound final state. ``memo``: a dict shared by the transitions of
+    one job: the transition enters only through the bound states' 99 % extent, so the pair-only part
+    is computed once and a transition whose extent changes no pair's limit reuses the result."""
     g = job.grid
     N, r = g.N, g.r
-    n1 = np.full(len(pa["k_i"]), N, dtype=np.int64)
-    for im in (pa["im_i"], pa["im_f"]):
-        m = (im > 0) & (im < N)
-        n1 = np.where(m, np.minimum(n1, im + 1), n1)
-    kmin = np.minimum(pa["k_i"], pa["k_f"])
-    kmax = np.maximum(pa["k_i"], pa["k_f"])
-    k_eff = np.where(kmin > 0.1, kmin, kmax)
-    lmax = np.maximum(pa["l_i"], pa["l_f"])
-    with np.errstate(divide="ignore", invalid="ignore"):
-        r_turn = (lmax + 0.5) / k_eff
-    idx_turn = np.minimum(np.searchsorted(r, np.where(k_eff > 1e-3, r_turn, 0.0)), N - 20)
-    mgf = int(N * job.min_grid_fraction)
-    min_idx = np.where(k_eff > 1e-3, np.minimum(np.maximum(idx_turn + 20, mgf), N), max(1, mgf))
-    n1 = np.where(n1 < min_idx, min_idx, n1)
+    base = memo.get("base") if memo is not None else None
+    if base is None:
+        n1 = np.full(len(pa["k_i"]), N, dtype=np.int64)
+        for im in (pa["im_i"], pa["im_f"]):
+            m = (im > 0) & (im < N)
+            n1 = np.where(m, np.minimum(n1, im + 1), n1)
+        kmin = np.minimum(pa["k_i"], pa["k_f"])
+        kmax = np.maximum(pa["k_i"], pa["k_f"])
+        k_eff = np.where(kmin > 0.1, kmin, kmax)
+        lmax = np.maximum(pa["l_i"], pa["l_f"])
+        with np.errstate(divide="ignore", invalid="ignore"):
+            r_turn = (lmax + 0.5) / k_eff
+        idx_turn = np.minimum(np.searchsorted(r, np.where(k_eff > 1e-3, r_turn, 0.0)), N - 20)
+        mgf = int(N * job.min_grid_fraction)
+        min_idx = np.where(k_eff > 1e-3, np.minimum(np.maximum(idx_turn + 20, mgf), N), max(1, mgf))
+        n1 = np.where(n1 < min_idx, min_idx, n1)
+        base = (n1, kmin, lmax, int(n1.min()) if len(n1) else N)
+        if memo is not None:
+            memo["base"] = base
+    n1, kmin, lmax, n1_min = base
     idx99 = max(0, g.extent99(t.u_i), g.extent99(t.u_f) if (t.excitation or not cupy) else 0)
+    key = idx99 if idx99 > n1_min else -1  # -1: the extent moves no limit
+    if memo is not None and key in memo:
+        return memo[key].copy()
     n1 = np.where(idx99 > n1, min(N, idx99 + 1), n1)
     ke = 0.5 * kmin ** 2
     uabs = np.abs(job.U_i) if job.U_f is None else np.maximum(np.abs(job.U_i), np.abs(job.U_f))
@@ -427,6 +451,8 @@ def _idx_limits(job: Job, pa, t: Transition, cupy: bool = False) -> np.ndarray:
         has = ok.any(axis=1)
         first = np.argmax(ok, axis=1)
         n1[sel] = np.where(has, T[np.arange(len(sel)), first] + 1, n1[sel])
+    if memo is not None:
+        memo[key] = n1.copy()
     return n1
 
 
@@ -452,6 +478,19 @@ def _dphis(job: Job, n1: np.ndarray, k_total: np.ndarray, eta_total: np.ndarray)
     return d
 
 
+_COPY_STREAMS: Dict[int, "torch.cuda.Stream"] = {}
+
+
+def _copy_stream(device) -> "torch.cuda.Stream":
+    """A side stream per device for large host-to-device transfers."""
+    idx = torch.device(device).index
+    idx = torch.cuda.current_device() if idx is None else idx
+    st = _COPY_STREAMS.get(idx)
+    if st is None:
+        st = _COPY_STREAMS[idx] = torch.cuda.Stream(device=idx)
+    return st
+
+
 class WaveMatrix:
     """Distinct 1-D functions of a job as rows of one host matrix (dedup by host buffer)."""
 
@@ -462,6 +501,14 @@ class WaveMatrix:
         self._by_id: Dict[int, int] = {}
         self._keep: List[object] = []
         self._ptrs: Dict[int, Tuple[int, np.ndarray]] = {}  # first row -> (count, data addresses)
+        self.ready: Optional[torch.cuda.Event] = None  # end of a side-stream upload not yet waited for
+
+    def wait_ready(self) -> None:
+        """Order the current stream after a side-stream upload (``upload(..., side_stream=True)``);
+        the kernels' launchers call it before their first launch."""
+        if self.ready is not None:
+            torch.cuda.current_stream().wait_event(self.ready)
+            self.ready = None
 
     def add_distinct(self, arrays: Sequence[np.ndarray], ptrs: Optional[np.ndarray] = None) -> int:
         """Append arrays known to be distinct C-contiguous objects of N float64 values that are not
@@ -510,10 +557,15 @@ class WaveMatrix:
             return None
         return b, off // rb
 
-    def upload(self, device) -> torch.Tensor:
+    def upload(self, device, side_stream: bool = False) -> torch.Tensor:
         """Copy every row to the device. Rows taken from one C-contiguous host matrix (in any
         order) are copied with that matrix in one transfer (asynchronous when it is pinned) and
-        gathered on the device; other rows that are consecutive in memory go as one block."""
+        gathered on the device; other rows that are consecutive in memory go as one block.
+
+        ``side_stream``: the large transfers and their gathers run on a copy stream of the device,
+        so that the small synchronous copies the caller issues meanwhile (descriptors) do not wait
+        behind them in the current stream; ``ready`` records their end, and whoever launches
+        kernels reading the matrix calls ``wait_ready()`` first."""
         N = self.N
         n = len(self.arrays)
         cached = self._uploaded.get(str(device))
@@ -563,12 +615,25 @@ class WaveMatrix:
         # index arrays of the gathers -- so that none of them waits behind a large asynchronous
         # copy in the stream; the grouped blocks (asynchronous from pinned memory) last
         self._copy_rows(out, done, N, n)
-        gathers = [(torch.as_tensor(rows, device=device),
-                    torch.as_tensor(np.asarray(idx, dtype=np.int64), device=device), block) for block, idx, rows in big]
-        for sel, dst, block in gathers:
-            src = torch.from_numpy(block)
-            dev_block = src.to(device, non_blocking=src.is_pinned())
-            out.index_copy_(0, dst, dev_block.index_select(0, sel)[:, :N])
+        side = bool(side_stream and big and out.is_cuda)
+        if side:
+            cs = _copy_stream(out.device)
+            cs.wait_stream(torch.cuda.current_stream(out.device))  # out belongs to the current stream
+            ctx = torch.cuda.stream(cs)
+        else:
+            ctx = contextlib.nullcontext()
+        with ctx:
+            gathers = [(torch.as_tensor(rows, device=device),
+                        torch.as_tensor(np.asarray(idx, dtype=np.int64), device=device), block)
+                       for block, idx, rows in big]
+            for sel, dst, block in gathers:
+                src = torch.from_numpy(block)
+                dev_block = src.to(device, non_blocking=src.is_pinned())
+                out.index_copy_(0, dst, dev_block.index_select(0, sel)[:, :N])
+        if side:
+            out.record_stream(cs)
+            self.ready = torch.cuda.Event()
+            self.ready.record(cs)
         self._uploaded[str(device)] = (n, out)
         return out
 
@@ -635,6 +700,25 @@ class JobPlan:
                         tail=self.tails.get((t, p)))
 
 
+def _unique_rows(a: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """np.unique(a, axis=0, return_inverse=True) for a 2-D float array: the distinct rows in
+    lexicographic order and the row of each input among them (by a stable lexsort of the columns,
+    which is several times faster than numpy's structured-row sort; same result)."""
+    order = np.lexsort(a.T[::-1])
+    srt = a[order]
+    new = np.ones(len(a), dtype=bool)
+    if len(a) > 1:
+        new[1:] = np.any(srt[1:] != srt[:-1], axis=1)
+    grp = np.cumsum(new) - 1
+    inv = np.empty(len(a), dtype=np.int64)
+    inv[order] = grp
+    return srt[new], inv
+
+
+_new_key = functools.partial(tuple.__new__, NodeSetKey)  # from one tuple of the fields, no Python frame
+_new_plan = functools.partial(tuple.__new__, NodeSetPlan)
+
+
 def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
     """Host planning (vectorised over pairs): integration limit, branch, node set, L=0
     corrections and outer tails for every (transition, pair)."""
@@ -669,18 +753,19 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
     moments_all = np.zeros((T, job.L_max + 1))
     nodesets: List[NodeSetPlan] = []
     ns_pos: Dict[NodeSetKey, int] = {}
+    idx_memo: dict = {}
     for ti, t in enumerate(job.transitions):
-        n1 = _idx_limits(job, pa, t)
+        n1 = _idx_limits(job, pa, t, memo=idx_memo)
         n1_all[ti] = n1
-        d = _dphis(job, n1, k_total, eta_total)
         # distinct node sets of this transition (pairs of one energy share k_total and eta); a
         # transition with the same integration limits as the previous one has the same node sets
         cand = np.nonzero(osc & (n1 >= 2))[0]
         if ti > 0 and np.array_equal(n1, n1_all[ti - 1]):
             ns_index[ti] = ns_index[ti - 1]
         elif len(cand):
+            d = _dphis(job, n1, k_total, eta_total)
             keys = np.stack([n1[cand].astype(np.float64), k_total[cand], d[cand], eta_total[cand]], axis=1)
-            uk, inv = np.unique(keys, axis=0, return_inverse=True)
+            uk, inv = _unique_rows(keys)
             pos = np.empty(len(uk), dtype=np.int64)
             # breakpoint counts of the linspace (eta == 0) sets for all keys at once, with the
             # arithmetic of plan_nodeset; Coulomb sets go through plan_nodeset one by one
@@ -690,8 +775,21 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
                 n_lin = np.ceil(span / (uk[:, 2] / uk[:, 1])) + 1
                 step = span / (n_lin - 1)
             lin_ok = (uk[:, 1] >= 1e-10) & (n_lin >= 2) & (step > 1e-12)
-            for u, rec in enumerate(uk.tolist()):
-                key = NodeSetKey(id(g), int(rec[0]), rec[1], rec[2], rec[3], int(job.CC_nodes))
+            keys = list(map(_new_key, zip(repeat(id(g)), u_n1.tolist(), uk[:, 1].tolist(), uk[:, 2].tolist(),
+                                          uk[:, 3].tolist(), repeat(int(job.CC_nodes)))))
+            if bool(np.all(np.abs(uk[:, 3]) < 1e-10)) and not any(map(ns_pos.__contains__, keys)):
+                # linspace sets only, none seen before (the usual case): built in bulk, in key order
+                ok = np.nonzero(lin_ok)[0]
+                pos[:] = -1
+                pos[ok] = len(nodesets) + np.arange(len(ok))
+                nodesets.extend(map(_new_plan, zip([keys[u] for u in ok.tolist()],
+                                                   n_lin[ok].astype(np.int64).tolist(), repeat(None),
+                                                   g.log_prefixes(u_n1[ok].tolist()),
+                                                   repeat(g.log_full))))
+                ns_pos.update(zip(keys, pos.tolist()))
+                keys = ()
+            for u, key in enumerate(keys):
+                rec = key[1:5]  # n1, k_total, dphi, eta_total
                 q = ns_pos.get(key)
                 if q is None:
                     if abs(rec[3]) < 1e-10:
@@ -756,6 +854,22 @@ def plan_job(job: Job, waves: Optional[WaveMatrix] = None) -> JobPlan:
                    tail_rm=np.array(dev_rm, dtype=np.float64), tail_rmax=np.array(dev_rmax, dtype=np.float64),
                    tail_mode=np.full(nd, 1 if legacy else 0, dtype=np.int32), moments=moments_all,
                    tail_limits=(max_seg, max_dphi))
+
+
+def _take(a: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    """a[idx] for a structured descriptor array, copied as raw rows (numpy copies structured
+    records field by field, which costs milliseconds for a few thousand descriptors)."""
+    rows = a.view(np.uint8).reshape(len(a), a.dtype.itemsize)
+    return rows[idx].view(a.dtype).reshape(-1)
+
+
+def _interleave(x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    """[x0, y0, x1, y1, ...] for two structured arrays of one dtype and length, as raw rows."""
+    n, isz = len(x), x.dtype.itemsize
+    out = np.empty((2 * n, isz), dtype=np.uint8)
+    out[0::2] = x.view(np.uint8).reshape(n, isz)
+    out[1::2] = y.view(np.uint8).reshape(n, isz)
+    return out.view(x.dtype).reshape(-1)
 
 
 def expand_multi(multi: np.ndarray) -> np.ndarray:
@@ -833,7 +947,7 @@ class FormLaunch:
                 d["stride"] = N
                 dots.append(d)
             if len(pl.ss_fo):
-                ss_forms.append(fh[pl.ss_fo])
+                ss_forms.append(_take(fh, pl.ss_fo))
                 ss_rows.append(np.asarray(ss_out, dtype=np.int64))
         pots = np.concatenate(pots) if pots else np.zeros(0, dtype=_lib.POTENTIAL_DTYPE)
         dots = np.concatenate(dots) if dots else np.zeros(0, dtype=_lib.DOT_DTYPE)
@@ -973,6 +1087,7 @@ class PreparedJob:
             wi_idx = np.array([waves.add(ci.chi_of_r) for ci, _ in job.pairs], dtype=np.int64)
             wf_idx = np.array([waves.add(cf.chi_of_r) for _, cf in job.pairs], dtype=np.int64)
         tidx = [(waves.add(t.u_i), waves.add(t.u_f)) for t in job.transitions]
+        self.waves = waves
         self.wave_rows = (np.asarray(wi_idx), np.asarray(wf_idx), tidx)
         self.F = F = waves.upload(dev)
         self.h2d_bytes = len(waves.arrays) * N * 8
@@ -1085,8 +1200,7 @@ class PreparedJob:
             forms["a"][fo_a] = adir_a[first][gid]
             # T and B multi-folds of one pair launched next to each other, so that the continuum
             # wave both read (chi_f) is still in L2 for the second
-            multi = np.empty(2 * G, dtype=_lib.FOLD_MULTI_DTYPE)
-            multi[0::2], multi[1::2] = mT, mB
+            multi = _interleave(mT, mB)
             ns = self.nodesets
             if ns.n_fused:
                 # the groups of fused sets (one per set) go with the node-set launch, in its order
@@ -1096,11 +1210,9 @@ class PreparedJob:
                 fg = q >= 0
                 if int(np.count_nonzero(fg)) != ns.n_fused or len(np.unique(q[fg])) != ns.n_fused:
                     raise RuntimeError("fused node sets must serve exactly one multi-fold group each")
-                ff = np.empty(2 * ns.n_fused, dtype=_lib.FOLD_MULTI_DTYPE)
-                ff[2 * q[fg]], ff[2 * q[fg] + 1] = mT[fg], mB[fg]
-                ns.set_fused_folds(ff)
-                keep_g = np.repeat(~fg, 2)
-                multi = multi[keep_g]
+                sel = np.nonzero(fg)[0][np.argsort(q[fg], kind="stable")]  # groups in node-set order
+                ns.set_fused_folds(_interleave(_take(mT, sel), _take(mB, sel)))
+                multi = _take(multi, np.nonzero(np.repeat(~fg, 2))[0])
         elif self.nodesets.n_fused:
             raise RuntimeError("fused node sets without multi-folds")
         self.multi_host = multi
@@ -1245,6 +1357,7 @@ class PreparedJob:
             self.form_launch.launch(lib, job.L_max, self.ds, float(job.grid.r[0]), float(job.grid.r[-1]))
 
     def launch(self) -> None:
+        self.waves.wait_ready()
         self.nodesets.launch()
         self.launch_folds()
         self.launch_forms()
@@ -1486,6 +1599,8 @@ class MultiPrepared:
                 ev = torch.cuda.Event(enable_timing=True)
                 ev.record(torch.cuda.current_stream())
                 marks.append((name, ev))
+        for p in self.parts:
+            p.waves.wait_ready()
         mark("start")
         if self.n_sets:
             for s0 in range(0, self.n_sets, 65535):

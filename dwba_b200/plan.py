@@ -9,7 +9,7 @@ from __future__ import annotations
 
 import math
 import os
-from typing import NamedTuple, Optional, Tuple
+from typing import List, NamedTuple, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -79,6 +79,13 @@ class GridInfo:
             v = is_log_spaced(self.r[:n])
             self._log_prefix[n] = v
         return v
+
+    def log_prefixes(self, ns: Sequence[int]) -> List[bool]:
+        """log_prefix(n) for every n of a list (cached values looked up in bulk)."""
+        out = list(map(self._log_prefix.get, ns))
+        if None in out:
+            out = [self.log_prefix(n) if v is None else v for n, v in zip(ns, out)]
+        return out
 
     def extent99(self, u: np.ndarray) -> int:
         """Index of 99 % cumulative |u|^2 (dwba_matrix_elements.py:949-960); -1 if u is ~0."""

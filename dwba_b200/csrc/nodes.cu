@@ -74,31 +74,46 @@ constexpr int OWN_ROWS = 30;
 // of its set (folds[2 set] with the tridiagonal T, folds[2 set + 1] with the band B), with the
 // arithmetic of fold_multi_kernel, and writes the folded operands instead.
 template <int H>
-__device__ __forceinline__ void fold_row_from_taps(const dwba_fold_multi_t* __restrict__ m, int i, const double* tap) {
-  if (i >= m->n_clear) return;
-  const int n_f = m->n_f, n_src = m->n_src;
-  if (i >= m->n_out) {
-    for (int t = 0; t < n_f; ++t) m->out_dev[t][i] = 0.0;
+__device__ __forceinline__ void fold_row_from_taps(const dwba_fold_multi_t& m, int i, const double* tap) {
+  if (i >= m.n_clear) return;
+  const int n_f = m.n_f, n_src = m.n_src;
+  if (i >= m.n_out) {
+    for (int t = 0; t < n_f; ++t) m.out_dev[t][i] = 0.0;
     return;
   }
-  const double* __restrict__ g = m->g_dev;
+  const double* __restrict__ g = m.g_dev;
   double tp[2 * H + 1], gv[2 * H + 1];
+  bool in[2 * H + 1];
 #pragma unroll
   for (int d = -H; d <= H; ++d) {
     const int k = i + d;
-    const bool in = k >= 0 && k < n_src;
-    tp[d + H] = in ? tap[d + H] : 0.0;
-    gv[d + H] = in ? g[k] : 0.0;
+    in[d + H] = k >= 0 && k < n_src;
+    tp[d + H] = in[d + H] ? tap[d + H] : 0.0;
+    gv[d + H] = in[d + H] ? g[k] : 0.0;
   }
-  for (int t = 0; t < n_f; ++t) {
-    const double* __restrict__ f = m->f_dev[t];
-    double acc = 0.0;
+  // factors in chunks of FC: every tap load of a chunk is issued before its products, so the loads
+  // are in flight together instead of one factor's after the previous factor's store (the stores
+  // could alias the next factor's array for all the compiler knows)
+  constexpr int FC = 4;
+  for (int t0 = 0; t0 < n_f; t0 += FC) {
+    double fv[FC][2 * H + 1];
 #pragma unroll
-    for (int d = -H; d <= H; ++d) {
-      const int k = i + d;
-      if (k >= 0 && k < n_src) acc += tp[d + H] * (f[k] * gv[d + H]);
+    for (int c = 0; c < FC; ++c) {
+      const bool live = t0 + c < n_f;
+      const double* __restrict__ f = live ? m.f_dev[t0 + c] : g;
+#pragma unroll
+      for (int d = -H; d <= H; ++d) fv[c][d + H] = (live && in[d + H]) ? f[i + d] : 0.0;
     }
-    m->out_dev[t][i] = acc;
+#pragma unroll
+    for (int c = 0; c < FC; ++c) {
+      if (t0 + c < n_f) {
+        double acc = 0.0;
+#pragma unroll
+        for (int d = -H; d <= H; ++d)
+          if (in[d + H]) acc += tp[d + H] * (fv[c][d + H] * gv[d + H]);
+        m.out_dev[t0 + c][i] = acc;
+      }
+    }
   }
 }
 
@@ -109,10 +124,17 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
                                                               int* status,
                                                               const dwba_fold_multi_t* __restrict__ folds) {
   __shared__ double ccw[MAX_CC], ccx1[MAX_CC];
+  // the set's two multi-fold descriptors (T, then B), read by every row of the CTA
+  __shared__ dwba_fold_multi_t fm[FOLD ? 2 : 1];
   const int n_cc = NCC > 0 ? NCC : n_cc_rt;
   if (threadIdx.x < n_cc) {
     ccw[threadIdx.x] = ccw_g[threadIdx.x];
     ccx1[threadIdx.x] = rn_add(ccx_g[threadIdx.x], 1.0);
+  }
+  if (FOLD) {
+    constexpr int W = (int)(2 * sizeof(dwba_fold_multi_t) / sizeof(unsigned long long));
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(folds + 2 * (int64_t)blockIdx.y);
+    for (int w = threadIdx.x; w < W; w += blockDim.x) reinterpret_cast<unsigned long long*>(fm)[w] = src[w];
   }
   __syncthreads();
   const dwba_nodeset_t d = sets[blockIdx.y];
@@ -331,13 +353,12 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
       const double t2 = q_up + o_up;
       const double b1 = q_b1, b2 = q_b2 + o_b2, b3 = q_b3 + o_b3, b4 = o_b4;
       if (FOLD) {
-        const dwba_fold_multi_t* mt = folds + 2 * (int64_t)blockIdx.y;
         if (g < n1) {
           const double tt[3] = {t0, t1, t2};
-          fold_row_from_taps<1>(mt, g, tt);
+          fold_row_from_taps<1>(fm[0], g, tt);
         }
         const double bb[5] = {0.0, b1, b2, b3, b4};
-        fold_row_from_taps<2>(mt + 1, g, bb);
+        fold_row_from_taps<2>(fm[FOLD ? 1 : 0], g, bb);
       } else {
         if (g < n1) {
           d.ta_dev[3 * g + 0] = t0;

@@ -67,9 +67,23 @@ constexpr int OWN_ROWS = 30;
 #ifndef DWBA_NODESET_FILL
 #define DWBA_NODESET_FILL 32 // resident-CTA waves the launch aims for
 #endif
+// resident CTAs per SM the register budget is set for: 24 (80 registers) for the stored-operator
+// kernel; 32 (64 registers, a few spills) for the one applied at once to the folds, where the
+// extra warps hide more of the fold loads' latency than the spills cost (2.49 ms against 2.60 ms
+// on the 2048-set batch, bit-identical; 2 or 4 warps per CTA at 48-56 registers spill too much)
 #ifndef DWBA_NODESET_MIN_BLOCKS
 #define DWBA_NODESET_MIN_BLOCKS 24
 #endif
+#ifndef DWBA_NODESET_FOLD_MIN_BLOCKS
+#define DWBA_NODESET_FOLD_MIN_BLOCKS 32
+#endif
+#ifndef DWBA_NODESET_FC
+#define DWBA_NODESET_FC 2  // factors per chunk of the fold loads (2: 2.47 ms, 4: 2.49 ms, 8 spills: 3.32 ms)
+#endif
+#ifndef DWBA_NODESET_WARPS
+#define DWBA_NODESET_WARPS 1  // warps per CTA, each on its own row blocks of the CTA's set
+#endif
+constexpr int NS_WARPS = DWBA_NODESET_WARPS;
 // FOLD = true: the operators are not stored; each row applies them at once to the two multi-folds
 // of its set (folds[2 set] with the tridiagonal T, folds[2 set + 1] with the band B), with the
 // arithmetic of fold_multi_kernel, and writes the folded operands instead.
@@ -94,7 +108,7 @@ __device__ __forceinline__ void fold_row_from_taps(const dwba_fold_multi_t& m, i
   // factors in chunks of FC: every tap load of a chunk is issued before its products, so the loads
   // are in flight together instead of one factor's after the previous factor's store (the stores
   // could alias the next factor's array for all the compiler knows)
-  constexpr int FC = 4;
+  constexpr int FC = DWBA_NODESET_FC;
   for (int t0 = 0; t0 < n_f; t0 += FC) {
     double fv[FC][2 * H + 1];
 #pragma unroll
@@ -118,7 +132,8 @@ __device__ __forceinline__ void fold_row_from_taps(const dwba_fold_multi_t& m, i
 }
 
 template <int NCC, bool FOLD>  // NCC: CC nodes per interval known at compile time (0: n_cc at run time)
-__global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets,
+__global__ void __launch_bounds__(32 * NS_WARPS, FOLD ? DWBA_NODESET_FOLD_MIN_BLOCKS : DWBA_NODESET_MIN_BLOCKS)
+    nodeset_rows_kernel(const dwba_nodeset_t* __restrict__ sets,
                                                               const double* __restrict__ ccx_g,
                                                               const double* __restrict__ ccw_g, int n_cc_rt,
                                                               int* status,
@@ -152,13 +167,13 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
   s.step = rn_sub(s.stop, s.start) / (double)s.n_int;
   const int N = s.n_grid, n1 = s.n1;
   const double* __restrict__ r = s.r;
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const double r_first = r[0], r_lim = r[n1 - 1], r_last = r[N - 1];
   // with n1 == N and one spacing test for both, the B taps of a node are its T taps
   const bool shared = s.log1 == s.log2 && n1 == N;
   const bool any_log = s.log1 || s.log2;
 
-  for (int k0 = blockIdx.x * OWN_ROWS; k0 < N; k0 += gridDim.x * OWN_ROWS) {
+  for (int k0 = (blockIdx.x * NS_WARPS + warp) * OWN_ROWS; k0 < N; k0 += gridDim.x * NS_WARPS * OWN_ROWS) {
     const int g = k0 - 2 + lane;
     // sums for row g (o_*), row g+1 (x_*) and row g+2 (n_*)
     double o_di = 0.0, o_up = 0.0, o_b2 = 0.0, o_b3 = 0.0, o_b4 = 0.0;
@@ -377,6 +392,15 @@ __global__ void __launch_bounds__(32, DWBA_NODESET_MIN_BLOCKS) nodeset_rows_kern
   }
 }
 
+// row groups per set: enough warps in total to fill the GPU several times over, never more than
+// the largest set needs (each warp strides over its set's row blocks)
+dim3 nodeset_grid(int max_grid, int n_sets) {
+  const int need = (max_grid + OWN_ROWS * NS_WARPS - 1) / (OWN_ROWS * NS_WARPS);
+  const int fill = (int)(((int64_t)148 * 24 * DWBA_NODESET_FILL + (int64_t)n_sets * NS_WARPS - 1) /
+                         ((int64_t)n_sets * NS_WARPS));
+  return dim3(need < fill ? need : fill, n_sets);
+}
+
 }  // namespace
 
 extern "C" int dwba_build_nodesets(const dwba_nodeset_t* sets_dev, int n_sets, int max_grid, const double* cc_x_dev,
@@ -385,16 +409,12 @@ extern "C" int dwba_build_nodesets(const dwba_nodeset_t* sets_dev, int n_sets, i
   if (!sets_dev || !cc_x_dev || !cc_w_dev || !status_dev || n_cc < 2 || n_cc > MAX_CC || max_grid < 2 ||
       n_sets > 65535)
     return DWBA_ERR_INVALID_ARG;
-  // row groups per set: enough one-warp CTAs in total to fill the GPU several times over, never
-  // more than the largest set needs (the kernel strides over its set's rows)
-  const int need = (max_grid + OWN_ROWS - 1) / OWN_ROWS;
-  const int fill = (int)(((int64_t)148 * 24 * DWBA_NODESET_FILL + n_sets - 1) / n_sets);
-  dim3 grid(need < fill ? need : fill, n_sets);
+  const dim3 grid = nodeset_grid(max_grid, n_sets);
   if (n_cc == 5)
-    nodeset_rows_kernel<5, false><<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc,
+    nodeset_rows_kernel<5, false><<<grid, 32 * NS_WARPS, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc,
                                                                          status_dev, nullptr);
   else
-    nodeset_rows_kernel<0, false><<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc,
+    nodeset_rows_kernel<0, false><<<grid, 32 * NS_WARPS, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc,
                                                                          status_dev, nullptr);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;
@@ -407,14 +427,12 @@ extern "C" int dwba_build_nodesets_folded(const dwba_nodeset_t* sets_dev, const 
   if (!sets_dev || !folds_dev || !cc_x_dev || !cc_w_dev || !status_dev || n_cc < 2 || n_cc > MAX_CC ||
       max_grid < 2 || n_sets > 65535)
     return DWBA_ERR_INVALID_ARG;
-  const int need = (max_grid + OWN_ROWS - 1) / OWN_ROWS;
-  const int fill = (int)(((int64_t)148 * 24 * DWBA_NODESET_FILL + n_sets - 1) / n_sets);
-  dim3 grid(need < fill ? need : fill, n_sets);
+  const dim3 grid = nodeset_grid(max_grid, n_sets);
   if (n_cc == 5)
-    nodeset_rows_kernel<5, true><<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc,
+    nodeset_rows_kernel<5, true><<<grid, 32 * NS_WARPS, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc,
                                                                         status_dev, folds_dev);
   else
-    nodeset_rows_kernel<0, true><<<grid, 32, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc,
+    nodeset_rows_kernel<0, true><<<grid, 32 * NS_WARPS, 0, (cudaStream_t)stream>>>(sets_dev, cc_x_dev, cc_w_dev, n_cc,
                                                                         status_dev, folds_dev);
   DWBA_CHECK_LAUNCH();
   return DWBA_OK;

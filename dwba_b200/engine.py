@@ -10,7 +10,6 @@ launch; the L=0 corrections and the outer tails are added in FP64 on the host.
 """
 from __future__ import annotations
 
-import contextlib
 import ctypes
 from dataclasses import dataclass, field
 import functools
@@ -515,8 +514,7 @@ class WaveMatrix:
         rows yet (a packed batch's waves, with their data addresses), in order; returns the row of
         the first."""
         first = len(self.arrays)
-        for i, a in enumerate(arrays):
-            self._by_id[id(a)] = first + i
+        self._by_id.update(zip(map(id, arrays), range(first, first + len(arrays))))
         self.arrays.extend(arrays)
         self._keep.extend(arrays)
         if ptrs is not None:
@@ -593,9 +591,8 @@ class WaveMatrix:
                 grp[1].extend(idx.tolist())
                 grp[2].extend((off[ok] // rb).tolist())
                 grouped[idx] = True
-        for i, a in enumerate(self.arrays):
-            if grouped[i]:
-                continue
+        for i in np.nonzero(~grouped)[0].tolist():
+            a = self.arrays[i]
             rb = self._row_of(a, N, a.__array_interface__["data"][0], base_ptrs)
             if rb is not None:
                 groups.setdefault(id(rb[0]), [rb[0], [], []])
@@ -611,18 +608,30 @@ class WaveMatrix:
                 continue  # a small share of its span: per-row copies below
             big.append((base[lo:hi], idx, r_arr - lo))
             done[idx] = True
-        # every small (synchronous) copy first -- the rows outside the grouped matrices and the
-        # index arrays of the gathers -- so that none of them waits behind a large asynchronous
-        # copy in the stream; the grouped blocks (asynchronous from pinned memory) last
-        self._copy_rows(out, done, N, n)
         side = bool(side_stream and big and out.is_cuda)
         if side:
+            # the grouped blocks go first, on the copy stream, so that the transfer starts at once;
+            # the index arrays of the gathers and the remaining rows follow as asynchronous copies
+            # through pinned staging (the rows on the current stream), none of them blocking the host
             cs = _copy_stream(out.device)
             cs.wait_stream(torch.cuda.current_stream(out.device))  # out belongs to the current stream
-            ctx = torch.cuda.stream(cs)
+            with torch.cuda.stream(cs):
+                blocks = []
+                for block, _, _ in big:
+                    src = torch.from_numpy(block)
+                    blocks.append(src.to(device, non_blocking=src.is_pinned()))
+                for (_, idx, rows), dev_block in zip(big, blocks):
+                    sel, dst = _dev(rows, device), _dev(np.asarray(idx, dtype=np.int64), device)
+                    out.index_copy_(0, dst, dev_block.index_select(0, sel)[:, :N])
+            self._copy_rows(out, done, N, n, stage=True)
+            out.record_stream(cs)
+            self.ready = torch.cuda.Event()
+            self.ready.record(cs)
         else:
-            ctx = contextlib.nullcontext()
-        with ctx:
+            # every small (synchronous) copy first -- the rows outside the grouped matrices and the
+            # index arrays of the gathers -- so that none of them waits behind a large asynchronous
+            # copy in the stream; the grouped blocks (asynchronous from pinned memory) last
+            self._copy_rows(out, done, N, n)
             gathers = [(torch.as_tensor(rows, device=device),
                         torch.as_tensor(np.asarray(idx, dtype=np.int64), device=device), block)
                        for block, idx, rows in big]
@@ -630,21 +639,16 @@ class WaveMatrix:
                 src = torch.from_numpy(block)
                 dev_block = src.to(device, non_blocking=src.is_pinned())
                 out.index_copy_(0, dst, dev_block.index_select(0, sel)[:, :N])
-        if side:
-            out.record_stream(cs)
-            self.ready = torch.cuda.Event()
-            self.ready.record(cs)
         self._uploaded[str(device)] = (n, out)
         return out
 
-    def _copy_rows(self, out: torch.Tensor, done: np.ndarray, N: int, n: int) -> None:
+    def _copy_rows(self, out: torch.Tensor, done: np.ndarray, N: int, n: int, stage: bool = False) -> None:
         """Rows not taken from a grouped matrix: consecutive ones in memory as one block, the others
-        one by one."""
-        i = 0
-        while i < n:
-            if done[i]:
-                i += 1
-                continue
+        one by one (``stage``: pageable rows through pinned staging memory, asynchronously)."""
+        todo = np.nonzero(~done[:n])[0].tolist()
+        k = 0
+        while k < len(todo):
+            i = todo[k]
             a = self.arrays[i]
             p0 = a.__array_interface__["data"][0]
             j = i + 1
@@ -661,8 +665,10 @@ class WaveMatrix:
             else:
                 j = i + 1
                 src = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).reshape(1, N)
+            if stage and out.is_cuda and not src.is_pinned():
+                src = src.pin_memory()
             out[i:j].copy_(src, non_blocking=src.is_pinned())
-            i = j
+            k += j - i  # rows i..j-1 are consecutive entries of todo
 
 
 @dataclass

@@ -11,7 +11,9 @@
  *       (scalars: bytes of P x 12 doubles (k, l, idx_match, eta, phase_shift, sigma_l of cont_i,
  *                 then of cont_f),
  *        rows_i, rows_f: bytes of P int64 (row of each pair's chi in the batch's function matrix:
- *                 distinct chi objects numbered in order of first appearance, all cont_i first),
+ *                 distinct chi objects numbered in order of first appearance, pair by pair, cont_i
+ *                 before cont_f -- the order of a matrix whose rows hold the pairs' two waves in
+ *                 turn, which then goes to the device as one copy without a gather),
  *        arrays: list of the distinct chi objects in row order,
  *        ptrs: list of the data addresses of the distinct arrays, in row order)
  *   or None when some wave does not qualify (its chi_of_r not exactly an ndarray of N float64
@@ -131,9 +133,8 @@ static PyObject* pack_pairs(PyObject* self, PyObject* args) {
     int64_t* RI = (int64_t*)PyBytes_AS_STRING(ri);
     int64_t* RF = (int64_t*)PyBytes_AS_STRING(rf);
     PyObject** items = PySequence_Fast_ITEMS(seq);
-    /* pass 1: cont_i of every pair (their chi arrays take the first rows); pass 2: cont_f */
-    for (int side = 0; side < 2; ++side) {
-      for (Py_ssize_t p = 0; p < P; ++p) {
+    for (Py_ssize_t p = 0; p < P; ++p) {
+      for (int side = 0; side < 2; ++side) {
         PyObject* pr = items[p];
         PyObject* w = NULL;
         if (PyTuple_Check(pr) && PyTuple_GET_SIZE(pr) == 2) {

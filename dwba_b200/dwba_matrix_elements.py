@@ -163,7 +163,7 @@ class _WaveView:
 
 class _Packed:
     """A batch's waves packed in one pass by the host extension: scalars (P x 12), the rows of each
-    pair's two chi arrays among the distinct ones (``arrays``, cont_i first) and, once they are in a
+    pair's two chi arrays among the distinct ones (``arrays``, pair by pair) and, once they are in a
     WaveMatrix (``owner``), the row of the first (``first``)."""
     __slots__ = ("scalars", "rows_i", "rows_f", "arrays", "ptrs", "first", "owner")
 

@@ -477,6 +477,19 @@ def _dphis(job: Job, n1: np.ndarray, k_total: np.ndarray, eta_total: np.ndarray)
     return d
 
 
+def _in_order(idx, rows, N: int, block: np.ndarray) -> Optional[int]:
+    """First row of ``out`` when the rows ``idx`` of a gather are consecutive and take the block's
+    rows 0, 1, ... in order with exactly N columns (the block then copies straight into them)."""
+    n = len(idx)
+    if block.shape[0] != n or block.shape[1] != N:
+        return None
+    i = np.asarray(idx, dtype=np.int64)
+    r = np.asarray(rows, dtype=np.int64)
+    if r[0] != 0 or not (np.all(np.diff(r) == 1) and np.all(np.diff(i) == 1)):
+        return None
+    return int(i[0])
+
+
 _COPY_STREAMS: Dict[int, "torch.cuda.Stream"] = {}
 
 
@@ -617,12 +630,18 @@ class WaveMatrix:
             cs.wait_stream(torch.cuda.current_stream(out.device))  # out belongs to the current stream
             with torch.cuda.stream(cs):
                 blocks = []
-                for block, _, _ in big:
+                for block, idx, rows in big:
                     src = torch.from_numpy(block)
-                    blocks.append(src.to(device, non_blocking=src.is_pinned()))
+                    o = _in_order(idx, rows, N, block)
+                    if o is not None:  # the block's rows are these rows of out, in order: no gather
+                        out[o:o + len(idx)].copy_(src, non_blocking=src.is_pinned())
+                        blocks.append(None)
+                    else:
+                        blocks.append(src.to(device, non_blocking=src.is_pinned()))
                 for (_, idx, rows), dev_block in zip(big, blocks):
-                    sel, dst = _dev(rows, device), _dev(np.asarray(idx, dtype=np.int64), device)
-                    out.index_copy_(0, dst, dev_block.index_select(0, sel)[:, :N])
+                    if dev_block is not None:
+                        sel, dst = _dev(rows, device), _dev(np.asarray(idx, dtype=np.int64), device)
+                        out.index_copy_(0, dst, dev_block.index_select(0, sel)[:, :N])
             self._copy_rows(out, done, N, n, stage=True)
             out.record_stream(cs)
             self.ready = torch.cuda.Event()
@@ -632,9 +651,14 @@ class WaveMatrix:
             # index arrays of the gathers -- so that none of them waits behind a large asynchronous
             # copy in the stream; the grouped blocks (asynchronous from pinned memory) last
             self._copy_rows(out, done, N, n)
+            direct = [_in_order(idx, rows, N, block) for block, idx, rows in big]
             gathers = [(torch.as_tensor(rows, device=device),
                         torch.as_tensor(np.asarray(idx, dtype=np.int64), device=device), block)
-                       for block, idx, rows in big]
+                       for (block, idx, rows), o in zip(big, direct) if o is None]
+            for (block, idx, _), o in zip(big, direct):
+                if o is not None:
+                    src = torch.from_numpy(block)
+                    out[o:o + len(idx)].copy_(src, non_blocking=src.is_pinned())
             for sel, dst, block in gathers:
                 src = torch.from_numpy(block)
                 dev_block = src.to(device, non_blocking=src.is_pinned())

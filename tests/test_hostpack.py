@@ -25,8 +25,10 @@ def test_packed_scalars_and_rows_match_the_python_path():
     for j, k in enumerate(("k_i", "l_i", "im_i", "e_i", "d_i", "s_i", "k_f", "l_f", "im_f", "e_f", "d_f", "s_f")):
         assert np.array_equal(pk.scalars[:, j], pa[k].astype(np.float64)), k
     w = WaveMatrix(501)
-    rows_i = [w.add(ci.chi_of_r) for ci, _ in pairs]
-    rows_f = [w.add(cf.chi_of_r) for _, cf in pairs]
+    rows_i, rows_f = [], []
+    for ci, cf in pairs:  # numbered pair by pair, cont_i before cont_f
+        rows_i.append(w.add(ci.chi_of_r))
+        rows_f.append(w.add(cf.chi_of_r))
     assert list(pk.rows_i) == rows_i and list(pk.rows_f) == rows_f
     assert len(pk.arrays) == len(w.arrays) and all(a is b for a, b in zip(pk.arrays, w.arrays))
     assert list(pk.ptrs) == [a.__array_interface__["data"][0] for a in pk.arrays]

@@ -99,6 +99,7 @@ def _declare(lib):
         "dwba_cupy_exchange_forms": (c_int, [c_vp, c_int, c_int, c_dbl, c_dbl, c_vp]),
         "dwba_tc_ragged_workspace_bytes": (c_i64, [c_vp, c_int, c_int, c_int, c_vp]),
         "dwba_bilinear_tc_bf16_ragged": (c_int, [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp]),
+        "dwba_copy_from_host": (c_int, [c_vp, c_vp, c_i64, c_vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

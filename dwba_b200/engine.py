@@ -99,14 +99,66 @@ def _stream() -> int:
     return int(torch.cuda.current_stream().cuda_stream)
 
 
+class _Staging:
+    """A ring of page-locked host memory per device for the small arrays a call uploads
+    (descriptors): an array is copied into the ring and from there to the device by a kernel on the
+    current stream (``dwba_copy_from_host``), so that it neither blocks the host nor queues behind a
+    large transfer on the copy engines. A region of the ring is reused only after the event recorded
+    behind its copy has completed."""
+
+    SIZE = 32 << 20
+    MAX = 4 << 20  # larger arrays go through torch's pinned memory and the copy engines
+    _by_device: Dict[int, "_Staging"] = {}
+
+    def __init__(self):
+        self.buf = torch.empty(self.SIZE, dtype=torch.uint8, pin_memory=True)
+        self.host = self.buf.numpy()
+        self.ptr = self.buf.data_ptr()
+        self.head = 0
+        self.pending: List[Tuple[int, int, torch.cuda.Event]] = []
+
+    @classmethod
+    def get(cls, index: int) -> "_Staging":
+        st = cls._by_device.get(index)
+        if st is None:
+            st = cls._by_device[index] = cls()
+        return st
+
+    def copy(self, x: np.ndarray, out: torch.Tensor) -> None:
+        raw = x.reshape(-1).view(np.uint8)
+        n = len(raw)
+        need = (n + 255) // 256 * 256
+        if self.head + need > self.SIZE:
+            self.head = 0
+        a, b = self.head, self.head + need
+        keep = []
+        for s0, s1, ev in self.pending:
+            if s0 < b and a < s1:
+                ev.synchronize()  # an earlier copy from this region must have run
+            else:
+                keep.append((s0, s1, ev))
+        self.host[a:a + n] = raw
+        _lib.check(_lib.load().dwba_copy_from_host(out.data_ptr(), self.ptr + a, n, _stream()), "dwba_copy_from_host")
+        ev = torch.cuda.Event()
+        ev.record()
+        keep.append((a, b, ev))
+        self.pending = keep
+        self.head = b
+
+
 def _dev(x: np.ndarray, device) -> torch.Tensor:
-    """A host array on the device. To a GPU it goes through pinned staging memory as an
-    asynchronous copy on the current stream, so that the host does not wait while a large transfer
-    occupies the copy engine (the staging block is held by torch's pinned allocator until the copy
-    has run; later changes to ``x`` do not reach the copy)."""
-    t = torch.from_numpy(np.ascontiguousarray(x))
-    if torch.device(device).type != "cuda":
+    """A host array on the device. To a GPU, a small array goes through the staging ring (copied by
+    a kernel, _Staging) and a large one through pinned memory as an asynchronous copy on the current
+    stream: neither blocks the host, and later changes to ``x`` do not reach the copy."""
+    x = np.ascontiguousarray(x)
+    t = torch.from_numpy(x)
+    dev = torch.device(device)
+    if dev.type != "cuda":
         return t.to(device)
+    if 0 < x.nbytes <= _Staging.MAX:
+        out = torch.empty_like(t, device=dev)
+        _Staging.get(out.device.index).copy(x, out)
+        return out
     return t.pin_memory().to(device, non_blocking=True)
 
 
@@ -182,6 +234,7 @@ class NodeSetBatch:
         self.n_fused = len(self.fused_idx)
         self.fused_recs = None
         self.fused_folds_d = None
+        self.fused_groups = [(0, 0, self.n_fused)]
         if self.n_fused:
             fp = list(map(plans.__getitem__, self.fused_idx.tolist()))
             f_key, f_nb, f_br, f_l1, f_l2 = zip(*fp)  # fields of every fused set, without a Python loop
@@ -268,6 +321,16 @@ class NodeSetBatch:
         self.recs_d = _dev(recs.view(np.uint8), dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
 
+    def reorder_fused(self, perm: np.ndarray, groups: List[Tuple[int, int, int]]) -> None:
+        """Put the fused sets in the order ``perm`` (of their current order) and launch them in
+        ``groups`` (part k of a chunked wave upload, first set, end set): each group after its part
+        of the waves is on the device. Call before ``set_fused_folds``, whose folds follow the new order."""
+        perm = np.asarray(perm, dtype=np.int64)
+        self.fused_idx = self.fused_idx[perm]
+        self.fused_recs = _take(self.fused_recs, perm)
+        self.fused_recs_d = _dev(self.fused_recs.view(np.uint8), self.dg.device)
+        self.fused_groups = list(groups)
+
     def set_fused_folds(self, folds: np.ndarray) -> None:
         """The two multi-folds (T, then B) of every fused set, in the order of ``fused_idx``."""
         assert len(folds) == 2 * self.n_fused
@@ -286,7 +349,9 @@ class NodeSetBatch:
             b += self.n_fused * 8.0 * 2.0 * N + fused_fold_bytes(self.fused_folds)
         return b
 
-    def launch(self) -> None:
+    def launch(self, waves: Optional["WaveMatrix"] = None) -> None:
+        """Stored sets first (they read only the grid), then the fused sets, which read their pair's
+        waves: with ``waves``, each group of ``fused_groups`` after its part of the wave upload."""
         lib = _lib.load()
         N = self.dg.info.N
         for s0 in range(0, self.n, 65535):
@@ -294,13 +359,16 @@ class NodeSetBatch:
             _lib.check(lib.dwba_build_nodesets(_ptr(self.recs_d) + s0 * _lib.NODESET_DTYPE.itemsize, n, N,
                                                _ptr(self.ccx), _ptr(self.ccw), self.n_cc, _ptr(self.status),
                                                _stream()), "dwba_build_nodesets")
-        for s0 in range(0, self.n_fused, 65535):
-            n = min(65535, self.n_fused - s0)
-            _lib.check(lib.dwba_build_nodesets_folded(_ptr(self.fused_recs_d) + s0 * _lib.NODESET_DTYPE.itemsize,
-                                                      _ptr(self.fused_folds_d) + 2 * s0 * _lib.FOLD_MULTI_DTYPE.itemsize,
-                                                      n, N, _ptr(self.fccx), _ptr(self.fccw), self.n_cc,
-                                                      _ptr(self.fused_status), _stream()),
-                       "dwba_build_nodesets_folded")
+        pending = waves is not None and waves.chunks is not None
+        for k, g0, g1 in (self.fused_groups if pending else [(-1, 0, self.n_fused)]):
+            if pending:
+                waves.wait_chunk(k)
+            for s0 in range(g0, g1, 65535):
+                n = min(65535, g1 - s0)
+                _lib.check(lib.dwba_build_nodesets_folded(
+                    _ptr(self.fused_recs_d) + s0 * _lib.NODESET_DTYPE.itemsize,
+                    _ptr(self.fused_folds_d) + 2 * s0 * _lib.FOLD_MULTI_DTYPE.itemsize, n, N, _ptr(self.fccx),
+                    _ptr(self.fccw), self.n_cc, _ptr(self.fused_status), _stream()), "dwba_build_nodesets_folded")
 
     def check(self) -> None:
         if self.n and int(self.status.item()) != 0:
@@ -477,6 +545,9 @@ def _dphis(job: Job, n1: np.ndarray, k_total: np.ndarray, eta_total: np.ndarray)
     return d
 
 
+WAVE_CHUNKS = 4  # parts of a side-stream wave upload that kernels can wait for one by one
+
+
 def _in_order(idx, rows, N: int, block: np.ndarray) -> Optional[int]:
     """First row of ``out`` when the rows ``idx`` of a gather are consecutive and take the block's
     rows 0, 1, ... in order with exactly N columns (the block then copies straight into them)."""
@@ -514,6 +585,9 @@ class WaveMatrix:
         self._keep: List[object] = []
         self._ptrs: Dict[int, Tuple[int, np.ndarray]] = {}  # first row -> (count, data addresses)
         self.ready: Optional[torch.cuda.Event] = None  # end of a side-stream upload not yet waited for
+        # side-stream upload of a block copied in row order: (first row, end row, event after it) of
+        # each of its WAVE_CHUNKS parts, so that kernels reading only early rows can start sooner
+        self.chunks: Optional[List[Tuple[int, int, torch.cuda.Event]]] = None
 
     def wait_ready(self) -> None:
         """Order the current stream after a side-stream upload (``upload(..., side_stream=True)``);
@@ -521,6 +595,26 @@ class WaveMatrix:
         if self.ready is not None:
             torch.cuda.current_stream().wait_event(self.ready)
             self.ready = None
+        self.chunks = None
+
+    def chunk_of(self, rows: np.ndarray) -> np.ndarray:
+        """For each row of the device matrix, the part of a chunked upload after which it is on the
+        device (len(chunks) when the whole upload must be waited for, 0 when nothing is pending)."""
+        rows = np.asarray(rows, dtype=np.int64)
+        if self.chunks is None:
+            return np.zeros(len(rows), dtype=np.int64)
+        out = np.full(len(rows), len(self.chunks), dtype=np.int64)
+        for k, (lo, hi, _) in enumerate(self.chunks):
+            out[(rows >= lo) & (rows < hi)] = k
+        return out
+
+    def wait_chunk(self, k: int) -> None:
+        """Order the current stream after part k of a chunked upload (after all of it for k beyond
+        the parts)."""
+        if self.chunks is None or k >= len(self.chunks):
+            self.wait_ready()
+        else:
+            torch.cuda.current_stream().wait_event(self.chunks[k][2])
 
     def add_distinct(self, arrays: Sequence[np.ndarray], ptrs: Optional[np.ndarray] = None) -> int:
         """Append arrays known to be distinct C-contiguous objects of N float64 values that are not
@@ -628,12 +722,25 @@ class WaveMatrix:
             # through pinned staging (the rows on the current stream), none of them blocking the host
             cs = _copy_stream(out.device)
             cs.wait_stream(torch.cuda.current_stream(out.device))  # out belongs to the current stream
+            chunks = []
             with torch.cuda.stream(cs):
                 blocks = []
                 for block, idx, rows in big:
                     src = torch.from_numpy(block)
                     o = _in_order(idx, rows, N, block)
-                    if o is not None:  # the block's rows are these rows of out, in order: no gather
+                    if o is not None and src.is_pinned() and not chunks:
+                        # the block's rows are these rows of out, in order: no gather; copied in
+                        # parts with an event after each
+                        nb = len(idx)
+                        cuts = [nb * k // WAVE_CHUNKS for k in range(WAVE_CHUNKS + 1)]
+                        for a, b in zip(cuts[:-1], cuts[1:]):
+                            if b > a:
+                                out[o + a:o + b].copy_(src[a:b], non_blocking=True)
+                                ev = torch.cuda.Event()
+                                ev.record(cs)
+                                chunks.append((o + a, o + b, ev))
+                        blocks.append(None)
+                    elif o is not None:  # the block's rows are these rows of out, in order: no gather
                         out[o:o + len(idx)].copy_(src, non_blocking=src.is_pinned())
                         blocks.append(None)
                     else:
@@ -646,6 +753,7 @@ class WaveMatrix:
             out.record_stream(cs)
             self.ready = torch.cuda.Event()
             self.ready.record(cs)
+            self.chunks = chunks or None
         else:
             # every small (synchronous) copy first -- the rows outside the grouped matrices and the
             # index arrays of the gathers -- so that none of them waits behind a large asynchronous
@@ -685,13 +793,18 @@ class WaveMatrix:
                 j += 1
             if ok and j - i > 1 and a.base is not None:
                 block = np.lib.stride_tricks.as_strided(a, shape=(j - i, N), strides=(8 * N, 8))
-                src = torch.from_numpy(block)
             else:
                 j = i + 1
-                src = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).reshape(1, N)
-            if stage and out.is_cuda and not src.is_pinned():
-                src = src.pin_memory()
-            out[i:j].copy_(src, non_blocking=src.is_pinned())
+                block = np.ascontiguousarray(a, dtype=np.float64).reshape(1, N)
+            src = torch.from_numpy(block)
+            if stage and out.is_cuda and block.nbytes <= _Staging.MAX and not src.is_pinned():
+                # small rows by the staging ring's kernel copy: a copy-engine transfer would wait
+                # behind the large one on the side stream, and every later launch on this stream with it
+                _Staging.get(out.device.index).copy(np.ascontiguousarray(block), out[i:j])
+            else:
+                if stage and out.is_cuda and not src.is_pinned():
+                    src = src.pin_memory()
+                out[i:j].copy_(src, non_blocking=src.is_pinned())
             k += j - i  # rows i..j-1 are consecutive entries of todo
 
 
@@ -1241,6 +1354,17 @@ class PreparedJob:
                 if int(np.count_nonzero(fg)) != ns.n_fused or len(np.unique(q[fg])) != ns.n_fused:
                     raise RuntimeError("fused node sets must serve exactly one multi-fold group each")
                 sel = np.nonzero(fg)[0][np.argsort(q[fg], kind="stable")]  # groups in node-set order
+                if waves.chunks is not None:
+                    # sets whose pair's waves arrive in an earlier part of the upload go first, in
+                    # groups that each wait only for their part
+                    pp = pf[sel]
+                    ch = waves.chunk_of(np.maximum(wi_idx[pp], wf_idx[pp]))
+                    perm = np.argsort(ch, kind="stable")
+                    cs = ch[perm]
+                    starts = np.concatenate([[0], np.nonzero(np.diff(cs))[0] + 1])
+                    ends = np.concatenate([starts[1:], [len(cs)]])
+                    ns.reorder_fused(perm, [(int(cs[a]), int(a), int(b)) for a, b in zip(starts, ends)])
+                    sel = sel[perm]
                 ns.set_fused_folds(_interleave(_take(mT, sel), _take(mB, sel)))
                 multi = _take(multi, np.nonzero(np.repeat(~fg, 2))[0])
         elif self.nodesets.n_fused:
@@ -1387,8 +1511,8 @@ class PreparedJob:
             self.form_launch.launch(lib, job.L_max, self.ds, float(job.grid.r[0]), float(job.grid.r[-1]))
 
     def launch(self) -> None:
+        self.nodesets.launch(self.waves)  # stored sets at once, fused sets as their waves arrive
         self.waves.wait_ready()
-        self.nodesets.launch()
         self.launch_folds()
         self.launch_forms()
         self.launch_tails()

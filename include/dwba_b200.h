@@ -419,6 +419,16 @@ int dwba_outer_tails_batch(const dwba_tail_t* tails_dev, int n, int L_max, int m
                            double max_effective_dphi, dwba_stream_t stream);
 int dwba_outer_tail_on_device(const double* wave_host, double r_m, double r_max);
 
+/* Copy nbytes from page-locked host memory (allocated with cudaHostAlloc / cudaMallocHost, so that
+ * the device can address it) into device memory with a kernel on `stream` instead of the copy
+ * engines. No counterpart in the reference (its descriptors are CuPy arrays); the engine uses it for
+ * the small descriptor arrays a call builds while the call's large wave transfer occupies the copy
+ * engines, which would otherwise queue them behind it. Returns DWBA_ERR_INVALID_ARG when the
+ * source is not mapped page-locked host memory or the destination not device memory (checked at
+ * both ends of each range; like every entry point here, the extents are the caller's to get right).
+ * The host memory must stay unchanged until the copy has run on the stream. */
+int dwba_copy_from_host(void* dst_dev, const void* src_host, int64_t nbytes, dwba_stream_t stream);
+
 /* Library identity and device probe (the check_cupy_runtime analogue, dwba_matrix_elements.py:178-193). */
 int dwba_abi_version(void);
 const char* dwba_status_string(int status);

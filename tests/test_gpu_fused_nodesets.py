@@ -61,3 +61,35 @@ def test_fused_node_sets_match_stored_operators(kind):
     d2, e2 = un.collect()
     assert np.array_equal(d1, d2) and np.array_equal(e1, e2)
     assert np.isfinite(d1).all() and np.abs(e1).max() > 0
+
+
+def test_chunked_wave_upload_gives_the_same_integrals():
+    """A batch whose waves are rows of one pinned host matrix goes to the device in parts on a copy
+    stream, and the fused node sets of each part start as soon as it has arrived (their launch
+    order changes). The integrals must be bit-identical to those of the same waves from pageable
+    memory (one synchronous upload, sets in their planned order) and repeatable."""
+    from dwba_b200.dwba_matrix_elements import GPUCache, radial_ME_all_L_batch
+    from dwba_b200 import engine
+    g, z, bounds, pairs_pinned = bench.make_workload(N=3001, n_cont=96, n_bound=3, seed_shift=31, pinned=True)
+    _, _, _, pairs_plain = bench.make_workload(N=3001, n_cont=96, n_bound=3, seed_shift=31, pinned=False)
+    b_i, b_f = [b[0] for b in bounds], [b[1] for b in bounds]
+    cache = GPUCache.from_grid(g)
+    seen = []
+    orig = engine.NodeSetBatch.reorder_fused
+
+    def spy(self, perm, groups):
+        seen.append(len(groups))
+        return orig(self, perm, groups)
+    engine.NodeSetBatch.reorder_fused = spy
+    try:
+        res = []
+        for pairs in (pairs_pinned, pairs_plain, pairs_pinned):
+            cache.clear()
+            res.append(radial_ME_all_L_batch(g, z, z, b_i, b_f, pairs, 6, U_f_array=z, gpu_cache=cache,
+                                             engine="semisep", as_arrays=True))
+    finally:
+        engine.NodeSetBatch.reorder_fused = orig
+    assert seen and max(seen) > 1, "the pinned batch was not uploaded in parts"
+    for d, e in res[1:]:
+        assert np.array_equal(d, res[0][0]) and np.array_equal(e, res[0][1])
+    assert np.isfinite(res[0][0]).all() and np.abs(res[0][1]).max() > 0

@@ -10,6 +10,7 @@ launch; the L=0 corrections and the outer tails are added in FP64 on the host.
 """
 from __future__ import annotations
 
+import collections
 import ctypes
 from dataclasses import dataclass, field
 import functools
@@ -99,6 +100,33 @@ def _stream() -> int:
     return int(torch.cuda.current_stream().cuda_stream)
 
 
+class RingRegions:
+    """Region allocator of a ring buffer whose regions are freed in allocation order: ``alloc(n)``
+    returns the next region [a, b) (256-byte aligned) and the keys of the earlier regions it
+    overlaps, or that a wrap leaves behind, which must be released (waited for) before [a, b) is
+    written. Live regions never overlap."""
+
+    def __init__(self, size: int):
+        self.size, self.head = size, 0
+        self.live: "collections.deque[Tuple[int, int, object]]" = collections.deque()
+
+    def alloc(self, n: int, key) -> Tuple[int, int, list]:
+        need = (n + 255) // 256 * 256
+        if need > self.size:
+            raise ValueError("region larger than the ring")
+        release = []
+        if self.head + need > self.size:
+            while self.live and self.live[0][0] >= self.head:  # past this pass's end
+                release.append(self.live.popleft()[2])
+            self.head = 0
+        a, b = self.head, self.head + need
+        while self.live and self.live[0][0] < b and a < self.live[0][1]:
+            release.append(self.live.popleft()[2])
+        self.live.append((a, b, key))
+        self.head = b
+        return a, b, release
+
+
 class _Staging:
     """A ring of page-locked host memory per device for the small arrays a call uploads
     (descriptors): an array is copied into the ring and from there to the device by a kernel on the
@@ -114,8 +142,7 @@ class _Staging:
         self.buf = torch.empty(self.SIZE, dtype=torch.uint8, pin_memory=True)
         self.host = self.buf.numpy()
         self.ptr = self.buf.data_ptr()
-        self.head = 0
-        self.pending: List[Tuple[int, int, torch.cuda.Event]] = []
+        self.regions = RingRegions(self.SIZE)
 
     @classmethod
     def get(cls, index: int) -> "_Staging":
@@ -127,23 +154,13 @@ class _Staging:
     def copy(self, x: np.ndarray, out: torch.Tensor) -> None:
         raw = x.reshape(-1).view(np.uint8)
         n = len(raw)
-        need = (n + 255) // 256 * 256
-        if self.head + need > self.SIZE:
-            self.head = 0
-        a, b = self.head, self.head + need
-        keep = []
-        for s0, s1, ev in self.pending:
-            if s0 < b and a < s1:
-                ev.synchronize()  # an earlier copy from this region must have run
-            else:
-                keep.append((s0, s1, ev))
+        ev = torch.cuda.Event()
+        a, _, release = self.regions.alloc(n, ev)
+        for old in release:
+            old.synchronize()  # the earlier copy from this region must have run
         self.host[a:a + n] = raw
         _lib.check(_lib.load().dwba_copy_from_host(out.data_ptr(), self.ptr + a, n, _stream()), "dwba_copy_from_host")
-        ev = torch.cuda.Event()
         ev.record()
-        keep.append((a, b, ev))
-        self.pending = keep
-        self.head = b
 
 
 def _dev(x: np.ndarray, device) -> torch.Tensor:

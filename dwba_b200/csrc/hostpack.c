@@ -306,12 +306,63 @@ static PyObject* fill_results(PyObject* self, PyObject* args) {
   Py_RETURN_NONE;
 }
 
+/* fill_half(dicts, values, nl, side): dicts[2 i + side] of make_results gets {L: values[i, L]} as
+ * Python floats for every i, from a C-contiguous float64 array of (len(dicts) / 2) x nl values (the
+ * direct integrals with side 0, the exchange ones with side 1). */
+static PyObject* fill_half(PyObject* self, PyObject* args) {
+  (void)self;
+  PyObject *dicts, *val_obj;
+  Py_ssize_t nl;
+  int side;
+  if (!PyArg_ParseTuple(args, "O!Oni", &PyList_Type, &dicts, &val_obj, &nl, &side)) return NULL;
+  const Py_ssize_t nd = PyList_GET_SIZE(dicts);
+  if (nl < 1 || nd % 2 != 0 || (side != 0 && side != 1)) {
+    PyErr_SetString(PyExc_ValueError, "fill_half: bad sizes or side");
+    return NULL;
+  }
+  Py_buffer vb;
+  if (get_values(val_obj, (nd / 2) * nl, &vb) != 0) return NULL;
+  PyObject* keys[64];
+  const Py_ssize_t nk = nl < 64 ? nl : 64;
+  int ok = 1;
+  for (Py_ssize_t l = 0; l < nk; ++l) {
+    keys[l] = PyLong_FromSsize_t(l);
+    ok &= keys[l] != NULL;
+  }
+  for (Py_ssize_t i = side; ok && i < nd; i += 2) {
+    PyObject* d = PyList_GET_ITEM(dicts, i);
+    if (!PyDict_Check(d)) {
+      PyErr_SetString(PyExc_TypeError, "fill_half: dicts must hold dicts");
+      ok = 0;
+      break;
+    }
+    const double* v = (const double*)vb.buf + (i / 2) * nl;
+    for (Py_ssize_t l = 0; l < nl; ++l) {
+      PyObject* key = l < nk ? keys[l] : PyLong_FromSsize_t(l);
+      PyObject* f = key ? PyFloat_FromDouble(v[l]) : NULL;
+      const int rc = f ? PyDict_SetItem(d, key, f) : -1;
+      Py_XDECREF(f);
+      if (l >= nk) Py_XDECREF(key);
+      if (rc != 0) {
+        ok = 0;
+        break;
+      }
+    }
+  }
+  for (Py_ssize_t l = 0; l < nk; ++l) Py_XDECREF(keys[l]);
+  PyBuffer_Release(&vb);
+  if (!ok) return NULL;
+  Py_RETURN_NONE;
+}
+
 static PyMethodDef methods[] = {
     {"pack_pairs", pack_pairs, METH_VARARGS,
      "pack_pairs(pairs, N, ndarray_type) -> (scalars, rows_i, rows_f, arrays, ptrs) or None"},
     {"make_results", make_results, METH_VARARGS,
      "make_results(cls, T, P, nl) -> (results: T lists of P instances of cls, dicts: their 2 T P field dicts)"},
     {"fill_results", fill_results, METH_VARARGS, "fill_results(dicts, I_dir, I_exc, nl): the values of the dicts"},
+    {"fill_half", fill_half, METH_VARARGS,
+     "fill_half(dicts, values, nl, side): the direct (side 0) or exchange (side 1) dicts' values"},
     {NULL, NULL, 0, NULL}};
 
 static struct PyModuleDef module = {PyModuleDef_HEAD_INIT, "_hostpack", NULL, -1, methods, NULL, NULL, NULL, NULL};

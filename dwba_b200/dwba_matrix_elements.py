@@ -38,6 +38,7 @@ except ImportError:  # pragma: no cover - only when the extension was not built
     _hostpack = None
 
 OscillatoryMethod = Literal["legacy", "advanced", "full_split"]
+EARLY_DIRECT_MIN_FORMS = 256  # (transition, pair) count from which results come back in two parts
 SEMANTICS = ("cpu", "cupy")
 
 try:
@@ -325,10 +326,19 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
                                       lambda p: p.launch())
             pj.launch()
         else:
-            pj = PreparedJob(job, cache.dg, eng, plans=plans)
+            # direct rows copied back first only where the fill of their dicts is worth overlapping
+            early = not as_arrays and len(job.transitions) * len(job.pairs) >= EARLY_DIRECT_MIN_FORMS
+            pj = PreparedJob(job, cache.dg, eng, plans=plans, early_direct=early)
             pj.launch()
         # the result objects are made while the kernels run; collect() then waits for them
         skel = None if as_arrays else _skeleton(len(job.transitions), len(job.pairs), job.L_max + 1)
+        if skel is not None and getattr(pj, "early_direct", None) is not None:
+            # the direct integrals arrive before the exchange forms have run: their values are
+            # filled in meanwhile
+            _hostpack.fill_half(skel[1], pj.collect_direct(), job.L_max + 1, 0)
+            I_dir, I_exc = pj.collect()
+            _hostpack.fill_half(skel[1], np.ascontiguousarray(I_exc), job.L_max + 1, 1)
+            return skel[0]
         I_dir, I_exc = pj.collect()
     if as_arrays:
         return I_dir, I_exc

@@ -1122,9 +1122,11 @@ class FormLaunch:
             self.out_ss = torch.empty((self.n_ss, nl), dtype=torch.float64, device=dev)
         self.pots_host, self.dots_host = pots, dots
 
-    def launch(self, lib, L_max: int, ds: np.ndarray, r_min: float, r_max: float, marks: Optional[list] = None) -> None:
-        """Enqueue the potentials, the dot forms and the semiseparable forms. With ``marks`` (a list),
-        a CUDA event is recorded after each of the three and appended as (name, event)."""
+    def launch(self, lib, L_max: int, ds: np.ndarray, r_min: float, r_max: float, marks: Optional[list] = None,
+               parts=("potentials", "dots", "semisep")) -> None:
+        """Enqueue the potentials, the dot forms and the semiseparable forms (those of ``parts``).
+        With ``marks`` (a list), a CUDA event is recorded after each of the three and appended as
+        (name, event)."""
         st = _stream()
 
         def mark(name):
@@ -1132,14 +1134,14 @@ class FormLaunch:
                 ev = torch.cuda.Event(enable_timing=True)
                 ev.record(torch.cuda.current_stream())
                 marks.append((name, ev))
-        if self.n_pots:
+        if self.n_pots and "potentials" in parts:
             _lib.check(lib.dwba_multipole_potentials(_ptr(self.pots_d), self.n_pots, L_max, ds.ctypes.data, r_min, r_max,
                                                      st), "dwba_multipole_potentials")
         mark("potentials")
-        if self.n_dots:
+        if self.n_dots and "dots" in parts:
             _lib.check(lib.dwba_dot_forms(_ptr(self.dots_d), self.n_dots, L_max, st), "dwba_dot_forms")
         mark("dots")
-        if self.n_ss:
+        if self.n_ss and "semisep" in parts:
             _lib.check(lib.dwba_bilinear_semisep_fp64(_ptr(self.ss_forms_d), self.n_ss, L_max, ds.ctypes.data, r_min,
                                                       r_max, _ptr(self.out_ss), st), "dwba_bilinear_semisep_fp64")
             self.out.index_copy_(0, self.ss_rows_d, self.out_ss)
@@ -1214,11 +1216,13 @@ class PreparedJob:
     ``launch()`` enqueues every kernel on the current stream: node-set operators (those not
     yet cached for the grid, or all of them with ``rebuild_nodesets``), operand folds and the
     bilinear forms. ``collect()`` copies the results back once and adds the host-side L=0
-    corrections and outer tails. Results are indexed [transition, pair, L].
+    corrections and outer tails. Results are indexed [transition, pair, L]. With ``early_direct``
+    (exact engine, every direct form through the potentials), the direct rows are copied back
+    before the exchange forms run, and ``collect_direct()`` returns them first.
     """
 
     def __init__(self, job: Job, dg: DeviceGrid, engine: str = "dense", plans=None,
-                 rebuild_nodesets: bool = False, fuse_folds: Optional[bool] = None):
+                 rebuild_nodesets: bool = False, fuse_folds: Optional[bool] = None, early_direct: bool = False):
         if engine not in ENGINES:
             raise ValueError(f"unknown engine {engine!r}; choose from {ENGINES}")
         if job.L_max < 0:
@@ -1416,9 +1420,18 @@ class PreparedJob:
         tc = engine in TC_TERMS
         ss_fo = d_rows[~via_pot] if tc else np.sort(np.concatenate([d_rows[~via_pot], d_rows + 1]))
         self.direct_plan = DirectPlan(pot_b=pot_b, dot_fo=d_rows[via_pot], dot_t=d_t[via_pot], ss_fo=ss_fo)
+        self.early_direct = None
         if engine == "semisep":
             dp = self.direct_plan
             self.form_launch = FormLaunch([(forms, dp, N, _ptr(dg.r), dp.dot_fo, dp.ss_fo)], self.out, nl, dev)
+            if early_direct and len(dp.ss_fo) and bool(np.all(dp.ss_fo % 2 == 1)):
+                # every direct form goes through the potentials and dot forms, so the direct rows are
+                # final before the semiseparable (exchange) forms run
+                self.early_direct = {
+                    "dev": torch.empty((T * P, nl), dtype=torch.float64, device=dev),
+                    "host": torch.empty((T * P, nl), dtype=torch.float64, pin_memory=True),
+                    "tails": torch.empty((max(1, self.n_tail), nl), dtype=torch.float64, pin_memory=True),
+                    "event": torch.cuda.Event(), "done": None}
         if engine in TC_TERMS:
             # direct forms: potentials and dot products, the rest exact O(N L); exchange forms: tensor cores
             self.forms_ex_d = _dev(np.ascontiguousarray(forms[1::2]).view(np.uint8), dev)
@@ -1463,14 +1476,20 @@ class PreparedJob:
 
     def add_host_terms(self, I_dir, I_exc, tail_rows) -> None:
         """Outer tails (host- and device-evaluated) and L=0 corrections, then the non-finite guard."""
+        self.add_direct_host_terms(I_dir, tail_rows)
+        self.add_exchange_host_terms(I_exc)
+
+    def add_direct_host_terms(self, I_dir, tail_rows) -> None:
         pl = self.plans
         for (ti, p_i), tail in pl.tails.items():
             I_dir[ti, p_i] += tail
         if self.n_tail:
             I_dir[pl.tail_tp[:, 0], pl.tail_tp[:, 1], 1:] += tail_rows[:, 1:]
         I_dir[:, :, 0] += pl.corr_dir
-        I_exc[:, :, 0] += pl.corr_ex
         I_dir[~np.isfinite(I_dir)] = 0.0
+
+    def add_exchange_host_terms(self, I_exc) -> None:
+        I_exc[:, :, 0] += self.plans.corr_ex
         I_exc[~np.isfinite(I_exc)] = 0.0
 
     def launch_folds(self) -> None:
@@ -1530,6 +1549,24 @@ class PreparedJob:
     def launch(self) -> None:
         self.nodesets.launch(self.waves)  # stored sets at once, fused sets as their waves arrive
         self.waves.wait_ready()
+        if self.early_direct is not None:
+            # direct forms and tails first; their rows go back to the host while the exchange
+            # forms run (collect_direct)
+            self.launch_folds()
+            job = self.job
+            self.form_launch.launch(self.lib, job.L_max, self.ds, float(job.grid.r[0]), float(job.grid.r[-1]),
+                                    parts=("potentials", "dots"))
+            self.launch_tails()
+            ed = self.early_direct
+            ed["dev"].copy_(self.out[0:self.n_forms:2])
+            ed["host"].copy_(ed["dev"], non_blocking=True)
+            if self.n_tail:
+                ed["tails"].copy_(self.out[self.n_forms:], non_blocking=True)
+            ed["event"].record()
+            ed["done"] = None
+            self.form_launch.launch(self.lib, job.L_max, self.ds, float(job.grid.r[0]), float(job.grid.r[-1]),
+                                    parts=("semisep",))
+            return
         self.launch_folds()
         self.launch_forms()
         self.launch_tails()
@@ -1576,9 +1613,30 @@ class PreparedJob:
         m = np.maximum(f["n_rows"], f["n_cols"]).astype(np.float64)
         return float(np.sum(8.0 * (f["n_rows"].astype(np.float64) + f["n_cols"] + m)))
 
+    def collect_direct(self) -> np.ndarray:
+        """I_dir as a (T, P, L_max+1) array as soon as the direct forms and tails have run (their
+        rows are copied back before the exchange forms), for a caller that handles them while the
+        device finishes; ``collect()`` then returns the same array. Only with ``early_direct``."""
+        ed = self.early_direct
+        if ed is None:
+            raise RuntimeError("collect_direct: this job evaluates its direct forms with the exchange forms")
+        if ed["done"] is None:
+            ed["event"].synchronize()
+            I_dir = ed["host"].numpy().reshape(self.T, self.P, self.nl).copy()
+            self.add_direct_host_terms(I_dir, ed["tails"].numpy() if self.n_tail else None)
+            ed["done"] = I_dir
+        return ed["done"]
+
     def collect(self):
         """(I_dir, I_exc) as (T, P, L_max+1) float64 arrays."""
         nf = self.n_forms
+        if self.early_direct is not None:
+            I_dir = self.collect_direct()
+            res = self.out[1:nf:2].cpu().numpy()  # synchronises
+            self.nodesets.check()
+            I_exc = res.reshape(self.T, self.P, self.nl).copy()
+            self.add_exchange_host_terms(I_exc)
+            return I_dir, I_exc
         if self.engine in TC_TERMS:
             self.out[0:nf:2] = self.out_dir
             self.out[1:nf:2] = self.out_ex

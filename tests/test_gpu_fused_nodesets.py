@@ -14,8 +14,8 @@ import bench
 pytestmark = pytest.mark.gpu
 
 
-def _job(kind):
-    from dwba_b200.dwba_matrix_elements import GPUCache, _make_job
+def _inputs(kind):
+    """(grid, V, U, bounds, pairs) of the two test batches."""
     if kind == "log":
         g, z, bounds, pairs = bench.make_workload(N=3001, n_cont=96, n_bound=4, seed_shift=21)
         V = U = z
@@ -43,6 +43,12 @@ def _job(kind):
         u2p = (Z / 2) ** 2.5 / np.sqrt(6.0) * r * r * np.exp(-Z * r / 2)
         bounds = [(bench._Bound(0, u1s), bench._Bound(1, u2p))]
         V = U = -Z / r
+    return g, V, U, bounds, pairs
+
+
+def _job(kind):
+    from dwba_b200.dwba_matrix_elements import GPUCache, _make_job
+    g, V, U, bounds, pairs = _inputs(kind)
     cache = GPUCache.from_grid(g)
     job = _make_job(g, V, U, [b[0] for b in bounds], [b[1] for b in bounds], pairs, 6, U, {}, cache)
     return job, cache
@@ -93,3 +99,23 @@ def test_chunked_wave_upload_gives_the_same_integrals():
     for d, e in res[1:]:
         assert np.array_equal(d, res[0][0]) and np.array_equal(e, res[0][1])
     assert np.isfinite(res[0][0]).all() and np.abs(res[0][1]).max() > 0
+
+
+@pytest.mark.parametrize("kind", ["log", "coulomb"])
+def test_result_objects_with_direct_rows_first_match_the_arrays(kind):
+    """Returning result objects, the batch entry point copies the direct rows (dot forms and device
+    tails) back before the exchange forms run and fills their dicts meanwhile; every value must equal
+    the as_arrays call's (which collects everything at the end), including the tails' contribution."""
+    from dwba_b200.dwba_matrix_elements import GPUCache, RadialDWBAIntegrals, radial_ME_all_L_batch
+    g, V, U, bounds, pairs = _inputs(kind)
+    cache = GPUCache.from_grid(g)
+    b_i, b_f = [b[0] for b in bounds], [b[1] for b in bounds]
+    I_d, I_e = radial_ME_all_L_batch(g, V, U, b_i, b_f, pairs, 6, U_f_array=U, gpu_cache=cache, engine="semisep",
+                                     as_arrays=True)
+    res = radial_ME_all_L_batch(g, V, U, b_i, b_f, pairs, 6, U_f_array=U, gpu_cache=cache, engine="semisep")
+    assert len(res) == len(bounds) and all(len(r) == len(pairs) for r in res)
+    for t, row in enumerate(res):
+        for p, x in enumerate(row):
+            assert type(x) is RadialDWBAIntegrals
+            assert [x.I_L_direct[L] for L in range(7)] == I_d[t, p].tolist()
+            assert [x.I_L_exchange[L] for L in range(7)] == I_e[t, p].tolist()

@@ -102,11 +102,13 @@ def test_chunked_wave_upload_gives_the_same_integrals():
 
 
 @pytest.mark.parametrize("kind", ["log", "coulomb"])
-def test_result_objects_with_direct_rows_first_match_the_arrays(kind):
+def test_result_objects_with_direct_rows_first_match_the_arrays(kind, monkeypatch):
     """Returning result objects, the batch entry point copies the direct rows (dot forms and device
     tails) back before the exchange forms run and fills their dicts meanwhile; every value must equal
     the as_arrays call's (which collects everything at the end), including the tails' contribution."""
+    from dwba_b200 import dwba_matrix_elements as dme
     from dwba_b200.dwba_matrix_elements import GPUCache, RadialDWBAIntegrals, radial_ME_all_L_batch
+    monkeypatch.setattr(dme, "EARLY_DIRECT_MIN_FORMS", 1)  # the small Coulomb batch (with tails) too
     g, V, U, bounds, pairs = _inputs(kind)
     cache = GPUCache.from_grid(g)
     b_i, b_f = [b[0] for b in bounds], [b[1] for b in bounds]

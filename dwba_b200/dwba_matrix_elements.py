@@ -250,12 +250,14 @@ def _no_gc(fn):
     return wrapper
 
 
-def _early_upload(job, device):
+def _early_upload(job, device, prestaged=None):
     """The job's functions (continuum waves, bound pairs) as rows of one device matrix, copied before
     the host planning so that a copy from pinned memory overlaps it; planning and preparation then
-    find them uploaded."""
+    find them uploaded. ``prestaged``: a copy of the waves started before the job was made
+    (engine.prestage_waves), used when the packed waves turn out to be exactly its rows."""
     from .engine import WaveMatrix
     waves = WaveMatrix(job.grid.N)
+    waves.prestaged = prestaged
     packed = getattr(job, "_packed", None)
     if packed is not None:
         packed.first, packed.owner = waves.add_distinct(packed.arrays, packed.ptrs), waves
@@ -306,19 +308,22 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
     import torch
     if not torch.cuda.is_available():
         raise RuntimeError("radial_ME_all_L: no CUDA device available (the B200 engine has no CPU fallback)")
-    from .engine import PreparedJob, plan_job
+    from .engine import PreparedJob, plan_job, prestage_waves
     from . import tune
     cache = _cache_for(grid, gpu_cache)
     eng = _engine_name(engine)
-    job = _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, cache)
     with torch.cuda.device(cache.device):
+        # the waves' copy starts before packing when they are rows of one pinned matrix
+        n_bound = len(bound_i) if isinstance(bound_i, (list, tuple)) else 1
+        pre = prestage_waves(pairs, cache.info.N, 2 * n_bound, cache.device) if semantics == "cpu" else None
+        job = _make_job(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_array, kw, cache)
         if semantics == "cupy":
             from .cupy_mode import CupyPreparedJob
             pj = CupyPreparedJob(job, cache.dg)
             pj.launch()
             I_dir, I_exc = pj.collect()
             return (I_dir, I_exc) if as_arrays else _results(I_dir, I_exc)
-        plans = plan_job(job, _early_upload(job, cache.device))
+        plans = plan_job(job, _early_upload(job, cache.device, pre))
         if tune.is_auto(eng):
             cands = tune.candidates(eng)
             key = tune.TUNER.key(cache.info.N, 2 * len(job.transitions) * len(job.pairs), L_max, cands)

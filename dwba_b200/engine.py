@@ -591,6 +591,61 @@ def _copy_stream(device) -> "torch.cuda.Stream":
     return st
 
 
+class Prestaged(NamedTuple):
+    """Rows [r0, r0 + n) of a pinned host matrix already on their way to rows [0, n) of ``out`` (a
+    device matrix with room for ``out.shape[0] - n`` more rows), in parts with an event after each."""
+    out: torch.Tensor
+    base_ptr: int
+    row_bytes: int
+    r0: int
+    n: int
+    chunks: list
+
+
+def prestage_waves(pairs, N: int, n_extra: int, device) -> Optional[Prestaged]:
+    """Start the copy of a batch's waves before the batch is packed, when its first and last waves
+    are rows of one page-locked C-contiguous host matrix of N columns whose rows between them hold
+    the pairs' two waves in turn (2 P rows, the order packing numbers them in). The upload checks
+    every wave's address against that block afterwards and otherwise copies as usual; a block
+    copied in vain costs device bandwidth, not correctness."""
+    try:
+        c0, c1 = pairs[0][0].chi_of_r, pairs[-1][1].chi_of_r
+    except (AttributeError, IndexError, TypeError):
+        return None
+    b = getattr(c0, "base", None)
+    if (b is None or getattr(c1, "base", None) is not b or not isinstance(b, np.ndarray) or b.ndim != 2 or
+            b.dtype != np.float64 or not b.flags.c_contiguous or b.shape[1] != N or
+            not isinstance(c0, np.ndarray) or not isinstance(c1, np.ndarray) or c0.dtype != np.float64 or
+            c1.dtype != np.float64 or c0.shape != (N,) or c1.shape != (N,)):
+        return None
+    bp, rb = b.__array_interface__["data"][0], 8 * N
+    o0, o1 = c0.__array_interface__["data"][0] - bp, c1.__array_interface__["data"][0] - bp
+    if o0 % rb or o1 % rb:
+        return None
+    r0, r1 = o0 // rb, o1 // rb
+    n = r1 - r0 + 1
+    if not (0 <= r0 <= r1 < b.shape[0]) or n != 2 * len(pairs):
+        return None
+    src = torch.from_numpy(b[r0:r1 + 1])
+    if not src.is_pinned():
+        return None
+    dev = torch.device(device)
+    out = torch.empty((n + max(1, n_extra), N), dtype=torch.float64, device=dev)
+    cs = _copy_stream(out.device)
+    cs.wait_stream(torch.cuda.current_stream(out.device))  # out belongs to the current stream
+    chunks = []
+    with torch.cuda.stream(cs):
+        cuts = [n * k // WAVE_CHUNKS for k in range(WAVE_CHUNKS + 1)]
+        for a, c in zip(cuts[:-1], cuts[1:]):
+            if c > a:
+                out[a:c].copy_(src[a:c], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(cs)
+                chunks.append((a, c, ev))
+    out.record_stream(cs)
+    return Prestaged(out, bp + r0 * rb, rb, r0, n, chunks)
+
+
 class WaveMatrix:
     """Distinct 1-D functions of a job as rows of one host matrix (dedup by host buffer)."""
 
@@ -605,6 +660,7 @@ class WaveMatrix:
         # side-stream upload of a block copied in row order: (first row, end row, event after it) of
         # each of its WAVE_CHUNKS parts, so that kernels reading only early rows can start sooner
         self.chunks: Optional[List[Tuple[int, int, torch.cuda.Event]]] = None
+        self.prestaged: Optional[Prestaged] = None  # waves already on their way (prestage_waves)
 
     def wait_ready(self) -> None:
         """Order the current stream after a side-stream upload (``upload(..., side_stream=True)``);
@@ -693,6 +749,9 @@ class WaveMatrix:
         cached = self._uploaded.get(str(device))
         if cached is not None and cached[0] == n:
             return cached[1]  # already on the device (no rows added since)
+        pre, self.prestaged = self.prestaged, None
+        if side_stream and pre is not None and self._takes(pre):
+            return self._adopt(pre, device)
         out = torch.empty((max(1, n), N), dtype=torch.float64, device=device)
         done = np.zeros(n, dtype=bool)
         groups: Dict[int, list] = {}
@@ -788,6 +847,29 @@ class WaveMatrix:
                 src = torch.from_numpy(block)
                 dev_block = src.to(device, non_blocking=src.is_pinned())
                 out.index_copy_(0, dst, dev_block.index_select(0, sel)[:, :N])
+        self._uploaded[str(device)] = (n, out)
+        return out
+
+    def _takes(self, pre: Prestaged) -> bool:
+        """Whether the prestaged block holds exactly this matrix's first rows: the packed waves, in
+        order, at the block's addresses (and room for the rest)."""
+        first = self._ptrs.get(0)
+        if first is None or first[0] != pre.n or len(self.arrays) > pre.out.shape[0]:
+            return False
+        want = pre.base_ptr + pre.row_bytes * np.arange(pre.n, dtype=np.int64)
+        return bool(np.array_equal(first[1], want))
+
+    def _adopt(self, pre: Prestaged, device) -> torch.Tensor:
+        """Rows [0, n) are the prestaged block (its parts become ``chunks``); the other rows follow
+        as in ``upload``, after which ``ready`` covers everything."""
+        out, N, n = pre.out, self.N, len(self.arrays)
+        done = np.zeros(n, dtype=bool)
+        done[:pre.n] = True
+        self._copy_rows(out, done, N, n, stage=True)
+        cs = _copy_stream(out.device)
+        self.ready = torch.cuda.Event()
+        self.ready.record(cs)
+        self.chunks = list(pre.chunks)
         self._uploaded[str(device)] = (n, out)
         return out
 

@@ -333,7 +333,7 @@ def _run(grid, V_core_array, U_i_array, bound_i, bound_f, pairs, L_max, U_f_arra
         else:
             # direct rows copied back first only where the fill of their dicts is worth overlapping
             early = not as_arrays and len(job.transitions) * len(job.pairs) >= EARLY_DIRECT_MIN_FORMS
-            pj = PreparedJob(job, cache.dg, eng, plans=plans, early_direct=early)
+            pj = PreparedJob(job, cache.dg, eng, plans=plans, early_direct=early, early_nodesets=True)
             pj.launch()
         # the result objects are made while the kernels run; collect() then waits for them
         skel = None if as_arrays else _skeleton(len(job.transitions), len(job.pairs), job.L_max + 1)

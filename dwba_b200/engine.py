@@ -1298,13 +1298,16 @@ class PreparedJob:
     ``launch()`` enqueues every kernel on the current stream: node-set operators (those not
     yet cached for the grid, or all of them with ``rebuild_nodesets``), operand folds and the
     bilinear forms. ``collect()`` copies the results back once and adds the host-side L=0
-    corrections and outer tails. Results are indexed [transition, pair, L]. With ``early_direct``
+    corrections and outer tails. Results are indexed [transition, pair, L]. With ``early_nodesets``
+    the constructor enqueues the node sets as soon as their descriptors exist (the first
+    ``launch()`` then enqueues the rest). With ``early_direct``
     (exact engine, every direct form through the potentials), the direct rows are copied back
     before the exchange forms run, and ``collect_direct()`` returns them first.
     """
 
     def __init__(self, job: Job, dg: DeviceGrid, engine: str = "dense", plans=None,
-                 rebuild_nodesets: bool = False, fuse_folds: Optional[bool] = None, early_direct: bool = False):
+                 rebuild_nodesets: bool = False, fuse_folds: Optional[bool] = None, early_direct: bool = False,
+                 early_nodesets: bool = False):
         if engine not in ENGINES:
             raise ValueError(f"unknown engine {engine!r}; choose from {ENGINES}")
         if job.L_max < 0:
@@ -1472,6 +1475,12 @@ class PreparedJob:
                 multi = _take(multi, np.nonzero(np.repeat(~fg, 2))[0])
         elif self.nodesets.n_fused:
             raise RuntimeError("fused node sets without multi-folds")
+        self._nodesets_enqueued = False
+        if early_nodesets:
+            # the node sets (and the folds applied with them) need nothing built below: enqueued
+            # now, they run while the rest of the descriptors are made; launch() then skips them once
+            self.nodesets.launch(waves)
+            self._nodesets_enqueued = True
         self.multi_host = multi
         self.n_multi = len(multi)
         self.multi_d = _dev(multi.view(np.uint8), dev) if len(multi) else None
@@ -1629,7 +1638,10 @@ class PreparedJob:
             self.form_launch.launch(lib, job.L_max, self.ds, float(job.grid.r[0]), float(job.grid.r[-1]))
 
     def launch(self) -> None:
-        self.nodesets.launch(self.waves)  # stored sets at once, fused sets as their waves arrive
+        if self._nodesets_enqueued:
+            self._nodesets_enqueued = False  # enqueued by the constructor (early_nodesets)
+        else:
+            self.nodesets.launch(self.waves)  # stored sets at once, fused sets as their waves arrive
         self.waves.wait_ready()
         if self.early_direct is not None:
             # direct forms and tails first; their rows go back to the host while the exchange

@@ -562,7 +562,7 @@ def _dphis(job: Job, n1: np.ndarray, k_total: np.ndarray, eta_total: np.ndarray)
     return d
 
 
-WAVE_CHUNKS = 4  # parts of a side-stream wave upload that kernels can wait for one by one
+WAVE_CHUNKS = 8  # parts of a side-stream wave upload that kernels can wait for one by one
 
 
 def _in_order(idx, rows, N: int, block: np.ndarray) -> Optional[int]:

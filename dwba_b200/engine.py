@@ -17,6 +17,7 @@ import functools
 import hashlib
 from itertools import repeat
 import operator
+import threading
 from typing import Dict, List, NamedTuple, Optional, Sequence, Tuple
 
 import numpy as np
@@ -143,24 +144,32 @@ class _Staging:
         self.host = self.buf.numpy()
         self.ptr = self.buf.data_ptr()
         self.regions = RingRegions(self.SIZE)
+        self.lock = threading.Lock()  # callers on several host threads share the ring
+
+    _make_lock = threading.Lock()
 
     @classmethod
     def get(cls, index: int) -> "_Staging":
         st = cls._by_device.get(index)
         if st is None:
-            st = cls._by_device[index] = cls()
+            with cls._make_lock:
+                st = cls._by_device.get(index)
+                if st is None:
+                    st = cls._by_device[index] = cls()
         return st
 
     def copy(self, x: np.ndarray, out: torch.Tensor) -> None:
         raw = x.reshape(-1).view(np.uint8)
         n = len(raw)
         ev = torch.cuda.Event()
-        a, _, release = self.regions.alloc(n, ev)
-        for old in release:
-            old.synchronize()  # the earlier copy from this region must have run
-        self.host[a:a + n] = raw
-        _lib.check(_lib.load().dwba_copy_from_host(out.data_ptr(), self.ptr + a, n, _stream()), "dwba_copy_from_host")
-        ev.record()
+        with self.lock:
+            a, _, release = self.regions.alloc(n, ev)
+            for old in release:
+                old.synchronize()  # the earlier copy from this region must have run
+            self.host[a:a + n] = raw
+            _lib.check(_lib.load().dwba_copy_from_host(out.data_ptr(), self.ptr + a, n, _stream()),
+                       "dwba_copy_from_host")
+            ev.record()
 
 
 def _dev(x: np.ndarray, device) -> torch.Tensor:

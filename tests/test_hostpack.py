@@ -88,3 +88,28 @@ def test_result_objects_match_the_python_path():
         _hostpack.fill_results(dicts, np.zeros(2 * 3 * 4 - 1), np.zeros(2 * 3 * 4), 4)
     with pytest.raises(ValueError):
         _hostpack.fill_results(dicts, np.zeros(24, dtype=np.float32), np.zeros(24), 4)
+
+
+def test_prestaged_block_is_taken_only_for_its_exact_rows():
+    """A wave copy started before packing (engine.prestage_waves) is used only when the packed waves
+    are exactly the block's rows, in order; chunk_of maps rows to the parts of such an upload."""
+    from dwba_b200.engine import Prestaged
+    g, z, bounds, pairs = bench.make_workload(N=129, n_cont=10, n_bound=1, seed_shift=8)
+    base = pairs[0][0].chi_of_r.base
+    bp, rb = base.__array_interface__["data"][0], 8 * 129
+    pre = Prestaged(torch.empty((20 + 2, 129), dtype=torch.float64), bp, rb, 0, 20, [])
+    pk = _pack(pairs, 129)
+    w = WaveMatrix(129)
+    pk.first, pk.owner = w.add_distinct(pk.arrays, pk.ptrs), w
+    assert w._takes(pre)
+    assert not w._takes(pre._replace(base_ptr=bp + rb))  # the block one row off
+    assert not w._takes(pre._replace(n=19))
+    shuffled = pairs[1:] + pairs[:1]
+    pk2 = _pack(shuffled, 129)
+    w2 = WaveMatrix(129)
+    pk2.first, pk2.owner = w2.add_distinct(pk2.arrays, pk2.ptrs), w2
+    assert not w2._takes(pre)
+    w.chunks = [(0, 8, None), (8, 20, None)]
+    assert list(w.chunk_of(np.array([0, 7, 8, 19, 20, 21]))) == [0, 0, 1, 1, 2, 2]
+    w.chunks = None
+    assert list(w.chunk_of(np.array([3, 30]))) == [0, 0]

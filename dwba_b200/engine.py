@@ -1295,7 +1295,7 @@ def fusable_sets(plans: "JobPlan", T: int) -> Optional[np.ndarray]:
     first_p = np.full(n_sets, -1, dtype=np.int64)
     first_p[k[::-1]] = p_i[::-1]  # some pair of each set
     single = np.ones(n_sets, dtype=bool)
-    single[np.unique(k[p_i != first_p[k]])] = False  # another pair uses it
+    single[k[p_i != first_p[k]]] = False  # another pair uses it
     n_t = np.bincount(k, minlength=n_sets)
     ok = single & (n_t >= 1) & (n_t <= _lib.FOLD_MULTI - 1)
     return ok
@@ -1429,7 +1429,10 @@ class PreparedJob:
         if A_parts:
             cols = [np.concatenate(c) for c in zip(*A_parts)]
             t_a, p_a, k_a, adir_a, aex_a, bex_a, n1_a, nb_a, uf_a, ui_a, fo_a = cols
-            order = np.lexsort((t_a, k_a, p_a))
+            # by pair, then node set, then transition (a stable sort of one composite key: the order
+            # of np.lexsort((t_a, k_a, p_a)), which takes several times as long)
+            nk, nt = int(k_a.max()) + 1, int(t_a.max()) + 1
+            order = np.argsort((p_a * nk + k_a) * nt + t_a, kind="stable")
             t_a, p_a, k_a, adir_a, aex_a, bex_a, n1_a, nb_a, uf_a, ui_a, fo_a = (c[order] for c in cols)
             n = len(p_a)
             new_run = np.ones(n, dtype=bool)
@@ -1466,7 +1469,8 @@ class PreparedJob:
                 pos[ns.fused_idx] = np.arange(ns.n_fused)
                 q = pos[kf]
                 fg = q >= 0
-                if int(np.count_nonzero(fg)) != ns.n_fused or len(np.unique(q[fg])) != ns.n_fused:
+                if int(np.count_nonzero(fg)) != ns.n_fused or \
+                        int(np.count_nonzero(np.bincount(q[fg], minlength=ns.n_fused))) != ns.n_fused:
                     raise RuntimeError("fused node sets must serve exactly one multi-fold group each")
                 sel = np.nonzero(fg)[0][np.argsort(q[fg], kind="stable")]  # groups in node-set order
                 if waves.chunks is not None:

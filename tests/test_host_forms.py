@@ -232,3 +232,51 @@ def test_fused_node_sets_carry_their_pairs_folds():
     # a job with fewer single-pair sets than the threshold stores its operators
     small = _make_job(g, z, z, [b[0] for b in bounds], [b[1] for b in bounds], pairs[:8], 4, z, {}, Cache)
     assert PreparedJob(small, Cache.dg, "semisep", rebuild_nodesets=True).nodesets.n_fused == 0
+
+
+def test_fused_sets_grouped_by_the_part_of_the_wave_upload_they_read():
+    """With the waves uploaded in parts (WaveMatrix.chunks), the fused node sets are reordered so that
+    each launch group reads only waves of its part: the groups tile the sets in ascending part order,
+    every set's pair has its waves in the group's part (or the last group waits for everything), and
+    the records and fold descriptors are permuted together (each set keeps its own folds)."""
+    from dwba_b200.dwba_matrix_elements import _make_job
+    from dwba_b200.engine import FUSE_MIN_SETS, DeviceGrid, PreparedJob
+    from dwba_b200.plan import GridInfo
+    g, z, bounds, pairs = bench.make_workload(N=801, n_cont=FUSE_MIN_SETS + 10, n_bound=2, seed_shift=13)
+
+    class Cache:
+        info = GridInfo(g.r, g.w_simpson, g.w_trapz)
+        dg = DeviceGrid(info, torch.device("cpu"))
+    job = _make_job(g, z, z, [b[0] for b in bounds], [b[1] for b in bounds], pairs, 4, z, {}, Cache)
+    ref = PreparedJob(job, Cache.dg, "semisep", rebuild_nodesets=True)
+    waves = job._waves
+    waves.chunks = [(0, 37, None), (37, 90, None), (90, 120, None)]  # rows beyond 120: the whole upload
+    got = PreparedJob(job, Cache.dg, "semisep", plans=ref.plans, rebuild_nodesets=True)
+    ns, ns0 = got.nodesets, ref.nodesets
+    groups = ns.fused_groups
+    assert len(groups) > 1 and groups[0][1] == 0 and groups[-1][2] == ns.n_fused
+    assert all(a[2] == b[1] and a[0] < b[0] for a, b in zip(groups[:-1], groups[1:]))
+    wi, wf = job._wave_idx
+    set_pair = {}
+    for (t, p), k in np.ndenumerate(ref.plans.ns_index):
+        if k >= 0:
+            set_pair[int(k)] = p
+    for k_part, a, b in groups:
+        for j in range(a, b):
+            p = set_pair[int(ns.fused_idx[j])]
+            assert waves.chunk_of(np.array([max(wi[p], wf[p])]))[0] == k_part
+    # records and folds follow the same permutation of the sets
+    by_set0 = {int(k): (bytes(ns0.fused_recs[q].tobytes()),) for q, k in enumerate(ns0.fused_idx)}
+    by_set = {int(k): (bytes(ns.fused_recs[q].tobytes()),) for q, k in enumerate(ns.fused_idx)}
+    assert sorted(by_set) == sorted(by_set0)
+    def rel(m, job_):  # fold pointers as offsets into the job's function and operand matrices
+        F, O = job_.F.data_ptr(), job_.ops.data_ptr()
+        return ((int(m["g"]) - F,) + tuple(int(x) - F for x in m["f"][:m["n_f"]]) +
+                tuple(int(x) - O for x in m["out"][:m["n_f"]]) +
+                tuple(int(m[f]) for f in ("n_f", "half_band", "n_out", "n_src", "n_clear")))
+    for k in by_set0:  # the same record and the same folds (relative to each job's buffers)
+        assert by_set[k][0] == by_set0[k][0]
+        q0, q = list(ns0.fused_idx).index(k), list(ns.fused_idx).index(k)
+        for h in (0, 1):
+            assert rel(ns.fused_folds[2 * q + h], got) == rel(ns0.fused_folds[2 * q0 + h], ref)
+    assert list(ns.fused_idx) != list(ns0.fused_idx)  # the order did change

@@ -83,6 +83,17 @@ def test_result_objects_match_the_python_path():
         assert all(type(v) is float for v in x.I_L_exchange.values())
         with pytest.raises(dataclasses.FrozenInstanceError):
             x.I_L_direct = {}
+    # the direct and the exchange halves filled separately (direct rows first, as the batch entry
+    # point does while the exchange forms still run) give the same objects
+    I_d, I_e = rng.standard_normal((2, 5, 9)), rng.standard_normal((2, 5, 9))
+    res, dicts = dme._skeleton(2, 5, 9)
+    _hostpack.fill_half(dicts, I_d, 9, 0)
+    _hostpack.fill_half(dicts, I_e, 9, 1)
+    assert res == dme._results(I_d, I_e)
+    with pytest.raises(ValueError):
+        _hostpack.fill_half(dicts, I_d, 9, 2)
+    with pytest.raises(ValueError):
+        _hostpack.fill_half(dicts, I_d[:1], 9, 0)
     _, dicts = dme._skeleton(2, 3, 4)
     with pytest.raises(ValueError):
         _hostpack.fill_results(dicts, np.zeros(2 * 3 * 4 - 1), np.zeros(2 * 3 * 4), 4)

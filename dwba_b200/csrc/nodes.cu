@@ -78,7 +78,7 @@ constexpr int OWN_ROWS = 30;
 #define DWBA_NODESET_FOLD_MIN_BLOCKS 32
 #endif
 #ifndef DWBA_NODESET_FC
-#define DWBA_NODESET_FC 2  // factors per chunk of the fold loads (2: 2.47 ms, 4: 2.49 ms, 8 spills: 3.32 ms)
+#define DWBA_NODESET_FC 1  // factors per chunk of the fold loads (1: 2.39 ms, 2: 2.47 ms, 4: 2.49 ms, 8 spills: 3.32 ms)
 #endif
 #ifndef DWBA_NODESET_WARPS
 #define DWBA_NODESET_WARPS 1  // warps per CTA, each on its own row blocks of the CTA's set
@@ -125,7 +125,7 @@ __device__ __forceinline__ void fold_row_from_taps(const dwba_fold_multi_t& m, i
 #pragma unroll
         for (int d = -H; d <= H; ++d)
           if (in[d + H]) acc += tp[d + H] * (fv[c][d + H] * gv[d + H]);
-        m.out_dev[t0 + c][i] = acc;
+        __stcs(m.out_dev[t0 + c] + i, acc);  // streaming store: the folded operands are read by the next kernels from DRAM
       }
     }
   }
